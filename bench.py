@@ -1,0 +1,311 @@
+"""Benchmark: FP64 Mpoint-stages/s of the GATT_DNS RK4 time step on the 128^3 periodic box.
+
+Workload (one "step"): one full time step of main.F90:255-465 -- four RK4 stages of the
+compressible Navier-Stokes right-hand side with compact SL4 derivatives (cyclic line
+solves in x, y, z), the 10th-order compact filter, boundary conditions (none on the
+periodic box) and the max-change residual -- on a 128^3 grid, Re = 1600, Ma = 0.3, with a
+seeded solenoidal initial field.  Throughput counts grid points x 4 stages per step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun, one rank per GPU): every rank advances its own box (batch
+sharding of independent flows, no data-path collective: weak scaling); the timing is the
+max over ranks.  --impl reference times the CPU restatement of the reference on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_GRID = 128
+STAGES = 4
+# Sweep-model bytes per 3-D point-stage: 27 derivative sweeps x 16 B + 5 fields x 32 B of
+# RK state traffic + 15 filter sweeps x 16 B / 4 stages.
+BYTES_PER_POINT_STAGE = 27 * 16 + 5 * 32 + 15 * 16 / 4
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=N_GRID)
+    p.add_argument("--no-clocks", action="store_true")
+    return p.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1])); mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args, world, rank):
+    """CPU restatement of the reference, all host threads, rank 0 only."""
+    if rank != 0:
+        return
+    import oracle
+    from gatt_dns_b200 import case as cs
+    oracle.build()
+    c = cs.periodic_box(n=args.n)
+    o = oracle.Oracle(c)
+    cores = o.lib.orc_num_threads()
+    f = cs.solenoidal_turbulence(c, seed=1234)
+    dt = c.cfl_dt(f["U"], f["V"], f["W"], 0.5)
+    st = o.new_state(f)
+    t = 0.0
+    for _ in range(max(args.warmup, 1)):
+        o.step(st, t, dt); t += dt
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.step(st, t, dt); t += dt
+    el = time.perf_counter() - t0
+    npts = c.npts
+    value = npts * STAGES * args.steps / el / 1e6
+    line = {"metric": "FP64 Mpoint-stages/s (RK4 step, 128^3 periodic box)", "value": value,
+            "unit": "Mpoint-stages/s", "impl": "reference", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded solenoidal field)",
+            "config": {"workload": "periodic_box_%d^3_rk4_step" % args.n, "grid": [args.n] * 3, "Re": 1600,
+                       "Ma": 0.3, "scheme": "SL4 compact + 10th-order filter (alpha 0.49)"},
+            "cpu_baseline": {"value": value, "unit": "Mpoint-stages/s", "cores": cores, "kind": "port",
+                             "sample": "%d full RK4 steps of the %d^3 box (C restatement of the reference "
+                                       "Fortran, OpenMP over lines)" % (args.steps, args.n)},
+            "e2e": {"value": value, "unit": "Mpoint-stages/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(c, seconds=10.0):
+    """Oracle timed on a bounded sample (whole steps until ~`seconds` of CPU work)."""
+    import oracle
+    oracle.build()
+    from gatt_dns_b200 import case as cs
+    o = oracle.Oracle(c)
+    f = cs.solenoidal_turbulence(c, seed=1234)
+    dt = c.cfl_dt(f["U"], f["V"], f["W"], 0.5)
+    st = o.new_state(f)
+    o.step(st, 0.0, dt)  # warm
+    n, t0 = 0, time.perf_counter()
+    while True:
+        o.step(st, n * dt, dt)
+        n += 1
+        el = time.perf_counter() - t0
+        if el > seconds or n >= 20:
+            break
+    v = c.npts * STAGES * n / el / 1e6
+    return {"value": v, "unit": "Mpoint-stages/s", "cores": o.lib.orc_num_threads(), "kind": "port",
+            "sample": "%d full RK4 steps of the %d^3 box in %.1f s (C restatement of the reference Fortran, "
+                      "OpenMP over lines)" % (n, c.nx, el)}
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from gatt_dns_b200 import build as bld
+    if rank == 0:
+        bld.build()
+    if world > 1:
+        dist.barrier()
+    from gatt_dns_b200 import case as cs
+    from gatt_dns_b200.solver import GattDNS
+
+    c = cs.periodic_box(n=args.n)
+    f = cs.solenoidal_turbulence(c, seed=1234 + rank)
+    dt = c.cfl_dt(f["U"], f["V"], f["W"], 0.5)
+    stream = torch.cuda.Stream()
+    g = GattDNS(c, stream=stream.cuda_stream)
+    npts = c.npts
+
+    # pinned host buffers for the end-to-end leg
+    pinned = {k: torch.from_numpy(np.ascontiguousarray(f[k].ravel(order="F"))).pin_memory() for k in "UVWRE"}
+    host = {k: pinned[k].numpy().reshape((c.nx, c.ny, c.nz), order="F") for k in "UVWRE"}
+    pinned_out = {k: torch.empty(npts, dtype=torch.float64).pin_memory() for k in "UVWRE"}
+    host_out = {k: pinned_out[k].numpy().reshape((c.nx, c.ny, c.nz), order="F") for k in "UVWRE"}
+    g.upload(host)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # warm-up (also captures the step graphs)
+    g.run(max(args.warmup, 3), 0.0, dt)
+    t = max(args.warmup, 3) * dt
+
+    # ---- device-resident timed region -------------------------------------------
+    sampler = ClockSampler(local)
+    if not args.no_clocks:
+        sampler.start()
+        time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    l0 = g.kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    mc = g.run(args.steps, t, dt)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop() if not args.no_clocks else None
+    launches = g.kernel_launches() - l0
+    ms = ev0.elapsed_time(ev1)
+    t += args.steps * dt
+    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * npts * STAGES * args.steps / (ms_max / 1e3) / 1e6
+
+    # ---- end-to-end through the C-ABI with host buffers ------------------------------
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    e0.record(stream)
+    g.upload(host)                       # H2D of the flow from pinned memory
+    for s in range(args.steps):
+        g.step(t + s * dt, dt)           # per step: params H2D, graph, maxChange D2H + sync
+    g.download(out=host_out)             # D2H of the flow into pinned memory
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - w0
+    e_ms = max(e0.elapsed_time(e1), wall * 1e3)
+    et = torch.tensor([e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+    e2e_value = world * npts * STAGES * args.steps / (float(et.item()) / 1e3) / 1e6
+    field_bytes = 5 * npts * 8
+    h2d = (field_bytes + args.steps * 24) / args.steps
+    d2h = (field_bytes + args.steps * 5 * 8) / args.steps
+
+    # ---- per-kernel timing for the roofline (CUDA events around each launch) ------------
+    prof = g.profile_kernels(t, dt, nsteps=2)
+    # algorithmic bytes per launch: a line solve reads and writes each of its fields once
+    alg = {"sweep_d1_x": 5 * 16, "sweep_d1_y": 5 * 16, "sweep_d1_z": 5 * 16,
+           "sweep_d2_x": 4 * 16, "sweep_d2_y": 4 * 16, "sweep_d2_z": 4 * 16,
+           "filter_x": 5 * 16, "filter_y": 5 * 16, "filter_z": 5 * 16,
+           "visc": (13 + 9) * 8, "assemble_rk": (5 + 15 + 6 + 12 + 5 + 5 + 5 + 5) * 8, "maxchange": 10 * 8}
+    per_step = {k: v[0] * v[1] for k, v in prof.items()}
+    dom = max(per_step, key=per_step.get)
+    peak, peak_kind = measured_peaks()
+    dom_ms = prof[dom][0]
+    dom_bytes = alg.get(dom, 0) * npts
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_bytes else None
+    step_ms = ms_max / args.steps
+    stage_model = BYTES_PER_POINT_STAGE * npts * STAGES / (step_ms / 1e3) / 1e9
+
+    line = {"metric": "FP64 Mpoint-stages/s (RK4 step, 128^3 periodic box)", "value": value,
+            "unit": "Mpoint-stages/s", "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded solenoidal field, E(k)~k^4 exp(-2(k/4)^2), u_rms=1)",
+            "config": {"workload": "periodic_box_%d^3_rk4_step" % args.n, "grid": [args.n] * 3, "Re": 1600,
+                       "Ma": 0.3, "scheme": "SL4 compact + 10th-order filter (alpha 0.49)",
+                       "per_gpu": "one independent box per GPU",
+                       "parallelism": "batch-sharded replicas x%d" % world,
+                       "l2": "inputs larger than L2 (working set %.2f GB per GPU > 126 MB)" % (
+                           (5 * 5 + 15 + 9 + 12 + 2) * npts * 8 / 1e9)},
+            "e2e": {"value": e2e_value, "unit": "Mpoint-stages/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "path": "gatt_upload from pinned host, K x gatt_step (host maxChange each step), gatt_download"},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "peak_source": peak_kind,
+                         "step_sweep_model_gbs": stage_model, "step_sweep_model_frac": stage_model / peak},
+            "kernels_ms_per_launch": {k: round(v[0], 5) for k, v in prof.items() if v[1] > 0},
+            "max_change_last": [float(x) for x in mc[0]]}
+    if clocks:
+        line["clocks"] = clocks
+    if rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_baseline_sample(c)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    g.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1228 @@
+// C-ABI implementation of the B200 GATT_DNS hot path (see include/gatt_dns.h).
+//
+// One context = one grid, `nbatch` flow states, one CUDA stream.  Device memory per
+// member is laid out [member][slot][point]; the time step is captured once into a
+// CUDA graph (one per state-buffer parity) and replayed with per-step {t, dt} copied
+// into a device parameter block, so a step costs one small copy plus one graph launch.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gatt_dns.h"
+#include "bc.cuh"
+#include "pointwise.cuh"
+#include "sweep.cuh"
+
+using namespace gatt;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+#define CU(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(e_ == cudaErrorMemoryAllocation ? GATT_ERR_NOMEM : GATT_ERR_CUDA,          \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                       \
+    } while (0)
+
+#define TRY(expr)                     \
+    do {                              \
+        int r_ = (expr);              \
+        if (r_ != GATT_OK) return r_; \
+    } while (0)
+
+struct DevDir {
+    bool set = false;
+    int periodic = 0, nR = 0, nTypes = 0, N = 0, W = 0;
+    double *R = nullptr, *A = nullptr, *B = nullptr, *C = nullptr, *D = nullptr;
+};
+
+struct HostBC {
+    std::vector<int> ind;     // n*6, Fortran (n,6) column-major
+    std::vector<double> val;  // Dirichlet values
+    std::vector<int> dirs;    // Neumann / second-derivative directions
+    int n = 0;
+};
+
+struct Dist {
+    int type, var, ind[6], xoff;
+    double par;
+};
+
+constexpr int kBlock = 256;
+
+// kernel classes reported by gatt_profile_kernels (names in gatt_profile_name)
+enum {
+    PC_D1X = 0, PC_D1Y, PC_D1Z, PC_VISC, PC_D2X, PC_D2Y, PC_D2Z, PC_ASSEMBLE, PC_BC,
+    PC_FX, PC_FY, PC_FZ, PC_SFD, PC_MAXCHANGE, PC_OTHER, PC_N
+};
+const char *const kProfNames[PC_N] = {
+    "sweep_d1_x", "sweep_d1_y", "sweep_d1_z", "visc", "sweep_d2_x", "sweep_d2_y", "sweep_d2_z",
+    "assemble_rk", "bc", "filter_x", "filter_y", "filter_z", "sfd", "maxchange", "other"};
+
+}  // namespace
+
+struct gatt_ctx {
+    int nx, ny, nz, nb;
+    long long npts;
+    bool is3d;
+    Phys ph{};
+    bool phys_set = false;
+    DevDir mat[3][2];
+    uint8_t *ltype[3] = {nullptr, nullptr, nullptr};
+    bool lt_set[3] = {false, false, false};
+    int lt_max[3] = {0, 0, 0};  // largest 0-based type in each direction's map
+    int filt[3] = {0, 0, 0};
+    double fct = -1.0;
+    // boundary data (host) and the device program built from it
+    HostBC bc[3][5];
+    std::vector<int> cL, cD, cAd;
+    int cN = 0;
+    std::vector<double> coef1, coef2;
+    std::vector<Dist> dists;
+    std::vector<double> distx;
+    BcOp *d_ops = nullptr;
+    int nops = 0;
+    double *d_coef1 = nullptr, *d_coef2 = nullptr, *d_xs = nullptr;
+    bool bc_dirty = true;
+    // SFD
+    int sfd_type = 0;
+    double sfd_delta = 0;
+    double *chi = nullptr;
+    // state and scratch
+    double *qA = nullptr, *qB = nullptr, *delta = nullptr, *mean = nullptr;
+    double *d1 = nullptr, *tq = nullptr, *d2 = nullptr, *P = nullptr, *tmp = nullptr;
+    double *tin = nullptr, *tout = nullptr;  // host-facing scratch (rhs / deriv entry points)
+    bool mean_init = false;                  // SFD mean uploaded or copied from the state
+    int cur = 0;
+    unsigned long long *acc = nullptr;
+    double *hist = nullptr;
+    int hist_cap = 0;
+    StepParams *d_params = nullptr;
+    StepParams *h_params = nullptr;  // pinned, hist_cap entries
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int graph_kernels[2] = {0, 0};
+    bool capturing = false;
+    int capture_count = 0;
+    long long launches = 0;
+    int nsm = 148;
+    // per-kernel-class timing (gatt_profile_kernels): events around every launch
+    bool profiling = false;
+    int prof_cls = -1;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<int> ev_cls;  // class of each begin/end event pair
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------------
+
+int grid_for(const gatt_ctx *c, long long n)
+{
+    long long g = (n + kBlock - 1) / kBlock;
+    long long cap = (long long)c->nsm * 8;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+// Mark the start of a launch of kernel class `cls` (only records when profiling).
+int before_launch(gatt_ctx *c, int cls)
+{
+    c->prof_cls = cls;
+    if (!c->profiling) return GATT_OK;
+    cudaEvent_t e;
+    CU(cudaEventCreate(&e));
+    CU(cudaEventRecord(e, c->stream));
+    c->ev_pool.push_back(e);
+    return GATT_OK;
+}
+
+int after_launch(gatt_ctx *c)
+{
+    if (c->profiling && c->prof_cls >= 0) {
+        cudaEvent_t e;
+        CU(cudaEventCreate(&e));
+        CU(cudaEventRecord(e, c->stream));
+        c->ev_pool.push_back(e);
+        c->ev_cls.push_back(c->prof_cls);
+    }
+    c->prof_cls = -1;
+    if (c->capturing) c->capture_count++;
+    else c->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(GATT_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    return GATT_OK;
+}
+
+int line_len(const gatt_ctx *c, int d) { return d == 0 ? c->nx : (d == 1 ? c->ny : c->nz); }
+int nlines(const gatt_ctx *c, int d)
+{
+    return d == 0 ? c->ny * c->nz : (d == 1 ? c->nx * c->nz : c->nx * c->ny);
+}
+
+// State set of the current (which = 0) or next (which = 1) buffer.  In 2-D, slot W of
+// buffer A is the caller's W and slot W of buffer B is main.F90's Wnew, never swapped.
+StateSet state_set(const gatt_ctx *c, int which)
+{
+    double *buf = ((c->cur ^ which) == 0) ? c->qA : c->qB;
+    StateSet s;
+    for (int f = 0; f < 5; f++) s.v[f] = buf + f * c->npts;
+    if (!c->is3d) s.v[2] = (which == 0 ? c->qA : c->qB) + 2 * c->npts;
+    s.bstride = 5 * c->npts;
+    return s;
+}
+
+FieldSet fset(const gatt_ctx *c, double *p, int nslots)
+{
+    FieldSet f;
+    f.p = p;
+    f.bstride = (long long)nslots * c->npts;
+    f.npts = c->npts;
+    return f;
+}
+
+int nd1(const gatt_ctx *c) { return c->is3d ? D3_N : D2_N; }
+int ntq(const gatt_ctx *c) { return c->is3d ? T3_N : T2_N; }
+int nd2(const gatt_ctx *c) { return c->is3d ? S3_N : S2_N; }
+
+// ---------------------------------------------------------------------------
+// line-solve dispatch
+// ---------------------------------------------------------------------------
+
+template <bool XD, bool PER, int EPI>
+void *pick_kernel(int nR)
+{
+    switch (nR) {
+    case 2: return (void *)k_sweep<XD, PER, 2, EPI>;
+    case 3: return (void *)k_sweep<XD, PER, 3, EPI>;
+    case 4: return (void *)k_sweep<XD, PER, 4, EPI>;
+    case 5: return (void *)k_sweep<XD, PER, 5, EPI>;
+    case 6: return (void *)k_sweep<XD, PER, 6, EPI>;
+    case 7: return (void *)k_sweep<XD, PER, 7, EPI>;
+    case 8: return (void *)k_sweep<XD, PER, 8, EPI>;
+    case 9: return (void *)k_sweep<XD, PER, 9, EPI>;
+    case 10: return (void *)k_sweep<XD, PER, 10, EPI>;
+    case 11: return (void *)k_sweep<XD, PER, 11, EPI>;
+    default: return nullptr;
+    }
+}
+
+void *sweep_kernel(bool xd, bool per, int epi, int nR)
+{
+    if (xd) {
+        if (per) return epi ? pick_kernel<true, true, 1>(nR) : pick_kernel<true, true, 0>(nR);
+        return epi ? pick_kernel<true, false, 1>(nR) : pick_kernel<true, false, 0>(nR);
+    }
+    if (per) return epi ? pick_kernel<false, true, 1>(nR) : pick_kernel<false, true, 0>(nR);
+    return epi ? pick_kernel<false, false, 1>(nR) : pick_kernel<false, false, 0>(nR);
+}
+
+size_t sweep_smem(int N, int nR) { return (size_t)(N + nR) * kPad * sizeof(double); }
+constexpr size_t kMaxSmem = 227 * 1024;
+constexpr int kMaxNR = 11;  // widest band the shared-tile solver is instantiated for
+
+// Allow every line-solve instantiation the full shared-memory budget once per context,
+// outside any stream capture.
+int set_sweep_attributes()
+{
+    for (int xd = 0; xd < 2; xd++)
+        for (int per = 0; per < 2; per++)
+            for (int epi = 0; epi < 2; epi++)
+                for (int nR = 2; nR <= kMaxNR; nR++) {
+                    void *k = sweep_kernel(xd != 0, per != 0, epi, nR);
+                    CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+                }
+    return GATT_OK;
+}
+
+// Run one compact solve (direction d, coefficient kind) over nf fields.
+// in/out are set bases with per-member strides; slots index fields inside a set.
+// blend_dt: device dt for the filter blend (NULL = use `blend`).
+int sweep(gatt_ctx *c, int d, int kind, const double *in, long long in_bs, const int *in_slots,
+          double *out, long long out_bs, const int *out_slots, int nf, int nmembers, double blend,
+          const double *blend_dt, int cls = PC_OTHER)
+{
+    const DevDir &m = c->mat[d][kind];
+    if (!m.set || !c->lt_set[d]) return fail(GATT_ERR_STATE, "matrices not set for this direction");
+    if (c->lt_max[d] >= m.nTypes) return fail(GATT_ERR_STATE, "line types exceed this matrix set's nTypes");
+    if (nf > 16) return fail(GATT_ERR_BADARG, "too many fields in one sweep");
+    SweepArgs a;
+    memset(&a, 0, sizeof(a));
+    a.in = in; a.out = out; a.in_bstride = in_bs; a.out_bstride = out_bs; a.npts = c->npts;
+    for (int f = 0; f < nf; f++) { a.in_slot[f] = in_slots[f]; a.out_slot[f] = out_slots[f]; }
+    a.nx = c->nx; a.ny = c->ny; a.nz = c->nz;
+    a.N = m.N; a.nlines = nlines(c, d);
+    a.es = d == 1 ? c->nx : (long long)c->nx * c->ny;
+    a.os = d == 1 ? (long long)c->nx * c->ny : c->nx;
+    a.tiles_per_row = (c->nx + kTileLines - 1) / kTileLines;
+    a.R = m.R; a.A = m.A; a.B = m.B; a.C = m.C; a.D = m.D; a.W = m.W;
+    a.ltype = c->ltype[d];
+    a.blend = blend; a.blend_dt = blend_dt; a.blend_fct = c->fct;
+    const int epi = (blend_dt != nullptr || blend > 0) ? EPI_BLEND : EPI_STORE;
+    const size_t smem = sweep_smem(m.N, m.nR);
+    void *k = sweep_kernel(d == 0, m.periodic != 0, epi, m.nR);
+    if (k && smem <= kMaxSmem && m.N >= 2) {
+        dim3 grid(d == 0 ? (a.nlines + kTileLines - 1) / kTileLines
+                         : a.tiles_per_row * (d == 1 ? c->nz : c->ny),
+                  nf, nmembers);
+        void *args[] = {&a};
+        TRY(before_launch(c, cls));
+        CU(cudaLaunchKernel(k, grid, dim3(32), args, smem, c->stream));
+        return after_launch(c);
+    }
+    // long lines: global-memory variant, out of place through the scratch field
+    for (int b = 0; b < nmembers; b++) {
+        for (int f = 0; f < nf; f++) {
+            SweepArgs g = a;
+            g.in = in + b * in_bs; g.in_bstride = 0; g.in_slot[0] = in_slots[f];
+            g.out = c->tmp; g.out_bstride = 0; g.out_slot[0] = 0;
+            g.es = d == 0 ? 1 : a.es;
+            dim3 grid((a.nlines + 127) / 128, 1, 1);
+            TRY(before_launch(c, cls));
+            if (m.periodic) k_sweep_global<true><<<grid, 128, 0, c->stream>>>(g, m.nR);
+            else k_sweep_global<false><<<grid, 128, 0, c->stream>>>(g, m.nR);
+            TRY(after_launch(c));
+            TRY(before_launch(c, cls));
+            k_copy<<<grid_for(c, c->npts), kBlock, 0, c->stream>>>(out + b * out_bs + (long long)out_slots[f] * c->npts,
+                                                                  c->tmp, c->npts);
+            TRY(after_launch(c));
+        }
+    }
+    return GATT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// right-hand side + stage update
+// ---------------------------------------------------------------------------
+
+// nseq2d/nseq3d on stage input q, fused with the RK4 update into out (mode).
+int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet &out, int mode, int nmem,
+              double *d1, double *tq, double *d2, double *delta)
+{
+    const long long n = c->npts;
+    const double *qin = q.v[0];
+    const long long qbs = q.bstride;
+    const StepParams *sp = c->d_params;
+    if (c->is3d) {
+        const long long bd1 = D3_N * n, btq = T3_N * n, bd2 = S3_N * n;
+        // first derivatives of U, V, W, R, E (nseq.F90:178-216)
+        const int fin[5] = {0, 1, 2, 3, 4};
+        const int ox[5] = {D3_UX, D3_VX, D3_WX, D3_RX, D3_EX};
+        const int oy[5] = {D3_UY, D3_VY, D3_WY, D3_RY, D3_EY};
+        const int oz[5] = {D3_UZ, D3_VZ, D3_WZ, D3_RZ, D3_EZ};
+        TRY(sweep(c, 0, 0, qin, qbs, fin, d1, bd1, ox, 5, nmem, 0, nullptr, PC_D1X));
+        TRY(sweep(c, 1, 0, qin, qbs, fin, d1, bd1, oy, 5, nmem, 0, nullptr, PC_D1Y));
+        TRY(sweep(c, 2, 0, qin, qbs, fin, d1, bd1, oz, 5, nmem, 0, nullptr, PC_D1Z));
+        TRY(before_launch(c, PC_VISC));
+        k_visc3d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(c->ph, q, fset(c, d1, D3_N), fset(c, tq, T3_N), n);
+        TRY(after_launch(c));
+        // second sweeps (nseq.F90:241-306)
+        const int ix[4] = {T3_XX, T3_XY, T3_XZ, T3_QX}, sx[4] = {S3_TXXX, S3_TXYX, S3_TXZX, S3_HTX};
+        const int iy[4] = {T3_XY, T3_YY, T3_YZ, T3_QY}, sy[4] = {S3_TXYY, S3_TYYY, S3_TYZY, S3_HTY};
+        const int iz[4] = {T3_XZ, T3_YZ, T3_ZZ, T3_QZ}, sz[4] = {S3_TXZZ, S3_TYZZ, S3_TZZZ, S3_HTZ};
+        TRY(sweep(c, 0, 0, tq, btq, ix, d2, bd2, sx, 4, nmem, 0, nullptr, PC_D2X));
+        TRY(sweep(c, 1, 0, tq, btq, iy, d2, bd2, sy, 4, nmem, 0, nullptr, PC_D2Y));
+        TRY(sweep(c, 2, 0, tq, btq, iz, d2, bd2, sz, 4, nmem, 0, nullptr, PC_D2Z));
+        TRY(before_launch(c, PC_ASSEMBLE));
+        k_assemble3d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(
+            c->ph, q, q0, out, fset(c, delta, 5), fset(c, d1, D3_N), fset(c, tq, T3_N), fset(c, d2, S3_N), n, mode, sp);
+        return after_launch(c);
+    }
+    const long long bd1 = D2_N * n, btq = T2_N * n, bd2 = S2_N * n;
+    const int fin[4] = {0, 1, 3, 4};
+    const int ox[4] = {D2_UX, D2_VX, D2_RX, D2_EX};
+    const int oy[4] = {D2_UY, D2_VY, D2_RY, D2_EY};
+    TRY(sweep(c, 0, 0, qin, qbs, fin, d1, bd1, ox, 4, nmem, 0, nullptr, PC_D1X));
+    TRY(sweep(c, 1, 0, qin, qbs, fin, d1, bd1, oy, 4, nmem, 0, nullptr, PC_D1Y));
+    TRY(before_launch(c, PC_VISC));
+    k_visc2d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(c->ph, q, fset(c, d1, D2_N), fset(c, tq, T2_N), n);
+    TRY(after_launch(c));
+    const int ix[3] = {T2_XY, T2_XX, T2_QX}, sx[3] = {S2_TXYX, S2_TXXX, S2_HTX};
+    const int iy[3] = {T2_XY, T2_YY, T2_QY}, sy[3] = {S2_TXYY, S2_TYYY, S2_HTY};
+    TRY(sweep(c, 0, 0, tq, btq, ix, d2, bd2, sx, 3, nmem, 0, nullptr, PC_D2X));
+    TRY(sweep(c, 1, 0, tq, btq, iy, d2, bd2, sy, 3, nmem, 0, nullptr, PC_D2Y));
+    TRY(before_launch(c, PC_ASSEMBLE));
+    k_assemble2d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(
+        c->ph, q, q0, out, fset(c, delta, 5), fset(c, d1, D2_N), fset(c, tq, T2_N), fset(c, d2, S2_N), n, mode, sp);
+    return after_launch(c);
+}
+
+// ---------------------------------------------------------------------------
+// boundary program
+// ---------------------------------------------------------------------------
+
+int check_box(const gatt_ctx *c, const int *b)
+{
+    if (b[0] < 1 || b[1] > c->nx || b[0] > b[1] || b[2] < 1 || b[3] > c->ny || b[2] > b[3] || b[4] < 1 ||
+        b[5] > c->nz || b[4] > b[5])
+        return fail(GATT_ERR_BADARG, "boundary box outside the grid: [" + std::to_string(b[0]) + " " +
+                                         std::to_string(b[1]) + " " + std::to_string(b[2]) + " " +
+                                         std::to_string(b[3]) + " " + std::to_string(b[4]) + " " +
+                                         std::to_string(b[5]) + "]");
+    return GATT_OK;
+}
+
+// getNeumannIndices (nseq.F90:520-550)
+void neumann_box(const int *in, int dir, int len, int *out)
+{
+    for (int q = 0; q < 6; q++) out[q] = in[q];
+    switch (dir) {
+    case 1: out[1] += len; break;
+    case 2: out[0] -= len; break;
+    case 3: out[3] += len; break;
+    case 4: out[2] -= len; break;
+    case 5: out[5] += len; break;
+    case 6: out[4] -= len; break;
+    }
+}
+
+int build_bc_program(gatt_ctx *c)
+{
+    std::vector<BcOp> ops;
+    auto mk = [&](int code, int var, const int *box) {
+        BcOp o;
+        memset(&o, 0, sizeof(o));
+        o.code = code; o.var = var;
+        for (int q = 0; q < 6; q++) o.box[q] = box[q];
+        return o;
+    };
+    auto row = [&](const HostBC &h, int i, int *box) {
+        for (int q = 0; q < 6; q++) box[q] = h.ind[i + (size_t)h.n * q];
+    };
+    const int NL = (int)c->coef1.size(), N2 = (int)c->coef2.size();
+    const int order[4] = {GATT_VAR_U, GATT_VAR_V, GATT_VAR_W, GATT_VAR_E};
+    int box[6], ext[6];
+    // Dirichlet (nseq.F90:357-373)
+    for (int v : order) {
+        const HostBC &h = c->bc[GATT_BC_DIRICHLET][v];
+        for (int i = 0; i < h.n; i++) {
+            row(h, i, box); TRY(check_box(c, box));
+            BcOp o = mk(OP_SET, v, box); o.val = h.val[i]; ops.push_back(o);
+        }
+    }
+    {
+        const HostBC &h = c->bc[GATT_BC_DIRICHLET][GATT_VAR_R];
+        for (int i = 0; i < h.n; i++) {
+            row(h, i, box); TRY(check_box(c, box));
+            BcOp o = mk(OP_DIR_P, GATT_VAR_R, box); o.val = h.val[i]; ops.push_back(o);
+        }
+    }
+    // Neumann (kind 1, nseq.F90:377-400) and null second derivative (kind 2, :491-513)
+    auto neumann_lists = [&](int kind, int len, int coefsel) -> int {
+        if (len < 1 && (c->bc[kind][0].n || c->bc[kind][1].n || c->bc[kind][2].n || c->bc[kind][3].n ||
+                        c->bc[kind][4].n))
+            return fail(GATT_ERR_STATE, "Neumann coefficients not set");
+        for (int v : order) {
+            const HostBC &h = c->bc[kind][v];
+            for (int i = 0; i < h.n; i++) {
+                row(h, i, box);
+                const int d = h.dirs[i];
+                if (d < 1 || d > 6) return fail(GATT_ERR_BADARG, "Neumann direction must be 1..6");
+                neumann_box(box, d, len, ext); TRY(check_box(c, ext));
+                BcOp o = mk(OP_NEU, v, ext); o.dir = d; o.len = len; o.coef = coefsel; ops.push_back(o);
+            }
+        }
+        const HostBC &h = c->bc[kind][GATT_VAR_R];
+        for (int i = 0; i < h.n; i++) {
+            row(h, i, box);
+            const int d = h.dirs[i];
+            if (d < 1 || d > 6) return fail(GATT_ERR_BADARG, "Neumann direction must be 1..6");
+            neumann_box(box, d, len, ext); TRY(check_box(c, ext)); TRY(check_box(c, box));
+            ops.push_back(mk(OP_P_LOAD, 3, ext));
+            BcOp o = mk(OP_P_NEU, 3, ext); o.dir = d; o.len = len; o.coef = coefsel; ops.push_back(o);
+            ops.push_back(mk(OP_R_FROM_P, 3, box));
+        }
+        return GATT_OK;
+    };
+    TRY(neumann_lists(GATT_BC_NEUMANN, NL, 0));
+    // corners (nseq.F90:402-488)
+    for (int i = 0; i < c->cN; i++) {
+        for (int q = 0; q < 6; q++) box[q] = c->cL[i + (size_t)c->cN * q];
+        TRY(check_box(c, box));
+        int cd[3] = {c->cD[i], c->cD[i + c->cN], c->cD[i + 2 * c->cN]};
+        const int nd = std::abs(cd[0]) + std::abs(cd[1]) + std::abs(cd[2]);
+        if (nd == 0) return fail(GATT_ERR_BADARG, "corner without direction");
+        if (NL < 1) return fail(GATT_ERR_STATE, "Neumann coefficients not set");
+        if (c->cAd[i] == 1) {
+            ops.push_back(mk(OP_CORNER_E0, 4, box));
+            for (int a = 0; a < 3; a++) {
+                if (cd[a] != 1 && cd[a] != -1) continue;
+                const int d = cd[a] == 1 ? 2 * a + 1 : 2 * a + 2;
+                neumann_box(box, d, NL, ext); TRY(check_box(c, ext));
+                ops.push_back(mk(OP_P_FROM_E, 4, ext));
+                BcOp o = mk(OP_P_NEU, 4, ext); o.dir = d; o.len = NL; o.coef = 0; ops.push_back(o);
+                ops.push_back(mk(OP_E_ADD_P, 4, box));
+            }
+            BcOp o = mk(OP_E_DIV, 4, box); o.aux = nd; ops.push_back(o);
+        }
+        ops.push_back(mk(OP_R0, 3, box));
+        for (int a = 0; a < 3; a++) {
+            if (cd[a] != 1 && cd[a] != -1) continue;
+            const int d = cd[a] == 1 ? 2 * a + 1 : 2 * a + 2;
+            neumann_box(box, d, NL, ext); TRY(check_box(c, ext));
+            ops.push_back(mk(OP_P_LOAD, 3, ext));
+            BcOp o = mk(OP_P_NEU, 3, ext); o.dir = d; o.len = NL; o.coef = 0; ops.push_back(o);
+            ops.push_back(mk(OP_R_ADD_P, 3, box));
+        }
+        BcOp o = mk(OP_R_DIV_E, 3, box); o.aux = nd; ops.push_back(o);
+    }
+    TRY(neumann_lists(GATT_BC_SECOND, N2, 1));
+    // disturbances (runDisturbances.F90)
+    for (const Dist &d : c->dists) {
+        TRY(check_box(c, d.ind));
+        BcOp o = mk(OP_LID, d.var, d.ind); o.xoff = d.xoff; o.val = d.par; ops.push_back(o);
+    }
+    cudaFree(c->d_ops); c->d_ops = nullptr;
+    cudaFree(c->d_coef1); c->d_coef1 = nullptr;
+    cudaFree(c->d_coef2); c->d_coef2 = nullptr;
+    cudaFree(c->d_xs); c->d_xs = nullptr;
+    c->nops = (int)ops.size();
+    if (!ops.empty()) {
+        CU(cudaMalloc(&c->d_ops, ops.size() * sizeof(BcOp)));
+        CU(cudaMemcpy(c->d_ops, ops.data(), ops.size() * sizeof(BcOp), cudaMemcpyHostToDevice));
+    }
+    if (!c->coef1.empty()) {
+        CU(cudaMalloc(&c->d_coef1, c->coef1.size() * sizeof(double)));
+        CU(cudaMemcpy(c->d_coef1, c->coef1.data(), c->coef1.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    if (!c->coef2.empty()) {
+        CU(cudaMalloc(&c->d_coef2, c->coef2.size() * sizeof(double)));
+        CU(cudaMemcpy(c->d_coef2, c->coef2.data(), c->coef2.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    if (!c->distx.empty()) {
+        CU(cudaMalloc(&c->d_xs, c->distx.size() * sizeof(double)));
+        CU(cudaMemcpy(c->d_xs, c->distx.data(), c->distx.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    c->bc_dirty = false;
+    return GATT_OK;
+}
+
+void invalidate_graphs(gatt_ctx *c)
+{
+    if (c->stream && (c->graph[0] || c->graph[1])) cudaStreamSynchronize(c->stream);
+    for (int i = 0; i < 2; i++) {
+        if (c->graph[i]) cudaGraphExecDestroy(c->graph[i]);
+        c->graph[i] = nullptr;
+    }
+}
+
+int apply_bc(gatt_ctx *c, const StateSet &q, int nmem)
+{
+    if (c->bc_dirty) TRY(build_bc_program(c));
+    if (c->nops == 0) return GATT_OK;
+    BcProgram pg;
+    pg.ops = c->d_ops; pg.nops = c->nops; pg.coef1 = c->d_coef1; pg.coef2 = c->d_coef2; pg.xs = c->d_xs;
+    pg.gamma = c->ph.gamma; pg.nx = c->nx; pg.ny = c->ny; pg.nz = c->nz;
+    TRY(before_launch(c, PC_BC));
+    k_bc<<<nmem, 512, 0, c->stream>>>(pg, q, c->P, c->npts);
+    return after_launch(c);
+}
+
+// applyFilters2D/3D in place on set q (derivs.F90:303-552)
+int filter_set(gatt_ctx *c, const StateSet &q, int nmem, double blend, const double *blend_dt)
+{
+    const int f3[5] = {0, 1, 2, 3, 4}, f2[4] = {0, 1, 3, 4};
+    const int *fl = c->is3d ? f3 : f2;
+    const int nf = c->is3d ? 5 : 4;
+    const int ndir = c->is3d ? 3 : 2;
+    for (int d = 0; d < ndir; d++) {
+        if (!c->filt[d]) continue;
+        TRY(sweep(c, d, 1, q.v[0], q.bstride, fl, q.v[0], q.bstride, fl, nf, nmem, blend, blend_dt, PC_FX + d));
+    }
+    return GATT_OK;
+}
+
+int check_ready(const gatt_ctx *c, bool need_filter)
+{
+    if (!c->phys_set) return fail(GATT_ERR_STATE, "gatt_set_physics not called");
+    const int ndir = c->is3d ? 3 : 2;
+    for (int d = 0; d < ndir; d++) {
+        if (!c->mat[d][0].set || !c->lt_set[d]) return fail(GATT_ERR_STATE, "derivative matrices missing for a direction");
+        if (c->lt_max[d] >= c->mat[d][0].nTypes) return fail(GATT_ERR_STATE, "block types exceed the derivative nTypes");
+        if (need_filter && c->filt[d] && !c->mat[d][1].set)
+            return fail(GATT_ERR_STATE, "filter matrices missing for a filtered direction");
+        if (need_filter && c->filt[d] && c->lt_max[d] >= c->mat[d][1].nTypes)
+            return fail(GATT_ERR_STATE, "block types exceed the filter nTypes");
+    }
+    return GATT_OK;
+}
+
+// The whole of main.F90:255-420 for all members, enqueued on the stream.
+int step_body(gatt_ctx *c)
+{
+    const StateSet q0 = state_set(c, 0), qs = state_set(c, 1);
+    StateSet qst = qs;  // stage BC set: in 2-D RK4_2D hands the caller's W to applyBoundCond
+    if (!c->is3d) qst.v[2] = q0.v[2];
+    const int nm = c->nb;
+    CU(cudaMemsetAsync(c->acc, 0, sizeof(unsigned long long) * 5 * nm, c->stream));
+    for (int s = 1; s <= 4; s++) {
+        TRY(rhs_stage(c, s == 1 ? q0 : qs, q0, qs, s, nm, c->d1, c->tq, c->d2, c->delta));
+        TRY(apply_bc(c, qst, nm));
+    }
+    if (c->fct > 0) TRY(filter_set(c, qs, nm, 0.0, &c->d_params->dt));
+    else TRY(filter_set(c, qs, nm, 0.0, nullptr));
+    if (c->sfd_type > 0) {
+        TRY(before_launch(c, PC_SFD));
+        k_sfd<<<dim3(grid_for(c, c->npts), nm), kBlock, 0, c->stream>>>(qs, fset(c, c->mean, 5), c->chi, c->sfd_delta,
+                                                                          c->is3d ? 5 : 4, c->npts, c->d_params);
+        TRY(after_launch(c));
+    }
+    TRY(apply_bc(c, qs, nm));
+    TRY(before_launch(c, PC_MAXCHANGE));
+    k_maxchange<<<dim3(grid_for(c, c->npts), nm), kBlock, 0, c->stream>>>(qs, q0, c->acc, c->npts);
+    TRY(after_launch(c));
+    TRY(before_launch(c, PC_MAXCHANGE));
+    k_store_maxchange<<<1, 5 * nm < 1024 ? 5 * nm : 1024, 0, c->stream>>>(c->acc, c->hist, 5 * nm, c->d_params);
+    return after_launch(c);
+}
+
+int ensure_graph(gatt_ctx *c)
+{
+    const int g = c->cur;
+    if (c->graph[g]) return GATT_OK;
+    if (c->bc_dirty) TRY(build_bc_program(c));
+    cudaGraph_t graph;
+    c->capturing = true;
+    c->capture_count = 0;
+    CU(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = step_body(c);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    c->capturing = false;
+    if (rc != GATT_OK) { if (e == cudaSuccess) cudaGraphDestroy(graph); return rc; }
+    CU(e);
+    cudaError_t ei = cudaGraphInstantiate(&c->graph[g], graph, 0);
+    cudaGraphDestroy(graph);
+    CU(ei);
+    c->graph_kernels[g] = c->capture_count;
+    return GATT_OK;
+}
+
+int ensure_hist(gatt_ctx *c, int n)
+{
+    if (n <= c->hist_cap) return GATT_OK;
+    int cap = c->hist_cap ? c->hist_cap : 64;
+    while (cap < n) cap *= 2;
+    CU(cudaStreamSynchronize(c->stream));
+    cudaFree(c->hist);
+    cudaFreeHost(c->h_params);
+    c->hist = nullptr; c->h_params = nullptr;
+    CU(cudaMalloc(&c->hist, sizeof(double) * 5 * c->nb * (size_t)cap));
+    CU(cudaMallocHost(&c->h_params, sizeof(StepParams) * (size_t)cap));
+    c->hist_cap = cap;
+    invalidate_graphs(c);  // graphs hold the history pointer
+    return GATT_OK;
+}
+
+int run_steps(gatt_ctx *c, int nsteps, double t0, double dt, double *maxChange, bool check_each)
+{
+    TRY(check_ready(c, true));
+    if (nsteps < 1) return fail(GATT_ERR_BADARG, "nsteps < 1");
+    if (!(dt > 0) || !std::isfinite(dt)) return fail(GATT_ERR_BADARG, "dt must be positive and finite");
+    if (c->sfd_type > 0 && !c->chi) return fail(GATT_ERR_STATE, "SFD field not set");
+    TRY(ensure_hist(c, nsteps));
+    if (c->sfd_type > 0 && !c->mean_init) {
+        // Umean = U when no mean flow was given (main.F90:158-163)
+        const StateSet q = state_set(c, 0);
+        for (int b = 0; b < c->nb; b++)
+            for (int f = 0; f < 5; f++)
+                CU(cudaMemcpyAsync(c->mean + ((size_t)b * 5 + f) * c->npts, q.v[f] + b * q.bstride,
+                                   sizeof(double) * c->npts, cudaMemcpyDeviceToDevice, c->stream));
+        c->mean_init = true;
+    }
+    double t = t0;
+    for (int s = 0; s < nsteps; s++) {
+        c->h_params[s].t = t; c->h_params[s].dt = dt; c->h_params[s].slot = s;
+        TRY(ensure_graph(c));
+        CU(cudaMemcpyAsync(c->d_params, &c->h_params[s], sizeof(StepParams), cudaMemcpyHostToDevice, c->stream));
+        CU(cudaGraphLaunch(c->graph[c->cur], c->stream));
+        c->launches += c->graph_kernels[c->cur];
+        c->cur ^= 1;
+        t = t + dt;  // main.F90:423
+    }
+    const int nv = 5 * c->nb;
+    std::vector<double> h((size_t)nv * nsteps);
+    CU(cudaMemcpyAsync(h.data(), c->hist, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    if (maxChange) memcpy(maxChange, h.data() + (size_t)nv * (nsteps - 1), sizeof(double) * nv);
+    // divergence test of main.F90:433-438, per member and step
+    for (int s = check_each ? 0 : nsteps - 1; s < nsteps; s++)
+        for (int b = 0; b < c->nb; b++) {
+            const double *m = h.data() + (size_t)nv * s + 5 * b;
+            double sum = 0;
+            bool nan = false;
+            for (int f = 0; f < 5; f++) { nan |= std::isnan(m[f]); sum += m[f]; }
+            if (nan || sum == 0)
+                return fail(GATT_ERR_DIVERGED, "flow diverged (member " + std::to_string(b) + ", step " +
+                                                   std::to_string(s) + ")");
+        }
+    return GATT_OK;
+}
+
+int alloc_fields(gatt_ctx *c, double **p, int nslots, int members)
+{
+    CU(cudaMalloc(p, sizeof(double) * (size_t)c->npts * nslots * members));
+    CU(cudaMemsetAsync(*p, 0, sizeof(double) * (size_t)c->npts * nslots * members, c->stream));
+    return GATT_OK;
+}
+
+int ensure_host_scratch(gatt_ctx *c)
+{
+    if (!c->tin) TRY(alloc_fields(c, &c->tin, 5, 1));
+    if (!c->tout) TRY(alloc_fields(c, &c->tout, 5, 1));
+    return GATT_OK;
+}
+
+int check_member(const gatt_ctx *c, int b)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    if (b < 0 || b >= c->nb) return fail(GATT_ERR_BADARG, "batch member out of range");
+    return GATT_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+
+extern "C" {
+
+const char *gatt_strerror(int code)
+{
+    switch (code) {
+    case GATT_OK: return "ok";
+    case GATT_ERR_CUDA: return "CUDA error";
+    case GATT_ERR_BADARG: return "invalid argument";
+    case GATT_ERR_BADCOEF: return "invalid coefficient (non-finite value or zero pivot)";
+    case GATT_ERR_DIVERGED: return "flow diverged";
+    case GATT_ERR_TIMEOUT: return "device wait timed out";
+    case GATT_ERR_STATE: return "call out of order";
+    case GATT_ERR_NOMEM: return "out of device memory";
+    default: return "unknown error";
+    }
+}
+
+const char *gatt_last_error(void) { return g_err.c_str(); }
+
+int gatt_create(gatt_ctx **out, int nx, int ny, int nz, int nbatch)
+{
+    if (!out) return fail(GATT_ERR_BADARG, "null output pointer");
+    *out = nullptr;
+    if (nx < 2 || ny < 2 || nz < 1 || nbatch < 1) return fail(GATT_ERR_BADARG, "grid must be at least 2x2x1, nbatch >= 1");
+    if ((long long)nx * ny * nz > (1LL << 31)) return fail(GATT_ERR_BADARG, "grid too large");
+    if (nbatch > 65535) return fail(GATT_ERR_BADARG, "nbatch too large");
+    gatt_ctx *c = new gatt_ctx();
+    c->nx = nx; c->ny = ny; c->nz = nz; c->nb = nbatch;
+    c->npts = (long long)nx * ny * nz;
+    c->is3d = nz > 1;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);
+    int rc = GATT_OK;
+    auto chk = [&](int r) { if (rc == GATT_OK) rc = r; };
+    if (e != cudaSuccess) rc = fail(GATT_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    if (rc == GATT_OK) {
+        cudaError_t es = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (es != cudaSuccess) rc = fail(GATT_ERR_CUDA, cudaGetErrorString(es));
+        else c->own_stream = true;
+    }
+    if (rc == GATT_OK) {
+        chk(alloc_fields(c, &c->qA, 5, nbatch));
+        chk(alloc_fields(c, &c->qB, 5, nbatch));
+        chk(alloc_fields(c, &c->delta, 5, nbatch));
+        chk(alloc_fields(c, &c->d1, nd1(c), nbatch));
+        chk(alloc_fields(c, &c->tq, ntq(c), nbatch));
+        chk(alloc_fields(c, &c->d2, nd2(c), nbatch));
+        chk(alloc_fields(c, &c->P, 1, nbatch));
+        chk(alloc_fields(c, &c->tmp, 1, 1));
+    }
+    if (rc == GATT_OK) {
+        cudaError_t ea = cudaMalloc(&c->acc, sizeof(unsigned long long) * 5 * nbatch);
+        if (ea == cudaSuccess) ea = cudaMalloc(&c->d_params, sizeof(StepParams));
+        if (ea == cudaSuccess) ea = cudaMemsetAsync(c->d_params, 0, sizeof(StepParams), c->stream);
+        if (ea != cudaSuccess) rc = fail(GATT_ERR_NOMEM, cudaGetErrorString(ea));
+    }
+    if (rc == GATT_OK) chk(set_sweep_attributes());
+    if (rc == GATT_OK) chk(ensure_hist(c, 64));
+    if (rc == GATT_OK) {
+        cudaError_t es = cudaStreamSynchronize(c->stream);
+        if (es != cudaSuccess) rc = fail(GATT_ERR_CUDA, cudaGetErrorString(es));
+    }
+    if (rc != GATT_OK) { gatt_destroy(c); return rc; }
+    *out = c;
+    return GATT_OK;
+}
+
+void gatt_destroy(gatt_ctx *c)
+{
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    invalidate_graphs(c);
+    for (int d = 0; d < 3; d++) {
+        for (int k = 0; k < 2; k++) {
+            DevDir &m = c->mat[d][k];
+            cudaFree(m.R); cudaFree(m.A); cudaFree(m.B); cudaFree(m.C); cudaFree(m.D);
+        }
+        cudaFree(c->ltype[d]);
+    }
+    double *bufs[] = {c->qA, c->qB, c->delta, c->mean, c->d1, c->tq, c->d2, c->P, c->tmp, c->tin, c->tout, c->chi, c->hist,
+                      c->d_coef1, c->d_coef2, c->d_xs};
+    for (double *p : bufs) cudaFree(p);
+    cudaFree(c->d_ops); cudaFree(c->acc); cudaFree(c->d_params);
+    if (c->h_params) cudaFreeHost(c->h_params);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int gatt_set_stream(gatt_ctx *c, void *s)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    CU(cudaStreamSynchronize(c->stream));
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    c->own_stream = false;
+    c->stream = (cudaStream_t)s;
+    if (!s) {
+        CU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    invalidate_graphs(c);
+    return GATT_OK;
+}
+
+int gatt_set_physics(gatt_ctx *c, double Re, double Ma, double Pr, double gamma, double T0)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    const double v[5] = {Re, Ma, Pr, gamma, T0};
+    for (double x : v)
+        if (!std::isfinite(x) || x <= 0) return fail(GATT_ERR_BADARG, "physical parameters must be positive and finite");
+    if (gamma <= 1) return fail(GATT_ERR_BADARG, "gamma must exceed 1");
+    c->ph.Re = Re; c->ph.Ma = Ma; c->ph.Pr = Pr; c->ph.gamma = gamma; c->ph.T0 = T0;
+    c->phys_set = true;
+    invalidate_graphs(c);
+    return GATT_OK;
+}
+
+int gatt_set_matrices(gatt_ctx *c, int dir, int kind, int periodic, int nRHS, int nTypes, const double *A,
+                      const double *B, const double *C, const double *D, const double *R, int nBlocks,
+                      const int *blocks)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    if (dir < 1 || dir > 3 || kind < 0 || kind > 1) return fail(GATT_ERR_BADARG, "dir must be 1..3 and kind 0..1");
+    const int d = dir - 1;
+    const int N = line_len(c, d);
+    if (periodic != 0 && periodic != 1) return fail(GATT_ERR_BADARG, "periodic must be 0 or 1");
+    if (nTypes < 1 || nTypes > 255) return fail(GATT_ERR_BADARG, "nTypes must be 1..255");
+    // the band wraps around a line at most once (derivs.F90:583-602 index F(i +- l), l < nRHS)
+    if (nRHS < 1 || nRHS > N) return fail(GATT_ERR_BADARG, "nRHS out of range (1..N)");
+    if (N < 2) return fail(GATT_ERR_BADARG, "direction has a single node; it has no matrices");
+    if (!A || !B || !C || !R || (periodic && !D)) return fail(GATT_ERR_BADARG, "missing coefficient array");
+    if (nBlocks < 0 || (nBlocks > 0 && !blocks)) return fail(GATT_ERR_BADARG, "bad block list");
+    if (nBlocks == 0 && !c->lt_set[d]) return fail(GATT_ERR_BADARG, "no blocks given and none set for this direction");
+    const int W = 2 * nRHS - 1;
+    const int nA = N - 1, nB = N - periodic;
+    // repack to [type][row] (and [type][row][diag] for R), checking every value
+    std::vector<double> hA((size_t)nTypes * N, 0.0), hB((size_t)nTypes * N, 0.0), hC((size_t)nTypes * N, 0.0),
+        hD((size_t)nTypes * N, 0.0), hR((size_t)nTypes * N * W, 0.0);
+    for (int t = 0; t < nTypes; t++) {
+        for (int i = 0; i < nA; i++) {
+            hA[(size_t)t * N + i] = A[i + (size_t)nA * t];
+            hC[(size_t)t * N + i] = C[i + (size_t)nA * t];
+        }
+        for (int i = 0; i < nB; i++) hB[(size_t)t * N + i] = B[i + (size_t)nB * t];
+        if (periodic)
+            for (int i = 0; i < N; i++) hD[(size_t)t * N + i] = D[i + (size_t)N * t];
+        for (int i = 0; i < N; i++)
+            for (int q = 0; q < W; q++) hR[((size_t)t * N + i) * W + q] = R[i + (size_t)N * q + (size_t)N * W * t];
+    }
+    for (const std::vector<double> *v : {&hA, &hB, &hC, &hD, &hR})
+        for (double x : *v)
+            if (!std::isfinite(x)) return fail(GATT_ERR_BADCOEF, "non-finite coefficient (a zero pivot gives an infinite B)");
+    for (int t = 0; t < nTypes; t++)
+        for (int i = 0; i < nB; i++)
+            if (hB[(size_t)t * N + i] == 0.0) return fail(GATT_ERR_BADCOEF, "zero reciprocal pivot in B");
+    // type map from the blocks (derivs.F90:572-580: blocks(bn,1..5) = t, a1, a2, b1, b2)
+    std::vector<uint8_t> lt;
+    if (nBlocks > 0) {
+        const int na = d == 0 ? c->ny : c->nx;
+        const int nbd = d == 2 ? c->ny : c->nz;
+        lt.assign((size_t)na * nbd, 0);
+        std::vector<uint8_t> seen((size_t)na * nbd, 0);
+        for (int bn = 0; bn < nBlocks; bn++) {
+            const int t = blocks[bn], a1 = blocks[bn + nBlocks], a2 = blocks[bn + 2 * nBlocks];
+            const int b1 = blocks[bn + 3 * nBlocks], b2 = blocks[bn + 4 * nBlocks];
+            if (t < 1 || t > nTypes) return fail(GATT_ERR_BADARG, "block type out of range");
+            if (a1 < 1 || a2 > na || a1 > a2 || b1 < 1 || b2 > nbd || b1 > b2)
+                return fail(GATT_ERR_BADARG, "block line range outside the grid");
+            for (int bb = b1; bb <= b2; bb++)
+                for (int aa = a1; aa <= a2; aa++) {
+                    const size_t L = (size_t)(aa - 1) + (size_t)na * (bb - 1);
+                    if (seen[L]) return fail(GATT_ERR_BADARG, "blocks cover a line twice");
+                    seen[L] = 1;
+                    lt[L] = (uint8_t)(t - 1);
+                }
+        }
+        for (uint8_t s : seen)
+            if (!s) return fail(GATT_ERR_BADARG, "blocks leave a line uncovered");
+    } else {
+        // reuse the type map already set; its types must exist in this matrix set
+        std::vector<uint8_t> cur((size_t)nlines(c, d));
+        CU(cudaMemcpy(cur.data(), c->ltype[d], cur.size(), cudaMemcpyDeviceToHost));
+        for (uint8_t t : cur)
+            if (t >= nTypes) return fail(GATT_ERR_BADARG, "existing block types exceed nTypes");
+    }
+    CU(cudaStreamSynchronize(c->stream));
+    DevDir &m = c->mat[d][kind];
+    cudaFree(m.R); cudaFree(m.A); cudaFree(m.B); cudaFree(m.C); cudaFree(m.D);
+    m = DevDir();
+    CU(cudaMalloc(&m.R, hR.size() * sizeof(double)));
+    CU(cudaMalloc(&m.A, hA.size() * sizeof(double)));
+    CU(cudaMalloc(&m.B, hB.size() * sizeof(double)));
+    CU(cudaMalloc(&m.C, hC.size() * sizeof(double)));
+    CU(cudaMalloc(&m.D, hD.size() * sizeof(double)));
+    CU(cudaMemcpy(m.R, hR.data(), hR.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(m.A, hA.data(), hA.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(m.B, hB.data(), hB.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(m.C, hC.data(), hC.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(m.D, hD.data(), hD.size() * sizeof(double), cudaMemcpyHostToDevice));
+    m.periodic = periodic; m.nR = nRHS; m.nTypes = nTypes; m.N = N; m.W = W; m.set = true;
+    if (nBlocks > 0) {
+        if (!c->ltype[d]) CU(cudaMalloc(&c->ltype[d], lt.size()));
+        CU(cudaMemcpy(c->ltype[d], lt.data(), lt.size(), cudaMemcpyHostToDevice));
+        c->lt_set[d] = true;
+        int mx = 0;
+        for (uint8_t t : lt) mx = t > mx ? t : mx;
+        c->lt_max[d] = mx;
+    }
+    invalidate_graphs(c);
+    return GATT_OK;
+}
+
+int gatt_set_filter(gatt_ctx *c, int fx, int fy, int fz, double fct)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    if (!std::isfinite(fct) || fct == 0) return fail(GATT_ERR_BADARG, "FilterCharTime must be finite and non-zero (-1 = off)");
+    c->filt[0] = fx != 0; c->filt[1] = fy != 0; c->filt[2] = (fz != 0) && c->is3d;
+    c->fct = fct;
+    invalidate_graphs(c);
+    return GATT_OK;
+}
+
+int gatt_set_neumann(gatt_ctx *c, int n1, const double *c1, int n2, const double *c2)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    if (n1 < 0 || n2 < 0 || (n1 && !c1) || (n2 && !c2)) return fail(GATT_ERR_BADARG, "bad Neumann coefficient arrays");
+    c->coef1.assign(c1, c1 + n1);
+    c->coef2.assign(c2, c2 + n2);
+    c->bc_dirty = true;
+    invalidate_graphs(c);
+    return GATT_OK;
+}
+
+int gatt_set_bc(gatt_ctx *c, int var, int kind, int n, const int *ind, const double *val, const int *dirs)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    if (var < 0 || var > 4 || kind < 0 || kind > 2 || n < 0) return fail(GATT_ERR_BADARG, "bad var/kind/count");
+    if (n > 0 && !ind) return fail(GATT_ERR_BADARG, "missing index array");
+    if (n > 0 && kind == GATT_BC_DIRICHLET && !val) return fail(GATT_ERR_BADARG, "missing Dirichlet values");
+    if (n > 0 && kind != GATT_BC_DIRICHLET && !dirs) return fail(GATT_ERR_BADARG, "missing directions");
+    HostBC &h = c->bc[kind][var];
+    h.n = n;
+    h.ind.assign(ind, ind + (size_t)6 * n);
+    if (kind == GATT_BC_DIRICHLET) { h.val.assign(val, val + n); h.dirs.clear(); }
+    else { h.dirs.assign(dirs, dirs + n); h.val.clear(); }
+    c->bc_dirty = true;
+    invalidate_graphs(c);
+    return GATT_OK;
+}
+
+int gatt_set_corners(gatt_ctx *c, int cN, const int *cL, const int *cD, const int *cAd)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    if (cN < 0 || (cN > 0 && (!cL || !cD || !cAd))) return fail(GATT_ERR_BADARG, "bad corner arrays");
+    c->cN = cN;
+    c->cL.assign(cL, cL + (size_t)6 * cN);
+    c->cD.assign(cD, cD + (size_t)3 * cN);
+    c->cAd.assign(cAd, cAd + cN);
+    c->bc_dirty = true;
+    invalidate_graphs(c);
+    return GATT_OK;
+}
+
+int gatt_add_disturbance(gatt_ctx *c, int type, int var, const int *ind, const double *x, int npar, const double *par)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    if (type != GATT_DIST_LID_DRIVEN) return fail(GATT_ERR_BADARG, "unsupported disturbance type");
+    if (var < 0 || var > 4 || !ind || !x || npar < 1 || !par) return fail(GATT_ERR_BADARG, "bad disturbance arguments");
+    Dist d;
+    d.type = type; d.var = var;
+    for (int q = 0; q < 6; q++) d.ind[q] = ind[q];
+    if (d.ind[1] < d.ind[0]) return fail(GATT_ERR_BADARG, "empty disturbance box");
+    const int nxb = d.ind[1] - d.ind[0] + 1;
+    if (nxb > 1 && x[nxb - 1] == x[0]) return fail(GATT_ERR_BADARG, "degenerate disturbance coordinates");
+    d.xoff = (int)c->distx.size();
+    c->distx.insert(c->distx.end(), x, x + nxb);
+    d.par = par[0];
+    c->dists.push_back(d);
+    c->bc_dirty = true;
+    invalidate_graphs(c);
+    return GATT_OK;
+}
+
+int gatt_clear_disturbances(gatt_ctx *c)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    c->dists.clear();
+    c->distx.clear();
+    c->bc_dirty = true;
+    invalidate_graphs(c);
+    return GATT_OK;
+}
+
+int gatt_set_sfd(gatt_ctx *c, int type, double Delta, double chiValue, const double *chi)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    if (type < 0 || type > 2) return fail(GATT_ERR_BADARG, "SFD type must be 0, 1 or 2");
+    if (type == 2 && !chi) return fail(GATT_ERR_BADARG, "SFD type 2 needs the chi field");
+    if (!std::isfinite(Delta)) return fail(GATT_ERR_BADARG, "SFD Delta must be finite (-1 = frozen mean)");
+    c->sfd_type = type;
+    c->sfd_delta = Delta;
+    invalidate_graphs(c);
+    if (type == 0) return GATT_OK;
+    if (!c->chi) CU(cudaMalloc(&c->chi, sizeof(double) * c->npts));
+    if (type == 1) {
+        std::vector<double> h(c->npts, chiValue);
+        CU(cudaMemcpy(c->chi, h.data(), sizeof(double) * c->npts, cudaMemcpyHostToDevice));
+    } else {
+        CU(cudaMemcpy(c->chi, chi, sizeof(double) * c->npts, cudaMemcpyHostToDevice));
+    }
+    if (!c->mean) TRY(alloc_fields(c, &c->mean, 5, c->nb));
+    return GATT_OK;
+}
+
+static int copy_state(gatt_ctx *c, int b, int which, double *const *host, bool up)
+{
+    TRY(check_member(c, b));
+    const StateSet q = state_set(c, which);
+    for (int f = 0; f < 5; f++) {
+        if (!host[f]) continue;
+        double *dp = q.v[f] + b * q.bstride;
+        if (up) CU(cudaMemcpyAsync(dp, host[f], sizeof(double) * c->npts, cudaMemcpyHostToDevice, c->stream));
+        else CU(cudaMemcpyAsync(host[f], dp, sizeof(double) * c->npts, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CU(cudaStreamSynchronize(c->stream));
+    return GATT_OK;
+}
+
+int gatt_upload(gatt_ctx *c, int b, const double *U, const double *V, const double *W, const double *R, const double *E)
+{
+    double *h[5] = {(double *)U, (double *)V, (double *)W, (double *)R, (double *)E};
+    return copy_state(c, b, 0, h, true);
+}
+
+int gatt_download(gatt_ctx *c, int b, double *U, double *V, double *W, double *R, double *E)
+{
+    double *h[5] = {U, V, W, R, E};
+    return copy_state(c, b, 0, h, false);
+}
+
+static int copy_mean(gatt_ctx *c, int b, double *const *host, bool up)
+{
+    TRY(check_member(c, b));
+    if (!c->mean) TRY(alloc_fields(c, &c->mean, 5, c->nb));
+    for (int f = 0; f < 5; f++) {
+        if (!host[f]) continue;
+        double *dp = c->mean + ((size_t)b * 5 + f) * c->npts;
+        if (up) CU(cudaMemcpyAsync(dp, host[f], sizeof(double) * c->npts, cudaMemcpyHostToDevice, c->stream));
+        else CU(cudaMemcpyAsync(host[f], dp, sizeof(double) * c->npts, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CU(cudaStreamSynchronize(c->stream));
+    return GATT_OK;
+}
+
+int gatt_upload_mean(gatt_ctx *c, int b, const double *U, const double *V, const double *W, const double *R, const double *E)
+{
+    double *h[5] = {(double *)U, (double *)V, (double *)W, (double *)R, (double *)E};
+    TRY(copy_mean(c, b, h, true));
+    c->mean_init = true;
+    return GATT_OK;
+}
+
+int gatt_download_mean(gatt_ctx *c, int b, double *U, double *V, double *W, double *R, double *E)
+{
+    double *h[5] = {U, V, W, R, E};
+    return copy_mean(c, b, h, false);
+}
+
+int gatt_upload_wnew(gatt_ctx *c, int b, const double *Wn)
+{
+    TRY(check_member(c, b));
+    double *h[5] = {nullptr, nullptr, (double *)Wn, nullptr, nullptr};
+    return copy_state(c, b, 1, h, true);
+}
+
+int gatt_download_wnew(gatt_ctx *c, int b, double *Wn)
+{
+    TRY(check_member(c, b));
+    double *h[5] = {nullptr, nullptr, Wn, nullptr, nullptr};
+    return copy_state(c, b, 1, h, false);
+}
+
+int gatt_state_device_ptr(gatt_ctx *c, int b, int var, double **dptr)
+{
+    TRY(check_member(c, b));
+    if (var < 0 || var > 4 || !dptr) return fail(GATT_ERR_BADARG, "bad variable or output pointer");
+    const StateSet q = state_set(c, 0);
+    *dptr = q.v[var] + b * q.bstride;
+    return GATT_OK;
+}
+
+int gatt_apply_bc(gatt_ctx *c, double t)
+{
+    (void)t;
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    if (!c->phys_set) return fail(GATT_ERR_STATE, "gatt_set_physics not called");
+    TRY(apply_bc(c, state_set(c, 0), c->nb));
+    CU(cudaStreamSynchronize(c->stream));
+    return GATT_OK;
+}
+
+int gatt_deriv_dir(gatt_ctx *c, int dir, int kind, const double *F, double *dF)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    if (dir < 1 || dir > 3 || kind < 0 || kind > 1 || !F || !dF) return fail(GATT_ERR_BADARG, "bad arguments");
+    if (line_len(c, dir - 1) < 2) return fail(GATT_ERR_BADARG, "direction has a single node");
+    TRY(ensure_host_scratch(c));
+    CU(cudaMemcpyAsync(c->tin, F, sizeof(double) * c->npts, cudaMemcpyHostToDevice, c->stream));
+    const int s0 = 0;
+    TRY(sweep(c, dir - 1, kind, c->tin, 0, &s0, c->tout, 0, &s0, 1, 1, 0.0, nullptr));
+    CU(cudaMemcpyAsync(dF, c->tout, sizeof(double) * c->npts, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return GATT_OK;
+}
+
+int gatt_rhs(gatt_ctx *c, const double *U, const double *V, const double *W, const double *R, const double *E,
+             double *dU, double *dV, double *dW, double *dR, double *dE)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    TRY(check_ready(c, false));
+    if (!U || !V || !R || !E || !dU || !dV || !dR || !dE || (c->is3d && (!W || !dW)))
+        return fail(GATT_ERR_BADARG, "missing field");
+    TRY(ensure_host_scratch(c));
+    const double *in[5] = {U, V, W, R, E};
+    for (int f = 0; f < 5; f++) {
+        if (!in[f]) continue;
+        CU(cudaMemcpyAsync(c->tin + f * c->npts, in[f], sizeof(double) * c->npts, cudaMemcpyHostToDevice, c->stream));
+    }
+    StateSet q, o;
+    for (int f = 0; f < 5; f++) { q.v[f] = c->tin + f * c->npts; o.v[f] = c->tout + f * c->npts; }
+    q.bstride = o.bstride = 5 * c->npts;
+    TRY(rhs_stage(c, q, q, o, RK_STORE_RHS, 1, c->d1, c->tq, c->d2, nullptr));
+    double *out[5] = {dU, dV, dW, dR, dE};
+    for (int f = 0; f < 5; f++) {
+        if (!out[f] || (!c->is3d && f == 2)) continue;
+        CU(cudaMemcpyAsync(out[f], c->tout + f * c->npts, sizeof(double) * c->npts, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CU(cudaStreamSynchronize(c->stream));
+    return GATT_OK;
+}
+
+int gatt_filter(gatt_ctx *c, double blend)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    TRY(check_ready(c, true));
+    TRY(filter_set(c, state_set(c, 0), c->nb, blend > 0 ? blend : 0.0, nullptr));
+    CU(cudaStreamSynchronize(c->stream));
+    return GATT_OK;
+}
+
+int gatt_step(gatt_ctx *c, double t, double dt, double *maxChange)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    return run_steps(c, 1, t, dt, maxChange, true);
+}
+
+int gatt_run(gatt_ctx *c, int nsteps, double t0, double dt, double *maxChange)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    return run_steps(c, nsteps, t0, dt, maxChange, true);
+}
+
+int gatt_max_velocity(gatt_ctx *c, double *vmax)
+{
+    if (!c || !vmax) return fail(GATT_ERR_BADARG, "null argument");
+    CU(cudaMemsetAsync(c->acc, 0, sizeof(unsigned long long) * 3 * c->nb, c->stream));
+    TRY(before_launch(c, PC_OTHER));
+    k_maxvel<<<dim3(grid_for(c, c->npts), c->nb), kBlock, 0, c->stream>>>(state_set(c, 0), c->acc, c->npts);
+    TRY(after_launch(c));
+    std::vector<unsigned long long> h(3 * c->nb);
+    CU(cudaMemcpyAsync(h.data(), c->acc, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    for (size_t i = 0; i < h.size(); i++) memcpy(&vmax[i], &h[i], sizeof(double));
+    return GATT_OK;
+}
+
+int gatt_synchronize(gatt_ctx *c)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    CU(cudaStreamSynchronize(c->stream));
+    return GATT_OK;
+}
+
+long long gatt_kernel_launches(gatt_ctx *c) { return c ? c->launches : -1; }
+
+const char *gatt_profile_name(int cls) { return (cls >= 0 && cls < PC_N) ? kProfNames[cls] : nullptr; }
+
+int gatt_profile_kernels(gatt_ctx *c, double t0, double dt, int nsteps, double *ms, double *launches)
+{
+    if (!c || !ms || !launches || nsteps < 1) return fail(GATT_ERR_BADARG, "bad arguments");
+    TRY(check_ready(c, true));
+    TRY(ensure_hist(c, 1));
+    if (c->sfd_type > 0 && !c->mean_init) return fail(GATT_ERR_STATE, "run a step before profiling with SFD");
+    for (int i = 0; i < PC_N; i++) { ms[i] = 0; launches[i] = 0; }
+    double t = t0;
+    int rc = GATT_OK;
+    for (int s = 0; s < nsteps && rc == GATT_OK; s++) {
+        c->h_params[0].t = t; c->h_params[0].dt = dt; c->h_params[0].slot = 0;
+        CU(cudaMemcpyAsync(c->d_params, &c->h_params[0], sizeof(StepParams), cudaMemcpyHostToDevice, c->stream));
+        c->profiling = true;
+        rc = step_body(c);
+        c->profiling = false;
+        CU(cudaStreamSynchronize(c->stream));
+        size_t q = 0;
+        for (size_t i = 0; i < c->ev_cls.size(); i++, q += 2) {
+            float e = 0;
+            cudaEventElapsedTime(&e, c->ev_pool[q], c->ev_pool[q + 1]);
+            ms[c->ev_cls[i]] += e;
+            launches[c->ev_cls[i]] += 1;
+        }
+        for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+        c->ev_pool.clear();
+        c->ev_cls.clear();
+        c->cur ^= 1;
+        t = t + dt;
+    }
+    for (int i = 0; i < PC_N; i++) {
+        if (launches[i] > 0) ms[i] /= launches[i];
+        launches[i] /= nsteps;
+    }
+    return rc;
+}
+
+}  // extern "C"

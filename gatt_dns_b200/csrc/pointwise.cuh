@@ -1,0 +1,304 @@
+// Pointwise kernels of the Navier-Stokes right-hand side, the RK4 stage update, SFD
+// and the max-change residual (reference source/Fortran/nseq.F90:10-323,
+// timeIntegration.F90:8-156/338-498, main.F90:381-420).
+//
+// Field sets are [member][slot][point] arrays of FP64; every kernel is a grid-stride
+// loop over points with the batch member in blockIdx.y.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gatt {
+
+// slot numbering of the per-member scratch sets
+// 3-D first derivatives: slot 3*f + d, f in U,V,W,R,E and d in x,y,z
+enum { D3_UX = 0, D3_UY, D3_UZ, D3_VX, D3_VY, D3_VZ, D3_WX, D3_WY, D3_WZ,
+       D3_RX, D3_RY, D3_RZ, D3_EX, D3_EY, D3_EZ, D3_N };
+// 3-D stresses and heat fluxes
+enum { T3_XX = 0, T3_YY, T3_ZZ, T3_XY, T3_XZ, T3_YZ, T3_QX, T3_QY, T3_QZ, T3_N };
+// 3-D second-sweep results
+enum { S3_TXYX = 0, S3_TXYY, S3_TXZX, S3_TXZZ, S3_TYZY, S3_TYZZ, S3_TXXX, S3_TYYY, S3_TZZZ,
+       S3_HTX, S3_HTY, S3_HTZ, S3_N };
+// 2-D first derivatives: slot 2*f + d, f in U,V,R,E
+enum { D2_UX = 0, D2_UY, D2_VX, D2_VY, D2_RX, D2_RY, D2_EX, D2_EY, D2_N };
+enum { T2_XX = 0, T2_YY, T2_XY, T2_QX, T2_QY, T2_N };
+enum { S2_TXYX = 0, S2_TXYY, S2_TXXX, S2_TYYY, S2_HTX, S2_HTY, S2_N };
+
+struct Phys {
+    double Re, Ma, Pr, gamma, T0;
+};
+
+// Device-resident per-step parameters, written by one small copy before each step so
+// that a captured graph replays with new values.
+struct StepParams {
+    double t, dt;
+    long long slot;   // row of the max-change history to fill
+};
+
+// RK4 stage modes for the assembly epilogue (timeIntegration.F90:380-487)
+enum { RK_STORE_RHS = 0, RK_STAGE1 = 1, RK_STAGE2 = 2, RK_STAGE3 = 3, RK_STAGE4 = 4 };
+
+struct FieldSet {
+    double *p;            // base
+    long long bstride;    // elements between members
+    long long npts;
+    __device__ __forceinline__ double *f(int b, int slot) const { return p + b * bstride + slot * npts; }
+};
+
+// Pointers of the five state variables of one set (U, V, W, R, E); separate pointers
+// because in 2-D the W of a stage is a different array than U/V/R/E.
+struct StateSet {
+    double *v[5];
+    long long bstride;
+};
+
+__device__ __forceinline__ double sutherland_mu(const Phys &ph, double E)
+{
+    // nseq.F90:225-228 (and 77-80 in 2-D)
+    const double g = ph.gamma, Ma = ph.Ma, T0 = ph.T0;
+    const double mu1 = (1.0 + 110.0 / T0) / (g * (g - 1.0) * Ma * Ma * E + 110.0 / T0);
+    const double mu2 = g * (g - 1.0) * Ma * Ma * E;
+    return mu1 * mu2 * sqrt(mu2);
+}
+
+// Stresses and heat fluxes, 3-D (nseq.F90:225-239, 286-288)
+__global__ void k_visc3d(Phys ph, StateSet q, FieldSet d1, FieldSet tq, long long n)
+{
+    const int b = blockIdx.y;
+    const double *E = q.v[4] + b * q.bstride;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const double mu = sutherland_mu(ph, E[p]);
+        const double dux = d1.f(b, D3_UX)[p], dvy = d1.f(b, D3_VY)[p], dwz = d1.f(b, D3_WZ)[p];
+        const double tzz = -2.0 / 3.0 * (dux + dvy + dwz);
+        const double c = 1.0 / ph.Re * mu;
+        tq.f(b, T3_XX)[p] = c * (2.0 * dux + tzz);
+        tq.f(b, T3_YY)[p] = c * (2.0 * dvy + tzz);
+        tq.f(b, T3_ZZ)[p] = c * (2.0 * dwz + tzz);
+        tq.f(b, T3_XY)[p] = c * (d1.f(b, D3_UY)[p] + d1.f(b, D3_VX)[p]);
+        tq.f(b, T3_XZ)[p] = c * (d1.f(b, D3_UZ)[p] + d1.f(b, D3_WX)[p]);
+        tq.f(b, T3_YZ)[p] = c * (d1.f(b, D3_VZ)[p] + d1.f(b, D3_WY)[p]);
+        const double h = -ph.gamma / ph.Re / ph.Pr * mu;
+        tq.f(b, T3_QX)[p] = h * d1.f(b, D3_EX)[p];
+        tq.f(b, T3_QY)[p] = h * d1.f(b, D3_EY)[p];
+        tq.f(b, T3_QZ)[p] = h * d1.f(b, D3_EZ)[p];
+    }
+}
+
+// Stresses and heat fluxes, 2-D (nseq.F90:77-85, 109-110)
+__global__ void k_visc2d(Phys ph, StateSet q, FieldSet d1, FieldSet tq, long long n)
+{
+    const int b = blockIdx.y;
+    const double *E = q.v[4] + b * q.bstride;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const double mu = sutherland_mu(ph, E[p]);
+        const double dux = d1.f(b, D2_UX)[p], dvy = d1.f(b, D2_VY)[p];
+        const double c = 1.0 / ph.Re * mu;
+        tq.f(b, T2_XX)[p] = c * (2.0 * dux - 2.0 / 3.0 * (dux + dvy));
+        tq.f(b, T2_YY)[p] = c * (2.0 * dvy - 2.0 / 3.0 * (dux + dvy));
+        tq.f(b, T2_XY)[p] = c * (d1.f(b, D2_UY)[p] + d1.f(b, D2_VX)[p]);
+        const double h = -ph.gamma / ph.Re / ph.Pr * mu;
+        tq.f(b, T2_QX)[p] = h * d1.f(b, D2_EX)[p];
+        tq.f(b, T2_QY)[p] = h * d1.f(b, D2_EY)[p];
+    }
+}
+
+// RK4 update of one variable at one point (timeIntegration.F90:393-487)
+__device__ __forceinline__ void rk_update(int mode, double dt, double k, double q0, double *delta, double *qn)
+{
+    switch (mode) {
+    case RK_STORE_RHS: *qn = k; break;
+    case RK_STAGE1: *delta = dt / 6.0 * k; *qn = q0 + dt / 2.0 * k; break;
+    case RK_STAGE2: *delta = *delta + dt / 3.0 * k; *qn = q0 + dt / 2.0 * k; break;
+    case RK_STAGE3: *delta = *delta + dt / 3.0 * k; *qn = q0 + dt * k; break;
+    case RK_STAGE4: *qn = q0 + *delta + dt / 6.0 * k; break;
+    }
+}
+
+// Assembly of dR, dU, dV, dW, dE (nseq.F90:310-318) fused with the RK4 stage update.
+// q: stage input; q0: step start; out: stage output (may alias q: pointwise in place).
+__global__ void k_assemble3d(Phys ph, StateSet q, StateSet q0, StateSet out, FieldSet delta,
+                             FieldSet d1, FieldSet tq, FieldSet d2, long long n, int mode,
+                             const StepParams *sp)
+{
+    const int b = blockIdx.y;
+    const double dt = sp ? sp->dt : 0.0;
+    const double g = ph.gamma;
+    const double *U = q.v[0] + b * q.bstride, *V = q.v[1] + b * q.bstride, *W = q.v[2] + b * q.bstride;
+    const double *R = q.v[3] + b * q.bstride, *E = q.v[4] + b * q.bstride;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const double u = U[p], v = V[p], w = W[p], r = R[p], e = E[p];
+        const double dux = d1.f(b, D3_UX)[p], duy = d1.f(b, D3_UY)[p], duz = d1.f(b, D3_UZ)[p];
+        const double dvx = d1.f(b, D3_VX)[p], dvy = d1.f(b, D3_VY)[p], dvz = d1.f(b, D3_VZ)[p];
+        const double dwx = d1.f(b, D3_WX)[p], dwy = d1.f(b, D3_WY)[p], dwz = d1.f(b, D3_WZ)[p];
+        const double drx = d1.f(b, D3_RX)[p], dry = d1.f(b, D3_RY)[p], drz = d1.f(b, D3_RZ)[p];
+        const double dex = d1.f(b, D3_EX)[p], dey = d1.f(b, D3_EY)[p], dez = d1.f(b, D3_EZ)[p];
+        const double P = (g - 1.0) * r * e;
+        const double DPx = (g - 1.0) * (r * dex + drx * e);
+        const double DPy = (g - 1.0) * (r * dey + dry * e);
+        const double DPz = (g - 1.0) * (r * dez + drz * e);
+        const double vtx = d2.f(b, S3_TXXX)[p] + d2.f(b, S3_TXYY)[p] + d2.f(b, S3_TXZZ)[p];
+        const double vty = d2.f(b, S3_TYYY)[p] + d2.f(b, S3_TXYX)[p] + d2.f(b, S3_TYZZ)[p];
+        const double vtz = d2.f(b, S3_TZZZ)[p] + d2.f(b, S3_TXZX)[p] + d2.f(b, S3_TYZY)[p];
+        const double kR = -r * (dux + dvy + dwz) - drx * u - dry * v - drz * w;
+        const double kU = -(dux * u + duy * v + duz * w) + (vtx - DPx) / r;
+        const double kV = -(dvx * u + dvy * v + dvz * w) + (vty - DPy) / r;
+        const double kW = -(dwx * u + dwy * v + dwz * w) + (vtz - DPz) / r;
+        const double kE = -(dex * u + dey * v + dez * w)
+                        + (-P * (dux + dvy + dwz) + tq.f(b, T3_XX)[p] * dux + tq.f(b, T3_YY)[p] * dvy
+                           + tq.f(b, T3_ZZ)[p] * dwz + tq.f(b, T3_XY)[p] * (dvx + duy)
+                           + tq.f(b, T3_XZ)[p] * (dwx + duz) + tq.f(b, T3_YZ)[p] * (dwy + dvz)
+                           - d2.f(b, S3_HTX)[p] - d2.f(b, S3_HTY)[p] - d2.f(b, S3_HTZ)[p]) / r;
+        const double k[5] = {kU, kV, kW, kR, kE};
+#pragma unroll
+        for (int f = 0; f < 5; f++) {
+            double *dl = delta.p ? delta.f(b, f) + p : nullptr;
+            double q0v = (mode != RK_STORE_RHS) ? q0.v[f][b * q0.bstride + p] : 0.0;
+            double res;
+            double dtmp = dl ? *dl : 0.0;
+            rk_update(mode, dt, k[f], q0v, &dtmp, &res);
+            if (dl && mode != RK_STAGE4 && mode != RK_STORE_RHS) *dl = dtmp;
+            out.v[f][b * out.bstride + p] = res;
+        }
+    }
+}
+
+// 2-D assembly (nseq.F90:126-132) fused with the RK4 stage update.  W is left alone.
+__global__ void k_assemble2d(Phys ph, StateSet q, StateSet q0, StateSet out, FieldSet delta,
+                             FieldSet d1, FieldSet tq, FieldSet d2, long long n, int mode,
+                             const StepParams *sp)
+{
+    const int b = blockIdx.y;
+    const double dt = sp ? sp->dt : 0.0;
+    const double g = ph.gamma;
+    const double *U = q.v[0] + b * q.bstride, *V = q.v[1] + b * q.bstride;
+    const double *R = q.v[3] + b * q.bstride, *E = q.v[4] + b * q.bstride;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const double u = U[p], v = V[p], r = R[p], e = E[p];
+        const double dux = d1.f(b, D2_UX)[p], duy = d1.f(b, D2_UY)[p];
+        const double dvx = d1.f(b, D2_VX)[p], dvy = d1.f(b, D2_VY)[p];
+        const double drx = d1.f(b, D2_RX)[p], dry = d1.f(b, D2_RY)[p];
+        const double dex = d1.f(b, D2_EX)[p], dey = d1.f(b, D2_EY)[p];
+        const double P = (g - 1.0) * r * e;
+        const double DPx = (g - 1.0) * (r * dex + drx * e);
+        const double DPy = (g - 1.0) * (r * dey + dry * e);
+        const double vtx = d2.f(b, S2_TXXX)[p] + d2.f(b, S2_TXYY)[p];
+        const double vty = d2.f(b, S2_TYYY)[p] + d2.f(b, S2_TXYX)[p];
+        const double kR = -r * (dux + dvy) - drx * u - dry * v;
+        const double kU = -(dux * u + duy * v) + (vtx - DPx) / r;
+        const double kV = -(dvx * u + dvy * v) + (vty - DPy) / r;
+        const double kE = -(dex * u + dey * v)
+                        + (-P * (dux + dvy) + tq.f(b, T2_XX)[p] * dux + tq.f(b, T2_YY)[p] * dvy
+                           + tq.f(b, T2_XY)[p] * (dvx + duy) - d2.f(b, S2_HTX)[p] - d2.f(b, S2_HTY)[p]) / r;
+        const double k[5] = {kU, kV, 0.0, kR, kE};
+#pragma unroll
+        for (int f = 0; f < 5; f++) {
+            if (f == 2) continue;
+            double *dl = delta.p ? delta.f(b, f) + p : nullptr;
+            double q0v = (mode != RK_STORE_RHS) ? q0.v[f][b * q0.bstride + p] : 0.0;
+            double res;
+            double dtmp = dl ? *dl : 0.0;
+            rk_update(mode, dt, k[f], q0v, &dtmp, &res);
+            if (dl && mode != RK_STAGE4 && mode != RK_STORE_RHS) *dl = dtmp;
+            out.v[f][b * out.bstride + p] = res;
+        }
+    }
+}
+
+// SFD relaxation (main.F90:381-402)
+__global__ void k_sfd(StateSet q, FieldSet mean, const double *chi, double delta_sfd, int nvar,
+                      long long n, const StepParams *sp)
+{
+    const int b = blockIdx.y;
+    const double dt = sp->dt;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const double x = chi[p];
+        for (int f = 0; f < 5; f++) {
+            if (nvar == 4 && f == 2) continue;
+            double *qm = mean.f(b, f) + p;
+            double *qq = q.v[f] + b * q.bstride + p;
+            double m = *qm, v = *qq;
+            if (delta_sfd > 0) { m = m + dt / delta_sfd * (v - m); *qm = m; }
+            *qq = v - dt * x * (v - m);
+        }
+    }
+}
+
+// max|a - b| per variable, accumulated with an unsigned 64-bit max on the IEEE bits of
+// the (non-negative) differences; a NaN (positive payload) wins over every number.
+__global__ void k_maxchange(StateSet a, StateSet bset, unsigned long long *acc, long long n)
+{
+    const int b = blockIdx.y;
+    __shared__ unsigned long long red[5][32];
+    unsigned long long m[5] = {0, 0, 0, 0, 0};
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int f = 0; f < 5; f++) {
+            const double d = fabs(a.v[f][b * a.bstride + p] - bset.v[f][b * bset.bstride + p]);
+            const unsigned long long u = (unsigned long long)__double_as_longlong(d);
+            m[f] = u > m[f] ? u : m[f];
+        }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int f = 0; f < 5; f++) {
+        unsigned long long v = m[f];
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+            v = w > v ? w : v;
+        }
+        if (lane == 0) red[f][wid] = v;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = blockDim.x >> 5;
+#pragma unroll
+        for (int f = 0; f < 5; f++) {
+            unsigned long long v = lane < nw ? red[f][lane] : 0ull;
+            for (int o = 16; o > 0; o >>= 1) {
+                unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+                v = w > v ? w : v;
+            }
+            if (lane == 0) atomicMax(acc + b * 5 + f, v);
+        }
+    }
+}
+
+// max|U|, max|V|, max|W| (main.F90:196-204), same bit trick
+__global__ void k_maxvel(StateSet a, unsigned long long *acc, long long n)
+{
+    const int b = blockIdx.y;
+    unsigned long long m[3] = {0, 0, 0};
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int f = 0; f < 3; f++) {
+            const double d = fabs(a.v[f][b * a.bstride + p]);
+            const unsigned long long u = (unsigned long long)__double_as_longlong(d);
+            m[f] = u > m[f] ? u : m[f];
+        }
+    }
+#pragma unroll
+    for (int f = 0; f < 3; f++) {
+        unsigned long long v = m[f];
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+            v = w > v ? w : v;
+        }
+        if ((threadIdx.x & 31) == 0) atomicMax(acc + b * 3 + f, v);
+    }
+}
+
+// Copy the accumulated max-change of this step into row `slot` of the history.
+__global__ void k_store_maxchange(const unsigned long long *acc, double *hist, int nvals, const StepParams *sp)
+{
+    for (int i = threadIdx.x; i < nvals; i += blockDim.x)
+        hist[sp->slot * nvals + i] = __longlong_as_double((long long)acc[i]);
+}
+
+__global__ void k_copy(double *dst, const double *src, long long n)
+{
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        dst[p] = src[p];
+}
+
+}  // namespace gatt

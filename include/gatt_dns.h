@@ -1,0 +1,174 @@
+/*
+ * gatt_dns.h -- C-ABI of the B200 (sm_100a) implementation of the GATT_DNS
+ * per-RK4-stage hot path: compressible Navier-Stokes right-hand side, compact
+ * derivative and filter line solves, RK4 stage update, SFD relaxation, boundary
+ * conditions and the max-change residual.
+ *
+ * Drop-in boundary.  The reference Fortran solver (source/Fortran/main.F90) keeps
+ * its time loop, CFL control, logging and I/O, and calls these entry points instead
+ * of RK4_2D/RK4_3D, applyFilters2D/3D, the SFD block and applyBoundCond.  Every
+ * array argument has the exact shape and meaning of the array main.F90 passes today
+ * (column-major, 1-based indices inside index arrays); a Fortran
+ * `interface ... bind(C)` module for these functions ships as include/gatt_dns_mod.f90.
+ *
+ * Conventions
+ *  - Every function returns 0 (GATT_OK) or a GATT_ERR_* code; gatt_strerror() names it.
+ *  - Host pointers are read during the call only; nothing is retained.
+ *  - A context owns one CUDA stream (or the one given by gatt_set_stream); calls on
+ *    one context must come from one host thread at a time.  Contexts are independent.
+ *  - Fields are FP64, nx*ny*nz values, i fastest (Fortran order).  Variables are
+ *    numbered U=0, V=1, W=2, R=3, E=4 (R = density, E = internal energy).
+ *  - A context holds `nbatch` independent flow states that share the mesh,
+ *    coefficients and boundary data; batch members are advanced together.
+ */
+#ifndef GATT_DNS_H
+#define GATT_DNS_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gatt_ctx gatt_ctx;
+
+enum {
+    GATT_OK = 0,
+    GATT_ERR_CUDA = 1,      /* a CUDA runtime call failed (message in gatt_last_error) */
+    GATT_ERR_BADARG = 2,    /* invalid argument: size, index box, direction, coverage */
+    GATT_ERR_BADCOEF = 3,   /* non-finite coefficient or zero pivot in a matrix set */
+    GATT_ERR_DIVERGED = 4,  /* max-change is NaN or all zero (main.F90:433-438) */
+    GATT_ERR_TIMEOUT = 5,   /* a bounded device wait gave up */
+    GATT_ERR_STATE = 6,     /* call out of order (e.g. step before matrices are set) */
+    GATT_ERR_NOMEM = 7      /* device allocation failed */
+};
+
+enum { GATT_VAR_U = 0, GATT_VAR_V = 1, GATT_VAR_W = 2, GATT_VAR_R = 3, GATT_VAR_E = 4 };
+enum { GATT_BC_DIRICHLET = 0, GATT_BC_NEUMANN = 1, GATT_BC_SECOND = 2 };
+enum { GATT_DIST_LID_DRIVEN = 1 };
+
+const char *gatt_strerror(int code);
+/* Text of the last error raised on this host thread (CUDA message, argument name). */
+const char *gatt_last_error(void);
+
+/* Create a context for an nx*ny*nz grid (nz == 1 selects the 2-D equations of
+ * nseq2d/RK4_2D) holding nbatch flow states.  Replaces the allocations of
+ * main.F90:75-190 (decomp_2d_init on one rank: the whole grid is one pencil). */
+int gatt_create(gatt_ctx **ctx, int nx, int ny, int nz, int nbatch);
+void gatt_destroy(gatt_ctx *ctx);
+
+/* Use the caller's CUDA stream (a cudaStream_t passed as void*) for all work. */
+int gatt_set_stream(gatt_ctx *ctx, void *cuda_stream);
+
+/* Physical parameters of parameters.F90 (writeFortranParameters.m:10-14). */
+int gatt_set_physics(gatt_ctx *ctx, double Re, double Ma, double Pr, double gamma, double T0);
+
+/* One direction's compact-scheme arrays, exactly as matrices.F90 allocates them
+ * (writeFortranMatrices.m:73-110; consumed by derivs.F90:556-948):
+ *   dir 1..3 = x, y, z; kind 0 = derivative (derivsA?.. derivsR?), 1 = filter (filterA?..)
+ *   A(N-1,nTypes), B(N-periodic,nTypes), C(N-1,nTypes), D(N,nTypes) (periodic only,
+ *   else may be NULL), R(N, 2*nRHS-1, nTypes); blocks(nBlocks,5) = derivBlocks? with
+ *   1-based (type, a1, a2, b1, b2) line ranges.  The blocks must cover every line of the
+ *   direction exactly once.  The filter uses the derivative blocks (main.F90:360), so
+ *   kind 1 may pass nBlocks = 0 to reuse them. */
+int gatt_set_matrices(gatt_ctx *ctx, int dir, int kind, int periodic, int nRHS, int nTypes,
+                      const double *A, const double *B, const double *C, const double *D,
+                      const double *R, int nBlocks, const int *blocks);
+
+/* filterX/Y/Z and FilterCharTime of matrices.F90 / parameters.F90 (-1 = no blend). */
+int gatt_set_filter(gatt_ctx *ctx, int filterX, int filterY, int filterZ, double filterCharTime);
+
+/* neumannCoeffs / neumann2Coeffs of matrices.F90 (getBoundaryConditions.m:75-80). */
+int gatt_set_neumann(gatt_ctx *ctx, int neumannLength, const double *neumannCoeffs,
+                     int neumann2Length, const double *neumann2Coeffs);
+
+/* One boundary list of boundaryInfo.F90 (writeFortranBoundaries.m): var = U,V,W,E or
+ * GATT_VAR_R for pressure (the reference's 'P' lists: iPd/vPd/iPn/dPn/iPs/dPs);
+ * kind = Dirichlet (ind + val), Neumann or null-second-derivative (ind + dirs).
+ * ind(n,6) holds 1-based [i1 i2 j1 j2 k1 k2]; dirs are 1..6 = xi,xf,yi,yf,zi,zf.
+ * Replaces the nUd..dEs arguments of applyBoundCond (nseq.F90:327-345). */
+int gatt_set_bc(gatt_ctx *ctx, int var, int kind, int n, const int *ind, const double *val,
+                const int *dirs);
+
+/* Corners: cN, cL(cN,6), cD(cN,3), cAdiabatic(cN) of boundaryInfo.F90 (nseq.F90:402-488). */
+int gatt_set_corners(gatt_ctx *ctx, int cN, const int *cL, const int *cD, const int *cAdiabatic);
+
+/* One generated disturbance call of runDisturbances.F90 (writeFortranDisturbances.m:35-90):
+ * type GATT_DIST_LID_DRIVEN = lidDrivenMovement(nx,ny,nz,x,y,z,t,u,U0)
+ * (source/disturbances/lidDrivenMovement.F90), applied to variable `var` on the 1-based
+ * box ind[6] with the box's x coordinates x[ind[1]-ind[0]+1] and parameters par[npar]. */
+int gatt_add_disturbance(gatt_ctx *ctx, int type, int var, const int *ind, const double *x,
+                         int npar, const double *par);
+int gatt_clear_disturbances(gatt_ctx *ctx);
+
+/* SFD (main.F90:122-164, 381-402): type 0 off, 1 constant chi = chiValue, 2 field chi
+ * (nx*ny*nz, from calcSFDregion.m).  Delta <= 0 freezes the mean flow. */
+int gatt_set_sfd(gatt_ctx *ctx, int type, double Delta, double chiValue, const double *chi);
+
+/* Flow state of batch member b (host arrays of nx*ny*nz doubles each). */
+int gatt_upload(gatt_ctx *ctx, int b, const double *U, const double *V, const double *W,
+                const double *R, const double *E);
+int gatt_download(gatt_ctx *ctx, int b, double *U, double *V, double *W, double *R, double *E);
+/* SFD mean flow (Umean..Emean of main.F90:149-164). */
+int gatt_upload_mean(gatt_ctx *ctx, int b, const double *U, const double *V, const double *W,
+                     const double *R, const double *E);
+int gatt_download_mean(gatt_ctx *ctx, int b, double *U, double *V, double *W, double *R,
+                       double *E);
+/* In 2-D, main.F90 keeps Wnew apart from W (it is never copied back); its value enters the
+ * W max-change.  These move that array. */
+int gatt_upload_wnew(gatt_ctx *ctx, int b, const double *Wnew);
+int gatt_download_wnew(gatt_ctx *ctx, int b, double *Wnew);
+
+/* Device pointer of a state field of member b (var 0..4), for callers that keep the flow
+ * on the GPU between calls.  Valid until gatt_destroy. */
+int gatt_state_device_ptr(gatt_ctx *ctx, int b, int var, double **dptr);
+
+/* applyBoundCond on the device state at time t (nseq.F90:327-518), all members. */
+int gatt_apply_bc(gatt_ctx *ctx, double t);
+
+/* One compact line solve -- solveSystem{X,Y,Z}[per] (derivs.F90:556-948) -- of the host
+ * field F into dF with the derivative (kind 0) or filter (kind 1) coefficients of dir. */
+int gatt_deriv_dir(gatt_ctx *ctx, int dir, int kind, const double *F, double *dF);
+
+/* Navier-Stokes right-hand side -- nseq2d / nseq3d (nseq.F90:10-323) -- of host fields;
+ * in 2-D, W and dW are ignored. */
+int gatt_rhs(gatt_ctx *ctx, const double *U, const double *V, const double *W, const double *R,
+             const double *E, double *dU, double *dV, double *dW, double *dR, double *dE);
+
+/* applyFilters2D/3D (derivs.F90:303-552) in place on the device state of all members;
+ * blend = dt/FilterCharTime as main.F90:363 passes it. */
+int gatt_filter(gatt_ctx *ctx, double blend);
+
+/* One time step on the device state of all members: RK4_2D/RK4_3D, the filter, SFD,
+ * applyBoundCond at t+dt, the max-change residual, and U = Unew (main.F90:255-465 minus the
+ * CFL/dt control, logging and I/O).  maxChange receives 5*nbatch values (member-major);
+ * it may be NULL.  Returns GATT_ERR_DIVERGED when a member's max-change is NaN or sums to
+ * zero, as main.F90:433-438 stops. */
+int gatt_step(gatt_ctx *ctx, double t, double dt, double *maxChange);
+
+/* nsteps fixed-dt steps (t advances by dt each step, as main.F90:423 does) without a host
+ * synchronisation per step; maxChange receives the last step's 5*nbatch values. */
+int gatt_run(gatt_ctx *ctx, int nsteps, double t0, double dt, double *maxChange);
+
+/* max|U|, max|V|, max|W| of every member (main.F90:196-204), for the caller's CFL. */
+int gatt_max_velocity(gatt_ctx *ctx, double *vmax);
+
+/* Wait for all work of the context. */
+int gatt_synchronize(gatt_ctx *ctx);
+
+/* Number of kernels this context launched since creation (for launch accounting). */
+long long gatt_kernel_launches(gatt_ctx *ctx);
+
+/* Profiling hook (no counterpart in the reference): runs nsteps uncaptured steps with a
+ * CUDA event pair around every kernel launch and returns, per kernel class, the mean
+ * device time of one launch in ms[GATT_NPROF] and the launches per step in
+ * launches[GATT_NPROF].  Advances the state like gatt_run.  gatt_profile_name(i) names
+ * class i. */
+#define GATT_NPROF 15
+int gatt_profile_kernels(gatt_ctx *ctx, double t0, double dt, int nsteps, double *ms, double *launches);
+const char *gatt_profile_name(int cls);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,233 @@
+"""GPU parity: the CUDA path through the C-ABI against the CPU oracle on the same inputs.
+
+Tolerances (FP64; the kernels keep the reference's per-line operation order, so the
+differences are rounding only):
+* one line solve or one RHS evaluation: 1e-12 relative (max-norm per field)
+* one time step: 1e-12 relative; 100 steps: 1e-9 relative
+"""
+import numpy as np
+import pytest
+
+from gatt_dns_b200 import case as cs
+
+pytestmark = pytest.mark.gpu
+
+RHS_TOL = 1e-12
+STEP_TOL = 1e-12
+LONG_TOL = 1e-9
+KEYS = ("U", "V", "W", "R", "E")
+
+
+def rel(a, b):
+    s = np.max(np.abs(b))
+    return float(np.max(np.abs(a - b)) / (s if s > 0 else 1.0))
+
+
+def fields(case):
+    return KEYS if case.is3d else ("U", "V", "R", "E")
+
+
+_CASES = {}
+
+
+def get_case(name):
+    if name not in _CASES:
+        if name == "box":
+            _CASES[name] = cs.periodic_box(n=32)
+        elif name == "box_aniso":
+            _CASES[name] = cs.periodic_box(nxyz=(40, 24, 16))
+        elif name == "lid":
+            _CASES[name] = cs.lid_driven(n=48)
+        elif name == "lid_tanh":
+            _CASES[name] = cs.lid_driven(nxy=(40, 36), mesh_type="tanh")
+        elif name == "cavity2d":
+            _CASES[name] = cs.cavity_channel(nx=48, ny=40, nz=1, sfd={"X": 0.05, "Delta": 10.0, "buffer": 8})
+        elif name == "cavity3d":
+            _CASES[name] = cs.cavity_channel(nx=24, ny=20, nz=8, adiabatic_corners=True,
+                                             sfd={"X": 0.05, "Delta": 10.0, "buffer": 6})
+        elif name == "long_x":
+            _CASES[name] = cs.lid_driven(nxy=(900, 12))
+    return _CASES[name]
+
+
+def flow_for(case, seed=5):
+    return cs.random_flow(case, seed=seed, amp=0.05)
+
+
+@pytest.fixture(scope="module")
+def libs(cuda_lib, oracle_lib):
+    return cuda_lib, oracle_lib
+
+
+def pair(name):
+    from gatt_dns_b200.solver import GattDNS
+    from oracle import Oracle
+    c = get_case(name)
+    return c, GattDNS(c), Oracle(c)
+
+
+@pytest.mark.parametrize("name", ["box", "box_aniso", "lid", "lid_tanh", "cavity2d", "cavity3d", "long_x"])
+@pytest.mark.parametrize("kind", ["deriv", "filter"])
+def test_line_solves(libs, name, kind):
+    c, g, o = pair(name)
+    rng = np.random.default_rng(11)
+    F = np.asfortranarray(rng.standard_normal((c.nx, c.ny, c.nz)))
+    for d in range(1, 4 if c.is3d else 3):
+        a = g.calc_derivs(F, d, kind)
+        b = o.calc_derivs(F, d, kind)
+        assert rel(a, b) < RHS_TOL, (name, kind, d, rel(a, b))
+    g.close()
+
+
+@pytest.mark.parametrize("name", ["box", "box_aniso", "lid", "lid_tanh", "cavity2d", "cavity3d"])
+def test_rhs(libs, name):
+    c, g, o = pair(name)
+    f = flow_for(c)
+    a, b = g.nseq(f), o.nseq(f)
+    for k in fields(c):
+        assert rel(a[k], b[k]) < RHS_TOL, (name, k, rel(a[k], b[k]))
+    g.close()
+
+
+@pytest.mark.parametrize("name", ["lid", "cavity2d", "cavity3d"])
+def test_boundary_conditions(libs, name):
+    c, g, o = pair(name)
+    f = flow_for(c, seed=9)
+    g.upload(f)
+    g.apply_bound_cond(0.0)
+    a = g.download()
+    b = o.apply_bound_cond(f)
+    for k in KEYS:
+        assert rel(a[k], b[k]) < 1e-14, (name, k)
+    g.close()
+
+
+@pytest.mark.parametrize("name", ["box", "lid", "cavity3d"])
+def test_filter_in_place(libs, name):
+    c, g, o = pair(name)
+    f = flow_for(c, seed=4)
+    for blend in (-1.0, 0.3):
+        g.upload(f)
+        g.apply_filters(blend)
+        a = g.download()
+        b = o.apply_filters(f, blend)
+        for k in fields(c):
+            assert rel(a[k], b[k]) < RHS_TOL, (name, blend, k)
+    g.close()
+
+
+@pytest.mark.parametrize("name", ["box", "box_aniso", "lid", "lid_tanh", "cavity2d", "cavity3d"])
+def test_step(libs, name):
+    c, g, o = pair(name)
+    f = flow_for(c, seed=2)
+    dt = 0.25 * c.cfl_dt(f["U"], f["V"], f["W"], 1.0)
+    g.upload(f)
+    st = o.new_state(f)
+    for s in range(3):
+        mg = g.step(s * dt, dt)[0]
+        mo = o.step(st, s * dt, dt)
+        assert np.allclose(mg, mo, rtol=1e-10, atol=1e-15), (name, s, mg, mo)
+    a = g.download()
+    for k in KEYS:
+        assert rel(a[k], st[k]) < STEP_TOL * 10, (name, k, rel(a[k], st[k]))
+    if c.sfd_type:
+        m = g.download_mean()
+        for k in fields(c):
+            assert rel(m[k], st["m" + k]) < STEP_TOL * 10
+    if not c.is3d:
+        assert rel(g.download_wnew(), st["Wnew"]) < 1e-14
+    assert g.kernel_launches() > 0
+    g.close()
+
+
+def test_lid_driven_100_steps(libs):
+    c, g, o = pair("lid")
+    f = cs.uniform_flow(c)
+    f = o.apply_bound_cond(f)
+    dt = c.cfl_dt(f["U"], f["V"], f["W"], 0.5)
+    g.upload(f)
+    st = o.new_state(f)
+    for s in range(100):
+        o.step(st, s * dt, dt)
+    mg = g.run(100, 0.0, dt)[0]
+    a = g.download()
+    for k in ("U", "V", "R", "E"):
+        assert rel(a[k], st[k]) < LONG_TOL, (k, rel(a[k], st[k]))
+    assert np.all(np.isfinite(mg))
+    g.close()
+
+
+def test_batched_members_match_single_runs(libs):
+    from gatt_dns_b200.solver import GattDNS
+    c = get_case("box")
+    fa, fb = flow_for(c, seed=1), flow_for(c, seed=2)
+    dt = 0.2 * c.cfl_dt(fa["U"], fa["V"], fa["W"], 1.0)
+    gb = GattDNS(c, nbatch=2)
+    gb.upload(fa, 0)
+    gb.upload(fb, 1)
+    mc = gb.run(3, 0.0, dt)
+    outs = [gb.download(0), gb.download(1)]
+    for i, f in enumerate((fa, fb)):
+        g1 = GattDNS(c)
+        g1.upload(f)
+        m1 = g1.run(3, 0.0, dt)[0]
+        o1 = g1.download()
+        assert np.array_equal(m1, mc[i])
+        for k in KEYS:
+            assert np.array_equal(o1[k], outs[i][k])
+        g1.close()
+    gb.close()
+
+
+def test_full_size_box_one_step(libs):
+    """128^3 periodic box: one step against the oracle, plus exact mass conservation."""
+    from gatt_dns_b200.solver import GattDNS
+    from oracle import Oracle
+    c = cs.periodic_box(n=128)
+    f = cs.solenoidal_turbulence(c, seed=1234)
+    dt = c.cfl_dt(f["U"], f["V"], f["W"], 0.5)
+    g = GattDNS(c)
+    g.upload(f)
+    mg = g.step(0.0, dt)[0]
+    a = g.download()
+    o = Oracle(c)
+    st = o.new_state(f)
+    mo = o.step(st, 0.0, dt)
+    assert np.allclose(mg, mo, rtol=1e-10)
+    for k in KEYS:
+        assert rel(a[k], st[k]) < STEP_TOL * 10, k
+    m0 = np.sum(f["R"])
+    mg2 = g.run(10, dt, dt)
+    b = g.download()
+    assert abs(np.sum(b["R"]) - m0) / m0 < 1e-12
+    g.close()
+
+
+def test_errors_are_reported(libs):
+    import ctypes
+    from gatt_dns_b200 import _lib
+    from gatt_dns_b200.solver import GattDNS
+    c = get_case("lid")
+    g = GattDNS(c)
+    L = g.lib
+    m = c.mats[0]
+    A, B, C, R = (np.asfortranarray(x) for x in (m.A, m.B.copy(), m.C, m.R))
+    B[3, 0] = np.inf
+    blocks = np.asfortranarray(m.blocks.astype(np.int32))
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    rc = L.gatt_set_matrices(g.h, 1, 0, 0, m.nRHS, m.nTypes, dp(A), dp(B), dp(C), None, dp(R), blocks.shape[0], ip(blocks))
+    assert rc == 3  # GATT_ERR_BADCOEF
+    B = np.asfortranarray(m.B)
+    bad = blocks.copy()
+    bad[0, 2] = bad[0, 2] - 1  # leaves a line uncovered
+    rc = L.gatt_set_matrices(g.h, 1, 0, 0, m.nRHS, m.nTypes, dp(A), dp(B), dp(C), None, dp(R), bad.shape[0], ip(bad))
+    assert rc == 2  # GATT_ERR_BADARG
+    # a NaN in the state is reported as divergence (main.F90:433-438)
+    f = cs.uniform_flow(c)
+    f["E"][7, 7, 0] = np.nan
+    g.upload(f)
+    with pytest.raises(_lib.GattError) as e:
+        g.step(0.0, 1e-3)
+    assert e.value.code == 4
+    g.close()
