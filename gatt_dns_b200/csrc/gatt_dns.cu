@@ -8,6 +8,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -45,8 +46,9 @@ int fail(int code, const std::string &msg)
 
 struct DevDir {
     bool set = false;
-    int periodic = 0, nR = 0, nTypes = 0, N = 0, W = 0;
-    double *R = nullptr, *A = nullptr, *B = nullptr, *C = nullptr, *D = nullptr;
+    int periodic = 0, nR = 0, nTypes = 0, N = 0, W = 0, Wp = 0, P = 1;
+    double *Rm = nullptr;  // band coefficients [nTypes][N][Wp]
+    double *Q = nullptr;   // row records [nTypes][N][kQ] (see sweep.cuh)
 };
 
 struct HostBC {
@@ -206,47 +208,62 @@ int nd2(const gatt_ctx *c) { return c->is3d ? S3_N : S2_N; }
 // line-solve dispatch
 // ---------------------------------------------------------------------------
 
-template <bool XD, bool PER, int EPI>
+template <bool XD, bool PER, bool BIG>
 void *pick_kernel(int nR)
 {
     switch (nR) {
-    case 2: return (void *)k_sweep<XD, PER, 2, EPI>;
-    case 3: return (void *)k_sweep<XD, PER, 3, EPI>;
-    case 4: return (void *)k_sweep<XD, PER, 4, EPI>;
-    case 5: return (void *)k_sweep<XD, PER, 5, EPI>;
-    case 6: return (void *)k_sweep<XD, PER, 6, EPI>;
-    case 7: return (void *)k_sweep<XD, PER, 7, EPI>;
-    case 8: return (void *)k_sweep<XD, PER, 8, EPI>;
-    case 9: return (void *)k_sweep<XD, PER, 9, EPI>;
-    case 10: return (void *)k_sweep<XD, PER, 10, EPI>;
-    case 11: return (void *)k_sweep<XD, PER, 11, EPI>;
+    case 2: return (void *)k_sweep<XD, PER, 2, BIG>;
+    case 3: return (void *)k_sweep<XD, PER, 3, BIG>;
+    case 4: return (void *)k_sweep<XD, PER, 4, BIG>;
+    case 5: return (void *)k_sweep<XD, PER, 5, BIG>;
+    case 6: return (void *)k_sweep<XD, PER, 6, BIG>;
+    case 7: return (void *)k_sweep<XD, PER, 7, BIG>;
+    case 8: return (void *)k_sweep<XD, PER, 8, BIG>;
+    case 9: return (void *)k_sweep<XD, PER, 9, BIG>;
+    case 10: return (void *)k_sweep<XD, PER, 10, BIG>;
+    case 11: return (void *)k_sweep<XD, PER, 11, BIG>;
     default: return nullptr;
     }
 }
 
-void *sweep_kernel(bool xd, bool per, int epi, int nR)
+void *sweep_kernel(bool xd, bool per, int nR, bool big)
 {
-    if (xd) {
-        if (per) return epi ? pick_kernel<true, true, 1>(nR) : pick_kernel<true, true, 0>(nR);
-        return epi ? pick_kernel<true, false, 1>(nR) : pick_kernel<true, false, 0>(nR);
+    if (big) {
+        if (xd) return per ? pick_kernel<true, true, true>(nR) : pick_kernel<true, false, true>(nR);
+        return per ? pick_kernel<false, true, true>(nR) : pick_kernel<false, false, true>(nR);
     }
-    if (per) return epi ? pick_kernel<false, true, 1>(nR) : pick_kernel<false, true, 0>(nR);
-    return epi ? pick_kernel<false, false, 1>(nR) : pick_kernel<false, false, 0>(nR);
+    if (xd) return per ? pick_kernel<true, true, false>(nR) : pick_kernel<true, false, false>(nR);
+    return per ? pick_kernel<false, true, false>(nR) : pick_kernel<false, false, false>(nR);
 }
 
-size_t sweep_smem(int N, int nR) { return (size_t)(N + nR) * kPad * sizeof(double); }
-constexpr size_t kMaxSmem = 227 * 1024;
+size_t sweep_smem(int N, int P, int nR, int Wp) { return sweep_smem_doubles(N, P, nR, Wp) * sizeof(double); }
+// 227 KB per block, less a margin for the kernel's few static shared variables
+constexpr size_t kMaxSmem = 227 * 1024 - 256;
 constexpr int kMaxNR = 11;  // widest band the shared-tile solver is instantiated for
+
+// Row blocks per line: about 32 rows per block (shorter dependency chains, more warps per
+// tile), a power of two up to kMaxP, and every block at least nR+1 rows long.
+int choose_blocks(int N, int nR)
+{
+    static int rows = [] {
+        const char *e = getenv("GATT_BLOCK_ROWS");
+        const int v = e ? atoi(e) : 0;
+        return v >= 4 ? v : 32;
+    }();
+    int P = 1;
+    while (P * 2 <= kMaxP && N / (P * 2) >= rows && N / (P * 2) >= nR + 1) P *= 2;
+    return P;
+}
 
 // Allow every line-solve instantiation the full shared-memory budget once per context,
 // outside any stream capture.
 int set_sweep_attributes()
 {
-    for (int xd = 0; xd < 2; xd++)
-        for (int per = 0; per < 2; per++)
-            for (int epi = 0; epi < 2; epi++)
+    for (int big = 0; big < 2; big++)
+        for (int xd = 0; xd < 2; xd++)
+            for (int per = 0; per < 2; per++)
                 for (int nR = 2; nR <= kMaxNR; nR++) {
-                    void *k = sweep_kernel(xd != 0, per != 0, epi, nR);
+                    void *k = sweep_kernel(xd != 0, per != 0, nR, big != 0);
                     CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
                 }
     return GATT_OK;
@@ -271,20 +288,20 @@ int sweep(gatt_ctx *c, int d, int kind, const double *in, long long in_bs, const
     a.N = m.N; a.nlines = nlines(c, d);
     a.es = d == 1 ? c->nx : (long long)c->nx * c->ny;
     a.os = d == 1 ? (long long)c->nx * c->ny : c->nx;
-    a.tiles_per_row = (c->nx + kTileLines - 1) / kTileLines;
-    a.R = m.R; a.A = m.A; a.B = m.B; a.C = m.C; a.D = m.D; a.W = m.W;
+    a.tiles_per_row = (c->nx + kLanes - 1) / kLanes;
+    a.Rm = m.Rm; a.Q = m.Q; a.W = m.W; a.Wp = m.Wp; a.P = m.P;
     a.ltype = c->ltype[d];
     a.blend = blend; a.blend_dt = blend_dt; a.blend_fct = c->fct;
-    const int epi = (blend_dt != nullptr || blend > 0) ? EPI_BLEND : EPI_STORE;
-    const size_t smem = sweep_smem(m.N, m.nR);
-    void *k = sweep_kernel(d == 0, m.periodic != 0, epi, m.nR);
+    a.epi = (blend_dt != nullptr || blend > 0) ? EPI_BLEND : EPI_STORE;
+    const size_t smem = sweep_smem(m.N, m.P, m.nR, m.Wp);
+    void *k = sweep_kernel(d == 0, m.periodic != 0, m.nR, m.P > 4);
     if (k && smem <= kMaxSmem && m.N >= 2) {
-        dim3 grid(d == 0 ? (a.nlines + kTileLines - 1) / kTileLines
+        dim3 grid(d == 0 ? (a.nlines + kLanes - 1) / kLanes
                          : a.tiles_per_row * (d == 1 ? c->nz : c->ny),
                   nf, nmembers);
         void *args[] = {&a};
         TRY(before_launch(c, cls));
-        CU(cudaLaunchKernel(k, grid, dim3(32), args, smem, c->stream));
+        CU(cudaLaunchKernel(k, grid, dim3(32 * m.P), args, smem, c->stream));
         return after_launch(c);
     }
     // long lines: global-memory variant, out of place through the scratch field
@@ -778,7 +795,8 @@ void gatt_destroy(gatt_ctx *c)
     for (int d = 0; d < 3; d++) {
         for (int k = 0; k < 2; k++) {
             DevDir &m = c->mat[d][k];
-            cudaFree(m.R); cudaFree(m.A); cudaFree(m.B); cudaFree(m.C); cudaFree(m.D);
+            cudaFree(m.Rm);
+            cudaFree(m.Q);
         }
         cudaFree(c->ltype[d]);
     }
@@ -887,21 +905,54 @@ int gatt_set_matrices(gatt_ctx *c, int dir, int kind, int periodic, int nRHS, in
         for (uint8_t t : cur)
             if (t >= nTypes) return fail(GATT_ERR_BADARG, "existing block types exceed nTypes");
     }
+    // Kernel row records (sweep.cuh): the reference's factors in uniform row semantics
+    // plus the block propagators of the partitioned recurrences (long double products).
+    const int P = choose_blocks(N, nRHS);
+    const int Wp = (W + 3) / 4 * 4;
+    std::vector<double> hRm((size_t)nTypes * N * Wp, 0.0), hQ((size_t)nTypes * N * kQ, 0.0);
+    for (int t = 0; t < nTypes; t++) {
+        const double *tA = &hA[(size_t)t * N], *tB = &hB[(size_t)t * N], *tC = &hC[(size_t)t * N];
+        double *q = &hQ[(size_t)t * N * kQ];
+        for (int r = 0; r < N; r++) {
+            double *qr = q + (size_t)r * kQ;
+            if (!periodic) {
+                qr[kQfA] = r > 0 ? tA[r - 1] : 0.0;       // derivs.F90:607
+                qr[kQfB] = tB[r];
+                qr[kQbC] = r < N - 1 ? tC[r] : 0.0;       // derivs.F90:610
+            } else {
+                qr[kQfA] = r >= 2 ? tA[r - 1] : 0.0;      // derivs.F90:798
+                qr[kQfB] = r >= 1 ? tB[r - 1] : 0.0;      // derivs.F90:796-798
+                qr[kQbC] = (r >= 1 && r <= N - 2) ? tC[r] : 0.0;  // derivs.F90:801
+                qr[kQD] = hD[(size_t)t * N + r];          // derivs.F90:786-789
+            }
+            for (int k = 0; k < W; k++) hRm[((size_t)t * N + r) * Wp + k] = hR[((size_t)t * N + r) * W + k];
+        }
+        if (periodic) { q[kQcA] = tA[0]; q[kQcC] = tC[0]; }  // derivs.F90:792-793
+        for (int p = 0; p < P; p++) {
+            const int s0 = block_start(p, N, P), e0 = block_start(p + 1, N, P) - 1;
+            const int rs = (periodic && p == 0) ? 1 : s0;
+            long double prod = 1.0L;
+            for (int r = rs; r <= e0; r++) {
+                prod *= -(long double)q[(size_t)r * kQ + kQfA] * (long double)q[(size_t)r * kQ + kQfB];
+                q[(size_t)r * kQ + kQpi] = (double)prod;
+            }
+            prod = 1.0L;
+            for (int r = e0; r >= rs; r--) {
+                prod *= -(long double)q[(size_t)r * kQ + kQbC];
+                q[(size_t)r * kQ + kQrho] = (double)prod;
+            }
+        }
+    }
     CU(cudaStreamSynchronize(c->stream));
     DevDir &m = c->mat[d][kind];
-    cudaFree(m.R); cudaFree(m.A); cudaFree(m.B); cudaFree(m.C); cudaFree(m.D);
+    cudaFree(m.Rm);
+    cudaFree(m.Q);
     m = DevDir();
-    CU(cudaMalloc(&m.R, hR.size() * sizeof(double)));
-    CU(cudaMalloc(&m.A, hA.size() * sizeof(double)));
-    CU(cudaMalloc(&m.B, hB.size() * sizeof(double)));
-    CU(cudaMalloc(&m.C, hC.size() * sizeof(double)));
-    CU(cudaMalloc(&m.D, hD.size() * sizeof(double)));
-    CU(cudaMemcpy(m.R, hR.data(), hR.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(m.A, hA.data(), hA.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(m.B, hB.data(), hB.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(m.C, hC.data(), hC.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(m.D, hD.data(), hD.size() * sizeof(double), cudaMemcpyHostToDevice));
-    m.periodic = periodic; m.nR = nRHS; m.nTypes = nTypes; m.N = N; m.W = W; m.set = true;
+    CU(cudaMalloc(&m.Rm, hRm.size() * sizeof(double)));
+    CU(cudaMalloc(&m.Q, hQ.size() * sizeof(double)));
+    CU(cudaMemcpy(m.Rm, hRm.data(), hRm.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(m.Q, hQ.data(), hQ.size() * sizeof(double), cudaMemcpyHostToDevice));
+    m.periodic = periodic; m.nR = nRHS; m.nTypes = nTypes; m.N = N; m.W = W; m.Wp = Wp; m.P = P; m.set = true;
     if (nBlocks > 0) {
         if (!c->ltype[d]) CU(cudaMalloc(&c->ltype[d], lt.size()));
         CU(cudaMemcpy(c->ltype[d], lt.data(), lt.size(), cudaMemcpyHostToDevice));

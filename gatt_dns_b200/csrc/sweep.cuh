@@ -1,14 +1,28 @@
 // Compact line solves along x, y or z for sm_100a -- the B200 form of
 // solveSystem{X,Y,Z}[per] (reference source/Fortran/derivs.F90:556-948).
 //
-// Layout: fields are FP64, i fastest.  One warp owns a tile of 32 lines; the tile is
-// staged in shared memory as T[n][33] (row n = position along the line, column = line,
-// one double of padding so both the strided-line load and the per-line solve are free
-// of bank conflicts).  Each lane then runs the reference Thomas recurrence on its own
-// line in place -- one thread per line keeps the reference's operation order, so the
-// result matches the Fortran to rounding.  y- and z-lines are loaded with the warp
-// reading 32 neighbouring lines at one position (256 contiguous bytes); x-lines are
-// contiguous, so the warp reads along a line and transposes through the padded tile.
+// The reference solves every line with the precomputed Thomas factors of
+// prepareThomas.m: a band product rhs = R*F, a forward recurrence
+// y(i) = (rhs(i) - A y(i-1)) B and a backward recurrence x(i) = y(i) - C x(i+1); the cyclic
+// variant first forms x(1) = D . rhs and then runs the same two recurrences on rows 2..N.
+// Both recurrences are linear, so a line can be cut into P row blocks that run them
+// concurrently from zero start values and are then recombined exactly:
+//     y(i) = ytilde(i) + pi(i)  * y(start-1)     pi(i)  = prod_{k=start..i} (-A(k) B(k))
+//     x(i) = xtilde(i) + rho(i) * x(end+1)       rho(i) = prod_{k=i..end}   (-C(k))
+// where pi and rho depend only on the coefficients (precomputed per matrix type) and the
+// block boundary values follow from a P-step prefix/suffix.  The recombination changes the
+// floating-point order only for blocks after the first (forward) / before the last
+// (backward); with P = 1 the kernel performs the reference's operations in its order.
+//
+// Mapping: one CTA = one tile of 32 lines and P warps; lane = line, warp = row block.
+// The tile lives in shared memory as T[n][32] (row n, lane column): every per-row warp
+// access is 32 consecutive doubles (conflict-free).
+//  0. load: x-lines are contiguous, each lane reads 32-byte pieces of its own line;
+//     y/z-lines are strided, each row is one 256-byte coalesced warp access.
+//  1. halos to registers, then band product + forward recurrence of the block (in place)
+//  2. (cyclic) x(1), the reduced forward recurrence
+//  3. prefix of block boundary values, correction, backward recurrence (in place)
+//  4. suffix, correction, store (optionally blended with the input: filter time relaxation)
 #pragma once
 
 #include <cuda_runtime.h>
@@ -16,11 +30,18 @@
 
 namespace gatt {
 
-constexpr int kTileLines = 32;
-constexpr int kPad = 33;  // row pitch of the shared tile, in doubles
-constexpr int kChunk = 16;  // loads each lane keeps in flight while staging a tile
+constexpr int kLanes = 32;   // lines per tile
+constexpr int kMaxP = 16;    // largest number of row blocks per line
 
 enum SweepEpi { EPI_STORE = 0, EPI_BLEND = 1 };
+
+// Per-row coefficient record, in the kernel's uniform row semantics:
+//   forward  y(r) = (rhs(r) - fA(r) y(r-1)) * fB(r)
+//   backward x(r) = y(r) - bC(r) x(r+1)
+// plus the cyclic dot row D, the block propagators pi / rho, and (row 0 of a cyclic
+// type) the corner couplings A(1) = LHS(1,N) and C(1) = LHS(N,1).
+constexpr int kQ = 8;
+constexpr int kQfA = 0, kQfB = 1, kQbC = 2, kQD = 3, kQpi = 4, kQrho = 5, kQcA = 6, kQcC = 7;
 
 struct SweepArgs {
     const double *in;        // base of the input field set
@@ -36,13 +57,16 @@ struct SweepArgs {
     long long es;            // element stride along a strided line (y: nx, z: nx*ny)
     long long os;            // stride of the outer line index (y: nx*ny (k), z: nx (j))
     int tiles_per_row;       // strided: ceil(nx/32)
-    const double *R;         // [nTypes][N][W]
-    const double *A, *B, *C, *D;  // [nTypes][N]
+    const double *Rm;        // band coefficients [nTypes][N][Wp]
+    const double *Q;         // row records [nTypes][N][kQ]
     int W;                   // 2*nR-1
+    int Wp;                  // W padded to a multiple of 4
     const uint8_t *ltype;    // per-line matrix type (0-based)
     double blend;            // EPI_BLEND: out = in + blend*(solve - in) ...
     const double *blend_dt;  // ... or, when set, blend = *blend_dt / blend_fct (device dt)
     double blend_fct;
+    int epi;                 // SweepEpi
+    int P;                   // row blocks per line (1 .. kMaxP); CTA = 32*P threads
 };
 
 __device__ __forceinline__ double sweep_blend(const SweepArgs &a)
@@ -50,165 +74,362 @@ __device__ __forceinline__ double sweep_blend(const SweepArgs &a)
     return a.blend_dt ? *a.blend_dt / a.blend_fct : a.blend;
 }
 
-// Solve the line held in column `col` (stride kPad) in place.
-// Rows N .. N+NR-2 of the column hold copies of rows 0 .. NR-2 (the periodic wrap of
-// the band product).  Non-periodic: derivs.F90:583-611; periodic: derivs.F90:764-802.
-template <bool PER, int NR>
-__device__ __forceinline__ void solve_column(double *__restrict__ col, int N,
-                                             const double *__restrict__ Rt,
-                                             const double *__restrict__ At,
-                                             const double *__restrict__ Bt,
-                                             const double *__restrict__ Ct,
-                                             const double *__restrict__ Dt)
+// Line data is read once per sweep: keep it out of L1 so the coefficient records stay there.
+__device__ __forceinline__ void ld4_stream(const double *p, double *v)
+{
+    asm volatile("ld.global.L1::no_allocate.v4.f64 {%0,%1,%2,%3}, [%4];"
+                 : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "l"(p));
+}
+
+__device__ __forceinline__ double ld_stream(const double *p)
+{
+    double v;
+    asm volatile("ld.global.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ void st4(double *p, const double *v)
+{
+    asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v[0]), "d"(v[1]), "d"(v[2]), "d"(v[3])
+                 : "memory");
+}
+
+// First row of block p of a line of N rows cut into P blocks.
+__host__ __device__ __forceinline__ int block_start(int p, int N, int P) { return (p * N) / P; }
+
+__device__ __forceinline__ void ld4_coef(const double *p, double *v)
+{
+    asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "l"(p));
+}
+
+// Rows per chunk of a recurrence pass: the chunk's coefficients are loaded before its
+// dependent chain runs.
+constexpr int kCh = 8;
+
+// Shared memory of k_sweep, in doubles: the tile [N][32], the right halos of the row
+// blocks [P][NR-1][32], the block-exchange values [3][P][32], then the coefficients of the
+// tile's matrix type (band rows [N][Wp] and records [N][kQ]) when all its lines share one.
+__host__ __device__ __forceinline__ size_t sweep_smem_doubles(int N, int P, int NR, int Wp)
+{
+    return ((size_t)N + (size_t)P * (NR - 1) + 3 * (size_t)P) * kLanes + (size_t)N * (Wp + kQ);
+}
+
+// BIG: instantiation for P > 4 (up to 32*kMaxP threads); otherwise at most 128 threads,
+// which leaves the register allocator room for the chunk buffers.
+template <bool XD, bool PER, int NR, bool BIG>
+__global__ void __launch_bounds__(BIG ? 32 * kMaxP : 128) k_sweep(const SweepArgs a)
 {
     constexpr int W = 2 * NR - 1;
-    double w[W];
-    // window holds F[i-(NR-1) .. i+(NR-1)] (indices modulo N)
-#pragma unroll
-    for (int q = 0; q < W; q++) {
-        int idx = q - (NR - 1);
-        idx = idx < 0 ? idx + N : idx;
-        w[q] = col[idx * kPad];
-    }
-    double dprev = 0.0, x1 = 0.0;
-    for (int i = 0; i < N; i++) {
-        const double *Ri = Rt + (size_t)i * W;
-        double acc = __ldg(Ri + NR - 1) * w[NR - 1];
-#pragma unroll
-        for (int l = 1; l < NR; l++)
-            acc = acc + __ldg(Ri + NR - 1 + l) * w[NR - 1 + l] + __ldg(Ri + NR - 1 - l) * w[NR - 1 - l];
-        if (!PER) {
-            const double d = (i == 0) ? acc * __ldg(Bt) : (acc - __ldg(At + i - 1) * dprev) * __ldg(Bt + i);
-            col[i * kPad] = d;
-            dprev = d;
-        } else {
-            col[i * kPad] = acc;
-            x1 = (i == 0) ? acc * __ldg(Dt) : x1 + acc * __ldg(Dt + i);
-        }
-#pragma unroll
-        for (int q = 0; q < W - 1; q++) w[q] = w[q + 1];
-        if (i + 1 < N) w[W - 1] = col[(i + NR) * kPad];
-    }
-    if (!PER) {
-        double dn = col[(N - 1) * kPad];
-        for (int i = N - 2; i >= 0; i--) {
-            const double d = col[i * kPad] - __ldg(Ct + i) * dn;
-            col[i * kPad] = d;
-            dn = d;
-        }
-    } else {
-        col[0] = x1;
-        double d = (col[kPad] - __ldg(At) * x1) * __ldg(Bt);
-        col[(N - 1) * kPad] = col[(N - 1) * kPad] - __ldg(Ct) * x1;
-        col[kPad] = d;
-        for (int i = 1; i < N - 1; i++) {
-            d = (col[(i + 1) * kPad] - __ldg(At + i) * d) * __ldg(Bt + i);
-            col[(i + 1) * kPad] = d;
-        }
-        double dn = col[(N - 1) * kPad];
-        for (int i = N - 2; i >= 1; i--) {
-            const double e = col[i * kPad] - __ldg(Ct + i) * dn;
-            col[i * kPad] = e;
-            dn = e;
-        }
-    }
-}
-
-// One warp per CTA; grid = (tiles, fields, batch).  Dynamic shared memory:
-// (N + NR) * kPad doubles.
-template <bool XD, bool PER, int NR, int EPI>
-__global__ void __launch_bounds__(32) k_sweep(const SweepArgs a)
-{
+    constexpr int NV = (W + 3) / 4;                          // 32-byte vectors per band row
+    constexpr int RB = NR <= 4 ? 4 : (NR <= 7 ? 2 : 1);      // rows per chunk of the band pass
     extern __shared__ double T[];
-    const int lane = threadIdx.x;
-    const int f = blockIdx.y, b = blockIdx.z;
+    const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
+    const int P = a.P;
     const int N = a.N;
-    const double *__restrict__ F = a.in + (long long)b * a.in_bstride + (long long)a.in_slot[f] * a.npts;
-    double *G = a.out + (long long)b * a.out_bstride + (long long)a.out_slot[f] * a.npts;
-
-    long long base;
-    int nvalid, L0;
+    const int Wp = a.Wp;
+    const double *F = a.in + (long long)blockIdx.z * a.in_bstride + (long long)a.in_slot[blockIdx.y] * a.npts;
+    double *G = a.out + (long long)blockIdx.z * a.out_bstride + (long long)a.out_slot[blockIdx.y] * a.npts;
+    long long base, s;
+    int L;
+    bool valid;
     if (XD) {
-        // the tile's 32 x-lines are one contiguous run of nvalid*N doubles
-        L0 = blockIdx.x * kTileLines;
-        nvalid = min(kTileLines, a.nlines - L0);
-        base = (long long)L0 * N;
-        const double *__restrict__ src = F + base;
-        const int total = nvalid * N;
-        int l = 0, n = lane;
-        while (n >= N) { n -= N; l++; }
-        for (int i0 = 0; i0 < total; i0 += 32 * kChunk) {
-            double v[kChunk];
-#pragma unroll
-            for (int u = 0; u < kChunk; u++) {
-                const int idx = i0 + u * 32 + lane;
-                v[u] = idx < total ? src[idx] : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < kChunk; u++) {
-                if (i0 + u * 32 + lane < total) T[n * kPad + l] = v[u];
-                n += 32;
-                while (n >= N) { n -= N; l++; }
-            }
-        }
+        L = blockIdx.x * kLanes + lane;
+        valid = L < a.nlines;
+        base = (long long)L * N;
+        s = 1;
     } else {
         const int o = blockIdx.x / a.tiles_per_row;
-        const int i0 = (blockIdx.x % a.tiles_per_row) * kTileLines;
-        nvalid = min(kTileLines, a.nx - i0);
-        base = i0 + (long long)o * a.os;
-        L0 = i0 + a.nx * o;
-        if (lane < nvalid) {
-            const double *__restrict__ src = F + base + lane;
-            for (int n0 = 0; n0 < N; n0 += kChunk) {
-                double v[kChunk];
+        const int i = (blockIdx.x % a.tiles_per_row) * kLanes + lane;
+        valid = i < a.nx;
+        base = i + (long long)o * a.os;
+        s = a.es;
+        L = i + a.nx * o;
+    }
+    double *col = T + lane;
+    double *halo = T + (size_t)N * kLanes + (size_t)p * (NR - 1) * kLanes + lane;   // this block's right halo
+    double *xch = T + ((size_t)N + (size_t)P * (NR - 1)) * kLanes + lane;           // [3][P] (stride 32)
+    const double *Fl = F + base;
+    double *Gl = G + base;
+    const bool vec = XD && (N % 4 == 0);
+
+    // ---- 0. load the tile -------------------------------------------------------------
+    if (valid) {
+        if (vec) {
+            // lane streams its own line in 32-byte pieces, 4 pieces in flight
+            const int nj = N / 4;
+            int j = p;
+            for (; j + 3 * P < nj; j += 4 * P) {
+                double v[4][4];
 #pragma unroll
-                for (int u = 0; u < kChunk; u++) v[u] = (n0 + u < N) ? src[(long long)(n0 + u) * a.es] : 0.0;
+                for (int u = 0; u < 4; u++) ld4_stream(Fl + 4 * (j + u * P), v[u]);
 #pragma unroll
-                for (int u = 0; u < kChunk; u++)
-                    if (n0 + u < N) T[(n0 + u) * kPad + lane] = v[u];
+                for (int u = 0; u < 4; u++) {
+                    double *dst = col + 4 * (j + u * P) * kLanes;
+                    dst[0] = v[u][0]; dst[kLanes] = v[u][1]; dst[2 * kLanes] = v[u][2]; dst[3 * kLanes] = v[u][3];
+                }
+            }
+            for (; j < nj; j += P) {
+                double v[4];
+                ld4_stream(Fl + 4 * j, v);
+                double *dst = col + 4 * j * kLanes;
+                dst[0] = v[0]; dst[kLanes] = v[1]; dst[2 * kLanes] = v[2]; dst[3 * kLanes] = v[3];
+            }
+        } else {
+            // one coalesced row per warp access, 16 rows in flight per lane
+            const long long step = (long long)P * s;
+            int n = p;
+            for (; n + 15 * P < N; n += 16 * P) {
+                double v[16];
+                const double *src = Fl + (long long)n * s;
+#pragma unroll
+                for (int u = 0; u < 16; u++) v[u] = XD ? src[u * step] : ld_stream(src + u * step);
+#pragma unroll
+                for (int u = 0; u < 16; u++) col[(n + u * P) * kLanes] = v[u];
+            }
+            for (; n < N; n += P) col[n * kLanes] = XD ? Fl[n] : ld_stream(Fl + (long long)n * s);
+        }
+    }
+    // coefficient staging: one copy of the tile's matrix type when every line shares it
+    __shared__ int s_uniform;
+    const int t = valid ? a.ltype[L] : -1;
+    if (threadIdx.x < 32) {
+        const int t0 = __shfl_sync(0xffffffffu, t, 0);
+        const bool same = __all_sync(0xffffffffu, t == t0 || t < 0);
+        if (lane == 0) s_uniform = same ? t0 : -1;
+    }
+    __syncthreads();
+    const int tu = s_uniform;
+    double *sR = T + ((size_t)N + (size_t)P * (NR - 1) + 3 * (size_t)P) * kLanes;
+    double *sQ = sR + (size_t)N * Wp;
+    const int sp = block_start(p, N, P), ep = block_start(p + 1, N, P) - 1;
+    const double *Rm, *Q;
+    if (tu >= 0) {
+        // each warp copies the records of its own rows
+        const double *gR = a.Rm + ((size_t)tu * N + sp) * Wp;
+        const double *gQ = a.Q + ((size_t)tu * N + sp) * kQ;
+        const int nR4 = (ep - sp + 1) * Wp / 4, nQ4 = (ep - sp + 1) * kQ / 4;
+        for (int k = lane; k < nR4; k += kLanes) {
+            double v[4];
+            ld4_coef(gR + 4 * k, v);
+            double *d = sR + (size_t)sp * Wp + 4 * k;
+            d[0] = v[0]; d[1] = v[1]; d[2] = v[2]; d[3] = v[3];
+        }
+        for (int k = lane; k < nQ4; k += kLanes) {
+            double v[4];
+            ld4_coef(gQ + 4 * k, v);
+            double *d = sQ + (size_t)sp * kQ + 4 * k;
+            d[0] = v[0]; d[1] = v[1]; d[2] = v[2]; d[3] = v[3];
+        }
+        Rm = sR;
+        Q = sQ;
+        // other blocks' rows (cyclic corner terms in row 0, block-boundary propagators) are
+        // read by every warp: wait for all warps' copies
+        __syncthreads();
+    } else {
+        __syncthreads();
+        Rm = a.Rm + (size_t)(t < 0 ? 0 : t) * N * Wp;
+        Q = a.Q + (size_t)(t < 0 ? 0 : t) * N * kQ;
+    }
+
+    // ---- 1. halos, band product, forward recurrence ----------------------------------
+    // window w = F(i-NR+1 .. i+NR-1).  Left halo -> registers, right halo -> the block's
+    // shared halo rows; both are read before the barrier after which rows are overwritten.
+    double w[W];
+#pragma unroll
+    for (int k = 0; k < NR - 1; k++) {
+        int r = sp - (NR - 1) + k;
+        r += r < 0 ? N : 0;
+        w[k] = col[r * kLanes];
+        int r2 = ep + 1 + k;
+        r2 -= r2 >= N ? N : 0;
+        const double hv = col[r2 * kLanes];
+        __syncwarp();
+        halo[k * kLanes] = hv;
+    }
+#pragma unroll
+    for (int k = 0; k < NR; k++) w[NR - 1 + k] = col[(sp + k) * kLanes];
+    __syncthreads();
+
+    double yprev = 0.0, dot = 0.0;
+    const double *rp = Rm + (size_t)sp * Wp;
+    const double *qp = Q + (size_t)sp * kQ;
+    double *cp = col + sp * kLanes;
+    int i = sp;
+    // full chunks: every incoming row i+NR is a row of this block (i + NR <= ep)
+    const int nfull = (ep - NR + 1 - sp) / RB;
+    for (int c = 0; c < nfull; c++) {
+        double rc[RB][NV * 4], qc[RB][4], inc[RB];
+#pragma unroll
+        for (int u = 0; u < RB; u++) {
+            const double2 *r2 = reinterpret_cast<const double2 *>(rp + u * Wp);
+#pragma unroll
+            for (int v = 0; v < NV * 2; v++) { const double2 x = r2[v]; rc[u][2 * v] = x.x; rc[u][2 * v + 1] = x.y; }
+            const double2 *q2 = reinterpret_cast<const double2 *>(qp + u * kQ);
+            const double2 qa = q2[0], qb = q2[1];
+            qc[u][0] = qa.x; qc[u][1] = qa.y; qc[u][2] = qb.x; qc[u][3] = qb.y;
+            inc[u] = cp[(u + NR) * kLanes];
+        }
+#pragma unroll
+        for (int u = 0; u < RB; u++) {
+            double acc = rc[u][NR - 1] * w[NR - 1];
+#pragma unroll
+            for (int l = 1; l < NR; l++) acc = acc + rc[u][NR - 1 + l] * w[NR - 1 + l] + rc[u][NR - 1 - l] * w[NR - 1 - l];
+            if (!PER) {
+                const double y = (acc - qc[u][kQfA] * yprev) * qc[u][kQfB];
+                cp[u * kLanes] = y;
+                yprev = y;
+            } else {
+                cp[u * kLanes] = acc;
+                dot = (i + u == sp) ? acc * qc[u][kQD] : dot + acc * qc[u][kQD];
+            }
+#pragma unroll
+            for (int k = 0; k < W - 1; k++) w[k] = w[k + 1];
+            w[W - 1] = inc[u];
+        }
+        rp += RB * Wp; qp += RB * kQ; cp += RB * kLanes; i += RB;
+    }
+    // tail rows: the incoming row may come from the right halo
+    for (; i <= ep; i++, rp += Wp, qp += kQ, cp += kLanes) {
+        double rc[NV * 4], qc[4];
+        {
+            const double2 *r2 = reinterpret_cast<const double2 *>(rp);
+#pragma unroll
+            for (int v = 0; v < NV * 2; v++) { const double2 x = r2[v]; rc[2 * v] = x.x; rc[2 * v + 1] = x.y; }
+            const double2 *q2 = reinterpret_cast<const double2 *>(qp);
+            const double2 qa = q2[0], qb = q2[1];
+            qc[0] = qa.x; qc[1] = qa.y; qc[2] = qb.x; qc[3] = qb.y;
+        }
+        const int r = i + NR;
+        const double inc = r <= ep ? cp[NR * kLanes] : (r - ep - 1 < NR - 1 ? halo[(r - ep - 1) * kLanes] : 0.0);
+        double acc = rc[NR - 1] * w[NR - 1];
+#pragma unroll
+        for (int l = 1; l < NR; l++) acc = acc + rc[NR - 1 + l] * w[NR - 1 + l] + rc[NR - 1 - l] * w[NR - 1 - l];
+        if (!PER) {
+            const double y = (acc - qc[kQfA] * yprev) * qc[kQfB];
+            *cp = y;
+            yprev = y;
+        } else {
+            *cp = acc;
+            dot = (i == sp) ? acc * qc[kQD] : dot + acc * qc[kQD];
+        }
+#pragma unroll
+        for (int k = 0; k < W - 1; k++) w[k] = w[k + 1];
+        w[W - 1] = inc;
+    }
+
+    int r0 = sp;  // first row of this block in the recurrences (cyclic block 0 starts at row 1)
+    if (PER) {
+        xch[(2 * P + p) * kLanes] = dot;
+        __syncthreads();
+        // ---- 2. x(1) = D . rhs and the reduced forward recurrence (derivs.F90:786-799)
+        double x1 = xch[(2 * P) * kLanes];
+        for (int k = 1; k < P; k++) x1 = x1 + xch[(2 * P + k) * kLanes];
+        if (p == 0) r0 = 1;
+        const double cA = Q[kQcA], cC = Q[kQcC];
+        // rows 1 and N-1 carry the corner terms (derivs.F90:792-793)
+        if (r0 == 1) col[kLanes] = col[kLanes] - cA * x1;
+        if (ep == N - 1) col[(N - 1) * kLanes] = col[(N - 1) * kLanes] - cC * x1;
+        yprev = 0.0;
+        const double *qq = Q + (size_t)r0 * kQ;
+        double *cc = col + r0 * kLanes;
+        int r = r0;
+        for (; r + kCh - 1 <= ep; r += kCh, qq += kCh * kQ, cc += kCh * kLanes) {
+            double qv[kCh][4], g[kCh];
+#pragma unroll
+            for (int u = 0; u < kCh; u++) {
+                const double2 ab = *reinterpret_cast<const double2 *>(qq + u * kQ + kQfA);
+                qv[u][kQfA] = ab.x;
+                qv[u][kQfB] = ab.y;
+                g[u] = cc[u * kLanes];
+            }
+#pragma unroll
+            for (int u = 0; u < kCh; u++) {
+                const double y = (g[u] - qv[u][kQfA] * yprev) * qv[u][kQfB];
+                cc[u * kLanes] = y;
+                yprev = y;
             }
         }
-    }
-    __syncwarp();
-    if (lane < nvalid) {
-        double *col = T + lane;
-        // wrap rows for the band product
-#pragma unroll
-        for (int q = 0; q < NR - 1; q++) col[(N + q) * kPad] = col[q * kPad];
-        const int t = a.ltype[L0 + lane];
-        const size_t co = (size_t)t * N;
-        solve_column<PER, NR>(col, N, a.R + co * a.W, a.A + co, a.B + co, a.C + co, PER ? a.D + co : nullptr);
-    }
-    __syncwarp();
-    const double blend = (EPI == EPI_BLEND) ? sweep_blend(a) : 0.0;
-    if (XD) {
-        double *dst = G + base;
-        const double *src = F + base;
-        const int total = nvalid * N;
-        int l = 0, n = lane;
-        while (n >= N) { n -= N; l++; }
-        for (int idx = lane; idx < total; idx += 32) {
-            double v = T[n * kPad + l];
-            if (EPI == EPI_BLEND) { const double o = src[idx]; v = o + blend * (v - o); }
-            dst[idx] = v;
-            n += 32;
-            while (n >= N) { n -= N; l++; }
+        for (; r <= ep; r++, qq += kQ, cc += kLanes) {
+            const double y = (*cc - qq[kQfA] * yprev) * qq[kQfB];
+            *cc = y;
+            yprev = y;
         }
-    } else if (lane < nvalid) {
-        double *dst = G + base + lane;
-        const double *src = F + base + lane;
-#pragma unroll 8
-        for (int n = 0; n < N; n++) {
-            double v = T[n * kPad + lane];
-            if (EPI == EPI_BLEND) { const double o = src[(long long)n * a.es]; v = o + blend * (v - o); }
-            dst[(long long)n * a.es] = v;
+        if (p == 0) col[0] = x1;
+    }
+    xch[p * kLanes] = yprev;
+    __syncthreads();
+
+    // ---- 3. prefix, correction, backward recurrence ---------------------------------
+    double Y = 0.0;
+    for (int k = 0; k < p; k++) Y = xch[k * kLanes] + Q[(size_t)(block_start(k + 1, N, P) - 1) * kQ + kQpi] * Y;
+    double xprev = 0.0;
+    {
+        const double *qq = Q + (size_t)ep * kQ;
+        double *cc = col + ep * kLanes;
+        int r = ep;
+        for (; r - kCh + 1 >= r0; r -= kCh, qq -= kCh * kQ, cc -= kCh * kLanes) {
+            double bc[kCh], pi[kCh], g[kCh];
+#pragma unroll
+            for (int u = 0; u < kCh; u++) {
+                bc[u] = qq[-u * kQ + kQbC];
+                pi[u] = qq[-u * kQ + kQpi];
+                g[u] = cc[-u * kLanes];
+            }
+#pragma unroll
+            for (int u = 0; u < kCh; u++) {
+                const double y = g[u] + pi[u] * Y;  // Y = 0 in the first block
+                const double x = y - bc[u] * xprev;
+                cc[-u * kLanes] = x;
+                xprev = x;
+            }
+        }
+        for (; r >= r0; r--, qq -= kQ, cc -= kLanes) {
+            const double y = *cc + qq[kQpi] * Y;
+            const double x = y - qq[kQbC] * xprev;
+            *cc = x;
+            xprev = x;
+        }
+    }
+    xch[(P + p) * kLanes] = xprev;
+    __syncthreads();
+
+    // ---- 4. suffix, correction, store --------------------------------------------------
+    double X = 0.0;
+    for (int k = P - 1; k > p; k--) X = xch[(P + k) * kLanes] + Q[(size_t)block_start(k, N, P) * kQ + kQrho] * X;
+    if (!valid) return;
+    const bool blend_on = a.epi == EPI_BLEND;
+    const double blend = blend_on ? sweep_blend(a) : 0.0;
+    const double *qq = Q + (size_t)sp * kQ + kQrho;  // X = 0 in the last block
+    const double *cc = col + sp * kLanes;
+    if (vec && (sp % 4 == 0) && ((ep + 1) % 4 == 0)) {
+        for (int r = sp; r <= ep; r += 4, qq += 4 * kQ, cc += 4 * kLanes) {
+            double v[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) v[k] = cc[k * kLanes] + qq[k * kQ] * X;
+            if (PER && r == 0) v[0] = cc[0];  // x(1) is final
+            if (blend_on) {
+                double o[4];
+                ld4_stream(Fl + r, o);
+#pragma unroll
+                for (int k = 0; k < 4; k++) v[k] = o[k] + blend * (v[k] - o[k]);
+            }
+            st4(Gl + r, v);
+        }
+    } else {
+        double *gp = Gl + (long long)sp * s;
+        const double *fp = Fl + (long long)sp * s;
+#pragma unroll 4
+        for (int r = sp; r <= ep; r++, qq += kQ, cc += kLanes, gp += s, fp += s) {
+            double v = (PER && r == 0) ? *cc : *cc + (*qq) * X;
+            if (blend_on) { const double o = *fp; v = o + blend * (v - o); }
+            *gp = v;
         }
     }
 }
 
-// Fallback for lines too long for the shared tile: one thread per line, band product
-// written straight to the output and the Thomas recurrences run in place there.
-// Requires in != out.
+// Fallback for lines too long for the shared tile (N > ~850) or band widths without an
+// instantiation: one thread per line in the reference order, band product written to the
+// output and the recurrences run in place there.  Requires in != out.
 template <bool PER>
 __global__ void k_sweep_global(const SweepArgs a, int nR)
 {
@@ -226,10 +447,11 @@ __global__ void k_sweep_global(const SweepArgs a, int nR)
         base = i + (long long)o * a.os; s = a.es;
     }
     const int t = a.ltype[L];
-    const double *Rt = a.R + (size_t)t * N * a.W;
-    const double *At = a.A + (size_t)t * N, *Bt = a.B + (size_t)t * N, *Ct = a.C + (size_t)t * N;
+    const double *Rt = a.Rm + (size_t)t * N * a.Wp;
+    const double *Q = a.Q + (size_t)t * N * kQ;
+    auto q = [&](int r, int fld) { return Q[(size_t)r * kQ + fld]; };
     for (int i = 0; i < N; i++) {
-        const double *Ri = Rt + (size_t)i * a.W;
+        const double *Ri = Rt + (size_t)i * a.Wp;
         double acc = Ri[nR - 1] * F[base + (long long)i * s];
         for (int l = 1; l < nR; l++) {
             int ip = i + l; ip -= (ip >= N) ? N : 0;
@@ -239,24 +461,20 @@ __global__ void k_sweep_global(const SweepArgs a, int nR)
         G[base + (long long)i * s] = acc;
     }
     double *g = G + base;
-    if (!PER) {
-        double d = g[0] * Bt[0];
-        g[0] = d;
-        for (int i = 0; i < N - 1; i++) { d = (g[(i + 1) * s] - At[i] * d) * Bt[i + 1]; g[(i + 1) * s] = d; }
-        for (int i = N - 2; i >= 0; i--) { d = g[i * s] - Ct[i] * d; g[i * s] = d; }
-    } else {
-        const double *Dt = a.D + (size_t)t * N;
-        double x1 = g[0] * Dt[0];
-        for (int i = 1; i < N; i++) x1 = x1 + g[i * s] * Dt[i];
+    int r0 = 0;
+    if (PER) {
+        double x1 = g[0] * q(0, kQD);
+        for (int i = 1; i < N; i++) x1 = x1 + g[i * s] * q(i, kQD);
         g[0] = x1;
-        double d = (g[s] - At[0] * x1) * Bt[0];
-        g[(N - 1) * s] = g[(N - 1) * s] - Ct[0] * x1;
-        g[s] = d;
-        for (int i = 1; i < N - 1; i++) { d = (g[(i + 1) * s] - At[i] * d) * Bt[i]; g[(i + 1) * s] = d; }
-        d = g[(N - 1) * s];
-        for (int i = N - 2; i >= 1; i--) { d = g[i * s] - Ct[i] * d; g[i * s] = d; }
+        g[s] = g[s] - q(0, kQcA) * x1;
+        g[(N - 1) * s] = g[(N - 1) * s] - q(0, kQcC) * x1;
+        r0 = 1;
     }
-    const double blend = sweep_blend(a);
+    double y = 0.0;
+    for (int r = r0; r < N; r++) { y = (g[r * s] - q(r, kQfA) * y) * q(r, kQfB); g[r * s] = y; }
+    double x = 0.0;
+    for (int r = N - 1; r >= r0; r--) { x = g[r * s] - q(r, kQbC) * x; g[r * s] = x; }
+    const double blend = a.epi == EPI_BLEND ? sweep_blend(a) : 0.0;
     if (blend > 0) {
         for (int i = 0; i < N; i++) {
             const double o = F[base + (long long)i * s];
