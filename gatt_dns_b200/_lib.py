@@ -51,6 +51,7 @@ SIGNATURES = {
     "gatt_kernel_launches": (ctypes.c_longlong, [_c_void_p]),
     "gatt_profile_kernels": (_c_int, [_c_void_p, _c_double, _c_double, _c_int, _pd, _pd]),
     "gatt_profile_name": (ctypes.c_char_p, [_c_int]),
+    "gatt_max_change_noalloc": (_c_int, [_c_int, _c_int, ctypes.c_longlong, _pp, _pp, _pd, _c_void_p]),
 }
 
 _lib = None

@@ -200,9 +200,9 @@ FieldSet fset(const gatt_ctx *c, double *p, int nslots)
     return f;
 }
 
-int nd1(const gatt_ctx *c) { return c->is3d ? D3_N : D2_N; }
-int ntq(const gatt_ctx *c) { return c->is3d ? T3_N : T2_N; }
-int nd2(const gatt_ctx *c) { return c->is3d ? S3_N : S2_N; }
+int nd1(const gatt_ctx *c) { return c->is3d ? (int)D3_N : (int)D2_N; }
+int ntq(const gatt_ctx *c) { return c->is3d ? (int)T3_N : (int)T2_N; }
+int nd2(const gatt_ctx *c) { return c->is3d ? (int)S3_N : (int)S2_N; }
 
 // ---------------------------------------------------------------------------
 // line-solve dispatch
@@ -710,6 +710,32 @@ int check_member(const gatt_ctx *c, int b)
 {
     if (!c) return fail(GATT_ERR_BADARG, "null context");
     if (b < 0 || b >= c->nb) return fail(GATT_ERR_BADARG, "batch member out of range");
+    return GATT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// allocation-free max-change: the accumulators live in a file-scope device array
+// ---------------------------------------------------------------------------
+
+// Every GPU that loads this library holds this array (2560 bytes) until the process
+// exits.  Host code must not pass the symbol itself to a kernel: it names a host-side
+// stand-in.  The device address comes from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned long long g_noalloc_maxchange[kMaxChangeSlots];
+
+constexpr int kMaxDevices = 64;
+unsigned long long *g_noalloc_ptr[kMaxDevices] = {};
+
+int noalloc_scratch(unsigned long long **out)
+{
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(GATT_ERR_BADARG, "device ordinal beyond the supported range");
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        CU(cudaGetSymbolAddress(&p, g_noalloc_maxchange));
+        g_noalloc_ptr[dev] = static_cast<unsigned long long *>(p);
+    }
+    *out = g_noalloc_ptr[dev];
     return GATT_OK;
 }
 
@@ -1237,6 +1263,39 @@ int gatt_synchronize(gatt_ctx *c)
 }
 
 long long gatt_kernel_launches(gatt_ctx *c) { return c ? c->launches : -1; }
+
+int gatt_max_change_noalloc(int nsets, int nvar, long long n, const double *const *a, const double *const *b,
+                            double *maxChange, void *stream)
+{
+    if (nsets < 1 || nvar < 1 || nvar > 5 || n < 1 || !a || !b || !maxChange)
+        return fail(GATT_ERR_BADARG, "gatt_max_change_noalloc: need nsets >= 1, 1 <= nvar <= 5, n >= 1 and all arrays");
+    if ((long long)nsets * nvar > kMaxChangeSlots)
+        return fail(GATT_ERR_BADARG, "gatt_max_change_noalloc: nsets*nvar exceeds the " + std::to_string(kMaxChangeSlots) +
+                                         " accumulators of its static scratch");
+    PtrSets ps;
+    for (int k = 0; k < nsets * nvar; k++) {
+        if (!a[k] || !b[k]) return fail(GATT_ERR_BADARG, "gatt_max_change_noalloc: null field pointer");
+        ps.a[k] = a[k];
+        ps.b[k] = b[k];
+    }
+    unsigned long long *acc = nullptr;
+    TRY(noalloc_scratch(&acc));
+    cudaStream_t st = (cudaStream_t)stream;
+    // the array keeps the previous call's maxima: start this call from zero
+    CU(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * nsets * nvar, st));
+    int dev = 0, nsm = 148;
+    CU(cudaGetDevice(&dev));
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    long long g = (n + kBlock - 1) / kBlock;
+    if (g > (long long)nsm * 8) g = (long long)nsm * 8;
+    k_maxchange_sets<<<dim3((unsigned)g, nsets), kBlock, 0, st>>>(ps, nvar, acc, n);
+    CU(cudaGetLastError());
+    unsigned long long h[kMaxChangeSlots];
+    CU(cudaMemcpyAsync(h, acc, sizeof(unsigned long long) * nsets * nvar, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    for (int k = 0; k < nsets * nvar; k++) memcpy(&maxChange[k], &h[k], sizeof(double));
+    return GATT_OK;
+}
 
 const char *gatt_profile_name(int cls) { return (cls >= 0 && cls < PC_N) ? kProfNames[cls] : nullptr; }
 

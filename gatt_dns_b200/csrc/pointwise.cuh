@@ -264,6 +264,33 @@ __global__ void k_maxchange(StateSet a, StateSet bset, unsigned long long *acc, 
     }
 }
 
+// Max-change over independent (a, b) pointer sets: set s, variable v compares
+// a[s*nvar+v] with b[s*nvar+v] over n points into acc[s*nvar+v] (blockIdx.y = set).
+// (160 slots = 32 sets of the 5 variables; the pointer table is a 2.5 KB kernel parameter)
+constexpr int kMaxChangeSlots = 160;
+struct PtrSets {
+    const double *a[kMaxChangeSlots];
+    const double *b[kMaxChangeSlots];
+};
+
+__global__ void k_maxchange_sets(PtrSets ps, int nvar, unsigned long long *acc, long long n)
+{
+    const int s = blockIdx.y;
+    for (int v = 0; v < nvar; v++) {
+        const double *a = ps.a[s * nvar + v], *b = ps.b[s * nvar + v];
+        unsigned long long m = 0;
+        for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+            const unsigned long long u = (unsigned long long)__double_as_longlong(fabs(a[p] - b[p]));
+            m = u > m ? u : m;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long w = __shfl_xor_sync(0xffffffffu, m, o);
+            m = w > m ? w : m;
+        }
+        if ((threadIdx.x & 31) == 0) atomicMax(acc + s * nvar + v, m);
+    }
+}
+
 // max|U|, max|V|, max|W| (main.F90:196-204), same bit trick
 __global__ void k_maxvel(StateSet a, unsigned long long *acc, long long n)
 {

@@ -224,5 +224,15 @@ module gatt_dns
             integer(c_int), value :: cls
             type(c_ptr) :: gatt_profile_name
         end function
+        function gatt_max_change_noalloc(nsets, nvar, n, a, b, maxChange, stream) &
+                bind(C, name='gatt_max_change_noalloc')
+            import :: c_int, c_ptr, c_double, c_long_long
+            integer(c_int), value :: nsets, nvar
+            integer(c_long_long), value :: n
+            type(c_ptr), dimension(*) :: a, b
+            real(c_double), dimension(*) :: maxChange
+            type(c_ptr), value :: stream
+            integer(c_int) :: gatt_max_change_noalloc
+        end function
     end interface
 end module gatt_dns
