@@ -6,16 +6,21 @@
 // into a device parameter block, so a step costs one small copy plus one graph launch.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/gatt_dns.h"
 #include "bc.cuh"
 #include "pointwise.cuh"
+#include "rsweep.cuh"
 #include "sweep.cuh"
 
 using namespace gatt;
@@ -44,9 +49,15 @@ int fail(int code, const std::string &msg)
         if (r_ != GATT_OK) return r_; \
     } while (0)
 
+// Line-solve kernel families: shared-memory tile (any N), register-resident rows loaded
+// from global memory, register-resident rows fed by a TMA ring (persistent CTAs).
+enum SweepFamily { FAM_TILE = 0, FAM_REG = 1, FAM_PIPE = 2 };
+
 struct DevDir {
     bool set = false;
     int periodic = 0, nR = 0, nTypes = 0, N = 0, W = 0, Wp = 0, P = 1;
+    int rpb = 0;           // rows per block of the register-resident solver (0: shared-tile solver)
+    int family = 0;        // SweepFamily
     double *Rm = nullptr;  // band coefficients [nTypes][N][Wp]
     double *Q = nullptr;   // row records [nTypes][N][kQ] (see sweep.cuh)
 };
@@ -122,6 +133,8 @@ struct gatt_ctx {
     int capture_count = 0;
     long long launches = 0;
     int nsm = 148;
+    int *h_err = nullptr;   // pipeline wait give-up flag (pinned, device-mapped)
+    int *d_err = nullptr;
     // per-kernel-class timing (gatt_profile_kernels): events around every launch
     bool profiling = false;
     int prof_cls = -1;
@@ -134,6 +147,17 @@ namespace {
 // ---------------------------------------------------------------------------
 // small helpers
 // ---------------------------------------------------------------------------
+
+// Synchronize the context's stream and report a line-solve pipeline that gave up waiting.
+int sync_stream(gatt_ctx *c)
+{
+    CU(cudaStreamSynchronize(c->stream));
+    if (c->h_err && *(volatile int *)c->h_err) {
+        *(volatile int *)c->h_err = 0;
+        return fail(GATT_ERR_TIMEOUT, "a line-solve copy pipeline gave up (tile wait timed out or misaligned ring)");
+    }
+    return GATT_OK;
+}
 
 int grid_for(const gatt_ctx *c, long long n)
 {
@@ -236,6 +260,82 @@ void *sweep_kernel(bool xd, bool per, int nR, bool big)
     return per ? pick_kernel<false, true, false>(nR) : pick_kernel<false, false, false>(nR);
 }
 
+// Register-resident solvers: 16-row blocks (32-row blocks spill registers for most bands).
+constexpr int kRPB = 16;
+
+template <bool XD, bool PER, bool PIPE>
+void *pick_reg_kernel(int nR)
+{
+#define GATT_REG_CASE(n) \
+    case n: return PIPE ? (void *)k_psweep<XD, PER, n, kRPB> : (void *)k_rsweep<XD, PER, n, kRPB>;
+    switch (nR) {
+    GATT_REG_CASE(2) GATT_REG_CASE(3) GATT_REG_CASE(4) GATT_REG_CASE(5) GATT_REG_CASE(6) GATT_REG_CASE(7)
+    default: return nullptr;
+    }
+#undef GATT_REG_CASE
+}
+
+void *reg_kernel(bool pipe, bool xd, bool per, int nR)
+{
+    if (pipe) {
+        if (xd) return per ? pick_reg_kernel<true, true, true>(nR) : pick_reg_kernel<true, false, true>(nR);
+        return per ? pick_reg_kernel<false, true, true>(nR) : pick_reg_kernel<false, false, true>(nR);
+    }
+    if (xd) return per ? pick_reg_kernel<true, true, false>(nR) : pick_reg_kernel<true, false, false>(nR);
+    return per ? pick_reg_kernel<false, true, false>(nR) : pick_reg_kernel<false, false, false>(nR);
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled()
+{
+    static EncodeTiledFn fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return (EncodeTiledFn)f;
+    }();
+    return fn;
+}
+
+// Resident CTAs per SM of a kernel at a block size and dynamic shared memory (cached).
+int resident_ctas(const void *k, int threads, size_t smem)
+{
+    static std::mutex mu;
+    static std::map<std::tuple<const void *, int, size_t>, int> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_tuple(k, threads, smem);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, threads, smem) != cudaSuccess) n = 0;
+    cache[key] = n;
+    return n;
+}
+
+// Line-solve family for new matrices: GATT_SWEEP = tile | reg | pipe (default pipe).
+int choose_family()
+{
+    const char *e = getenv("GATT_SWEEP");
+    if (e && strcmp(e, "tile") == 0) return FAM_TILE;
+    if (e && strcmp(e, "reg") == 0) return FAM_REG;
+    return FAM_PIPE;
+}
+
+// Block height of the register-resident solvers for lines of N rows and band nR, or 0 when
+// the shared-tile solver handles them (N not a multiple of kRPB, more than kMaxP blocks, or a
+// band wider than kMaxNRreg).
+int choose_rpb(int N, int nR)
+{
+    if (choose_family() == FAM_TILE) return 0;
+    if (nR < 2 || nR > kMaxNRreg) return 0;
+    return (N % kRPB == 0 && N / kRPB <= kMaxP) ? kRPB : 0;
+}
+
 size_t sweep_smem(int N, int P, int nR, int Wp) { return sweep_smem_doubles(N, P, nR, Wp) * sizeof(double); }
 // 227 KB per block, less a margin for the kernel's few static shared variables
 constexpr size_t kMaxSmem = 227 * 1024 - 256;
@@ -266,7 +366,55 @@ int set_sweep_attributes()
                     void *k = sweep_kernel(xd != 0, per != 0, nR, big != 0);
                     CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
                 }
+    for (int xd = 0; xd < 2; xd++)
+        for (int per = 0; per < 2; per++)
+            for (int nR = 2; nR <= kMaxNRreg; nR++) {
+                void *k = reg_kernel(true, xd != 0, per != 0, nR);
+                CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+                CU(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+            }
     return GATT_OK;
+}
+
+// Pipelined register solver: build the tensor map (y/z), size the persistent grid, launch.
+// Returns GATT_ERR_STATE (without launching) when the layout does not meet the copy engine's
+// alignment rules, so that the caller falls back to k_rsweep.
+int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmembers, int cls)
+{
+    const int N = m.N;
+    const bool xd = d == 0;
+    const size_t smem = psweep_smem_bytes(xd, N, m.P, m.nTypes, m.Wp);
+    void *k = reg_kernel(true, xd, m.periodic != 0, m.nR);
+    if (!k || smem > kMaxSmem) return GATT_ERR_STATE;
+    // 16-byte aligned field starts and line starts (bulk copies), even strides (tensor map)
+    if ((reinterpret_cast<uintptr_t>(a.in) & 15) || (c->npts & 1) || (a.in_bstride & 1)) return GATT_ERR_STATE;
+    CUtensorMap map;
+    memset(&map, 0, sizeof(map));
+    if (!xd) {
+        if (N > 256 || (c->nx & 1)) return GATT_ERR_STATE;
+        EncodeTiledFn enc = encode_tiled();
+        if (!enc) return GATT_ERR_STATE;
+        int nslots = 1;
+        for (int f = 0; f < a.nf; f++) nslots = std::max(nslots, a.in_slot[f] + 1);
+        const long long mstride = nmembers > 1 ? a.in_bstride : (long long)nslots * c->npts;
+        cuuint64_t dims[5] = {(cuuint64_t)c->nx, (cuuint64_t)c->ny, (cuuint64_t)c->nz, (cuuint64_t)nslots,
+                              (cuuint64_t)nmembers};
+        cuuint64_t strides[4] = {(cuuint64_t)c->nx * 8, (cuuint64_t)c->nx * c->ny * 8, (cuuint64_t)c->npts * 8,
+                                 (cuuint64_t)mstride * 8};
+        cuuint32_t box[5] = {(cuuint32_t)kLanes, (cuuint32_t)(d == 1 ? N : 1), (cuuint32_t)(d == 2 ? N : 1), 1, 1};
+        cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+        CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<double *>(a.in), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return GATT_ERR_STATE;
+    }
+    const int per_sm = resident_ctas(k, 32 * m.P, smem);
+    if (per_sm < 1) return GATT_ERR_STATE;
+    const int grid = std::min(a.njobs, per_sm * c->nsm);
+    void *args[] = {&a, &map};
+    TRY(before_launch(c, cls));
+    CU(cudaLaunchKernel(k, dim3(grid), dim3(32 * m.P), args, smem, c->stream));
+    return after_launch(c);
 }
 
 // Run one compact solve (direction d, coefficient kind) over nf fields.
@@ -293,8 +441,19 @@ int sweep(gatt_ctx *c, int d, int kind, const double *in, long long in_bs, const
     a.ltype = c->ltype[d];
     a.blend = blend; a.blend_dt = blend_dt; a.blend_fct = c->fct;
     a.epi = (blend_dt != nullptr || blend > 0) ? EPI_BLEND : EPI_STORE;
-    const size_t smem = sweep_smem(m.N, m.P, m.nR, m.Wp);
-    void *k = sweep_kernel(d == 0, m.periodic != 0, m.nR, m.P > 4);
+    a.dir = d;
+    a.nf = nf;
+    a.ntiles = d == 0 ? (a.nlines + kLanes - 1) / kLanes : a.tiles_per_row * (d == 1 ? c->nz : c->ny);
+    a.njobs = a.ntiles * nf * nmembers;
+    a.err = c->d_err;
+    a.ntypes = m.nTypes;
+    if (m.family == FAM_PIPE && m.rpb) {
+        int r = launch_psweep(c, m, d, a, nmembers, cls);
+        if (r != GATT_ERR_STATE) return r;  // GATT_ERR_STATE: layout not expressible, use k_rsweep
+    }
+    const size_t smem = m.rpb ? (size_t)3 * m.P * kLanes * sizeof(double) : sweep_smem(m.N, m.P, m.nR, m.Wp);
+    void *k = m.rpb ? reg_kernel(false, d == 0, m.periodic != 0, m.nR)
+                    : sweep_kernel(d == 0, m.periodic != 0, m.nR, m.P > 4);
     if (k && smem <= kMaxSmem && m.N >= 2) {
         dim3 grid(d == 0 ? (a.nlines + kLanes - 1) / kLanes
                          : a.tiles_per_row * (d == 1 ? c->nz : c->ny),
@@ -636,7 +795,7 @@ int ensure_hist(gatt_ctx *c, int n)
     if (n <= c->hist_cap) return GATT_OK;
     int cap = c->hist_cap ? c->hist_cap : 64;
     while (cap < n) cap *= 2;
-    CU(cudaStreamSynchronize(c->stream));
+    TRY(sync_stream(c));
     cudaFree(c->hist);
     cudaFreeHost(c->h_params);
     c->hist = nullptr; c->h_params = nullptr;
@@ -676,7 +835,7 @@ int run_steps(gatt_ctx *c, int nsteps, double t0, double dt, double *maxChange, 
     const int nv = 5 * c->nb;
     std::vector<double> h((size_t)nv * nsteps);
     CU(cudaMemcpyAsync(h.data(), c->hist, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
-    CU(cudaStreamSynchronize(c->stream));
+    TRY(sync_stream(c));
     if (maxChange) memcpy(maxChange, h.data() + (size_t)nv * (nsteps - 1), sizeof(double) * nv);
     // divergence test of main.F90:433-438, per member and step
     for (int s = check_each ? 0 : nsteps - 1; s < nsteps; s++)
@@ -800,6 +959,8 @@ int gatt_create(gatt_ctx **out, int nx, int ny, int nz, int nbatch)
         cudaError_t ea = cudaMalloc(&c->acc, sizeof(unsigned long long) * 5 * nbatch);
         if (ea == cudaSuccess) ea = cudaMalloc(&c->d_params, sizeof(StepParams));
         if (ea == cudaSuccess) ea = cudaMemsetAsync(c->d_params, 0, sizeof(StepParams), c->stream);
+        if (ea == cudaSuccess) ea = cudaHostAlloc(&c->h_err, sizeof(int), cudaHostAllocMapped);
+        if (ea == cudaSuccess) { *c->h_err = 0; ea = cudaHostGetDevicePointer(&c->d_err, c->h_err, 0); }
         if (ea != cudaSuccess) rc = fail(GATT_ERR_NOMEM, cudaGetErrorString(ea));
     }
     if (rc == GATT_OK) chk(set_sweep_attributes());
@@ -831,6 +992,7 @@ void gatt_destroy(gatt_ctx *c)
     for (double *p : bufs) cudaFree(p);
     cudaFree(c->d_ops); cudaFree(c->acc); cudaFree(c->d_params);
     if (c->h_params) cudaFreeHost(c->h_params);
+    if (c->h_err) cudaFreeHost(c->h_err);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -838,7 +1000,7 @@ void gatt_destroy(gatt_ctx *c)
 int gatt_set_stream(gatt_ctx *c, void *s)
 {
     if (!c) return fail(GATT_ERR_BADARG, "null context");
-    CU(cudaStreamSynchronize(c->stream));
+    TRY(sync_stream(c));
     if (c->own_stream) cudaStreamDestroy(c->stream);
     c->own_stream = false;
     c->stream = (cudaStream_t)s;
@@ -933,7 +1095,8 @@ int gatt_set_matrices(gatt_ctx *c, int dir, int kind, int periodic, int nRHS, in
     }
     // Kernel row records (sweep.cuh): the reference's factors in uniform row semantics
     // plus the block propagators of the partitioned recurrences (long double products).
-    const int P = choose_blocks(N, nRHS);
+    const int rpb = choose_rpb(N, nRHS);
+    const int P = rpb ? N / rpb : choose_blocks(N, nRHS);
     const int Wp = (W + 3) / 4 * 4;
     std::vector<double> hRm((size_t)nTypes * N * Wp, 0.0), hQ((size_t)nTypes * N * kQ, 0.0);
     for (int t = 0; t < nTypes; t++) {
@@ -969,7 +1132,7 @@ int gatt_set_matrices(gatt_ctx *c, int dir, int kind, int periodic, int nRHS, in
             }
         }
     }
-    CU(cudaStreamSynchronize(c->stream));
+    TRY(sync_stream(c));
     DevDir &m = c->mat[d][kind];
     cudaFree(m.Rm);
     cudaFree(m.Q);
@@ -978,7 +1141,9 @@ int gatt_set_matrices(gatt_ctx *c, int dir, int kind, int periodic, int nRHS, in
     CU(cudaMalloc(&m.Q, hQ.size() * sizeof(double)));
     CU(cudaMemcpy(m.Rm, hRm.data(), hRm.size() * sizeof(double), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(m.Q, hQ.data(), hQ.size() * sizeof(double), cudaMemcpyHostToDevice));
-    m.periodic = periodic; m.nR = nRHS; m.nTypes = nTypes; m.N = N; m.W = W; m.Wp = Wp; m.P = P; m.set = true;
+    m.periodic = periodic; m.nR = nRHS; m.nTypes = nTypes; m.N = N; m.W = W; m.Wp = Wp; m.P = P; m.rpb = rpb;
+    m.family = rpb ? choose_family() : FAM_TILE;
+    m.set = true;
     if (nBlocks > 0) {
         if (!c->ltype[d]) CU(cudaMalloc(&c->ltype[d], lt.size()));
         CU(cudaMemcpy(c->ltype[d], lt.data(), lt.size(), cudaMemcpyHostToDevice));
@@ -1103,7 +1268,7 @@ static int copy_state(gatt_ctx *c, int b, int which, double *const *host, bool u
         if (up) CU(cudaMemcpyAsync(dp, host[f], sizeof(double) * c->npts, cudaMemcpyHostToDevice, c->stream));
         else CU(cudaMemcpyAsync(host[f], dp, sizeof(double) * c->npts, cudaMemcpyDeviceToHost, c->stream));
     }
-    CU(cudaStreamSynchronize(c->stream));
+    TRY(sync_stream(c));
     return GATT_OK;
 }
 
@@ -1129,7 +1294,7 @@ static int copy_mean(gatt_ctx *c, int b, double *const *host, bool up)
         if (up) CU(cudaMemcpyAsync(dp, host[f], sizeof(double) * c->npts, cudaMemcpyHostToDevice, c->stream));
         else CU(cudaMemcpyAsync(host[f], dp, sizeof(double) * c->npts, cudaMemcpyDeviceToHost, c->stream));
     }
-    CU(cudaStreamSynchronize(c->stream));
+    TRY(sync_stream(c));
     return GATT_OK;
 }
 
@@ -1176,7 +1341,7 @@ int gatt_apply_bc(gatt_ctx *c, double t)
     if (!c) return fail(GATT_ERR_BADARG, "null context");
     if (!c->phys_set) return fail(GATT_ERR_STATE, "gatt_set_physics not called");
     TRY(apply_bc(c, state_set(c, 0), c->nb));
-    CU(cudaStreamSynchronize(c->stream));
+    TRY(sync_stream(c));
     return GATT_OK;
 }
 
@@ -1190,7 +1355,7 @@ int gatt_deriv_dir(gatt_ctx *c, int dir, int kind, const double *F, double *dF)
     const int s0 = 0;
     TRY(sweep(c, dir - 1, kind, c->tin, 0, &s0, c->tout, 0, &s0, 1, 1, 0.0, nullptr));
     CU(cudaMemcpyAsync(dF, c->tout, sizeof(double) * c->npts, cudaMemcpyDeviceToHost, c->stream));
-    CU(cudaStreamSynchronize(c->stream));
+    TRY(sync_stream(c));
     return GATT_OK;
 }
 
@@ -1216,7 +1381,7 @@ int gatt_rhs(gatt_ctx *c, const double *U, const double *V, const double *W, con
         if (!out[f] || (!c->is3d && f == 2)) continue;
         CU(cudaMemcpyAsync(out[f], c->tout + f * c->npts, sizeof(double) * c->npts, cudaMemcpyDeviceToHost, c->stream));
     }
-    CU(cudaStreamSynchronize(c->stream));
+    TRY(sync_stream(c));
     return GATT_OK;
 }
 
@@ -1225,7 +1390,7 @@ int gatt_filter(gatt_ctx *c, double blend)
     if (!c) return fail(GATT_ERR_BADARG, "null context");
     TRY(check_ready(c, true));
     TRY(filter_set(c, state_set(c, 0), c->nb, blend > 0 ? blend : 0.0, nullptr));
-    CU(cudaStreamSynchronize(c->stream));
+    TRY(sync_stream(c));
     return GATT_OK;
 }
 
@@ -1250,7 +1415,7 @@ int gatt_max_velocity(gatt_ctx *c, double *vmax)
     TRY(after_launch(c));
     std::vector<unsigned long long> h(3 * c->nb);
     CU(cudaMemcpyAsync(h.data(), c->acc, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost, c->stream));
-    CU(cudaStreamSynchronize(c->stream));
+    TRY(sync_stream(c));
     for (size_t i = 0; i < h.size(); i++) memcpy(&vmax[i], &h[i], sizeof(double));
     return GATT_OK;
 }
@@ -1258,7 +1423,7 @@ int gatt_max_velocity(gatt_ctx *c, double *vmax)
 int gatt_synchronize(gatt_ctx *c)
 {
     if (!c) return fail(GATT_ERR_BADARG, "null context");
-    CU(cudaStreamSynchronize(c->stream));
+    TRY(sync_stream(c));
     return GATT_OK;
 }
 
@@ -1314,7 +1479,7 @@ int gatt_profile_kernels(gatt_ctx *c, double t0, double dt, int nsteps, double *
         c->profiling = true;
         rc = step_body(c);
         c->profiling = false;
-        CU(cudaStreamSynchronize(c->stream));
+        TRY(sync_stream(c));
         size_t q = 0;
         for (size_t i = 0; i < c->ev_cls.size(); i++, q += 2) {
             float e = 0;

@@ -1,0 +1,461 @@
+// Register-resident compact line solves for sm_100a: the fast forms of
+// solveSystem{X,Y,Z}[per] (reference source/Fortran/derivs.F90:556-948) for lines whose
+// length N is a multiple of the block height RPB (16 rows).
+//
+// Same algorithm and row records as k_sweep (sweep.cuh): band product, forward and backward
+// Thomas recurrences, cut into P = N / RPB row blocks that run from zero start values and
+// are recombined with the coefficient-only propagators pi / rho.  The difference is where
+// the line lives: each thread keeps its RPB rows (plus NR-1 halo rows either side) in
+// registers for the whole solve, and shared memory carries only the per-block boundary
+// values (3*P*32 doubles).  Register slot k holds row p*RPB - (NR-1) + k before the band
+// pass and row p*RPB + k after it; every register index is a compile-time constant.
+//
+// Two kernels feed the registers:
+//  * k_rsweep: one tile per CTA, rows loaded straight from global memory (halo rows are
+//    the neighbouring block's rows, L2 hits);
+//  * k_psweep: persistent CTAs with a two-stage shared-memory ring filled by the Tensor
+//    Memory Accelerator -- one cp.async.bulk.tensor box {32 x N} per y/z tile (it lands
+//    as [row][lane]) or 32 one-dimensional cp.async.bulk line copies per x tile -- so the
+//    next tile streams in while the current one is solved from registers and stored.
+//    The coefficient records of all line types are copied to shared memory once per CTA.
+//    Every mbarrier wait is bounded; a wait that gives up sets *err and the CTA returns.
+#pragma once
+
+#include <cuda.h>
+#include "sweep.cuh"
+
+namespace gatt {
+
+// Largest band half-width + 1 the register kernels are instantiated for.
+constexpr int kMaxNRreg = 7;
+// Shared-memory ring depth of k_psweep.
+constexpr int kStages = 2;
+// Longest mbarrier wait (ns) before a pipeline gives up.
+constexpr unsigned long long kWaitNs = 1000000000ull;
+
+// Shared memory of k_psweep in bytes: kStages tiles, the block exchange, the coefficient
+// records of every line type (band rows [nTypes][N][Wp], records [nTypes][N][kQ]), the
+// mbarriers.
+__host__ __device__ __forceinline__ size_t psweep_stage_doubles(bool xd, int N)
+{
+    return xd ? (size_t)kLanes * (N + 2) : (size_t)N * kLanes;
+}
+__host__ __device__ __forceinline__ size_t psweep_smem_bytes(bool xd, int N, int P, int ntypes, int Wp)
+{
+    return (kStages * psweep_stage_doubles(xd, N) + 3 * (size_t)P * kLanes + (size_t)ntypes * N * (Wp + kQ)) *
+               sizeof(double) +
+           kStages * 8;
+}
+
+// Coefficient load: read-only data path (global records) or plain (shared-memory copy).
+template <bool LDG, typename T>
+__device__ __forceinline__ T ldc(const T *p)
+{
+    if constexpr (LDG) return __ldg(p);
+    else return *p;
+}
+
+// ---- PTX helpers: mbarrier, bulk / tensor copies -----------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred q;\n mbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\n selp.u32 %0, 1, 0, q;\n}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for the phase with the given parity to complete; false after kWaitNs.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigned long long limit_ns = kWaitNs)
+{
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try(bar, parity))
+        if (global_ns() - t0 > limit_ns) return false;
+    return true;
+}
+
+// 5-D tiled tensor load (no multicast) completing on an mbarrier.
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            int c4, uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(bar)
+        : "memory");
+}
+
+// Contiguous global -> shared copy (16-byte aligned ends, size a multiple of 16).
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// ---- the solve of one row block from registers -------------------------------------------
+// On entry w[k] = row p*RPB - (NR-1) + k of this thread's line; on return w[j] (j < RPB) =
+// the solution at row p*RPB + j.  Every thread of the CTA calls it (three or four barriers).
+// Rr: band rows of this block, Qt: the line type's row records, Qr = Qt + p*RPB records.
+template <bool PER, int NR, int RPB, bool LDG>
+__device__ __forceinline__ void solve_block(double (&w)[RPB + 2 * (NR - 1)], const double *Rr, const double *Qt,
+                                            const double *Qr, double *xs, int lane, int p, int P)
+{
+    constexpr int W = 2 * NR - 1;
+    constexpr int H = NR - 1;
+    constexpr int WP = (W + 3) / 4 * 4;
+
+    // ---- band product; forward recurrence (non-cyclic) or D-dot (cyclic) ----------------
+    // row j's result goes to slot j: slot j is not read by rows after j.
+    double yprev = 0.0, dot = 0.0;
+#pragma unroll
+    for (int j = 0; j < RPB; j++) {
+        double rc[W + 1];
+        const double2 *r2 = reinterpret_cast<const double2 *>(Rr + j * WP);
+#pragma unroll
+        for (int v = 0; v < (W + 1) / 2; v++) {
+            const double2 x = ldc<LDG>(r2 + v);
+            rc[2 * v] = x.x;
+            rc[2 * v + 1] = x.y;
+        }
+        double acc = rc[NR - 1] * w[j + H];
+#pragma unroll
+        for (int l = 1; l < NR; l++) acc = acc + rc[NR - 1 + l] * w[j + H + l] + rc[NR - 1 - l] * w[j + H - l];
+        if (!PER) {
+            const double2 ab = ldc<LDG>(reinterpret_cast<const double2 *>(Qr + j * kQ + kQfA));
+            const double y = (acc - ab.x * yprev) * ab.y;
+            w[j] = y;
+            yprev = y;
+        } else {
+            const double d = ldc<LDG>(Qr + j * kQ + kQD);
+            dot = j == 0 ? acc * d : dot + acc * d;
+            w[j] = acc;
+        }
+    }
+
+    if (PER) {
+        // ---- x(1) = D . rhs, corner terms, reduced forward recurrence (derivs.F90:786-799)
+        xs[(2 * P + p) * kLanes + lane] = dot;
+        __syncthreads();
+        double x1 = xs[(2 * P) * kLanes + lane];
+        for (int k = 1; k < P; k++) x1 = x1 + xs[(2 * P + k) * kLanes + lane];
+        const double2 cc = ldc<LDG>(reinterpret_cast<const double2 *>(Qt + kQcA));  // row 0: (cA, cC)
+        yprev = 0.0;
+#pragma unroll
+        for (int j = 0; j < RPB; j++) {
+            if (j == 0 && p == 0) continue;  // row 0 is x(1)
+            double g = w[j];
+            if (j == 1 && p == 0) g = g - cc.x * x1;
+            if (j == RPB - 1 && p == P - 1) g = g - cc.y * x1;
+            const double2 ab = ldc<LDG>(reinterpret_cast<const double2 *>(Qr + j * kQ + kQfA));
+            const double y = (g - ab.x * yprev) * ab.y;
+            w[j] = y;
+            yprev = y;
+        }
+        if (p == 0) w[0] = x1;
+    }
+    xs[p * kLanes + lane] = yprev;
+    __syncthreads();
+
+    // ---- prefix of block-end values, correction, backward recurrence --------------------
+    double Y = 0.0;
+    for (int k = 0; k < p; k++) Y = xs[k * kLanes + lane] + ldc<LDG>(Qt + (size_t)((k + 1) * RPB - 1) * kQ + kQpi) * Y;
+    double xprev = 0.0;
+#pragma unroll
+    for (int j = RPB - 1; j >= 0; j--) {
+        if (PER && j == 0 && p == 0) break;  // x(1) is final
+        const double2 cp = ldc<LDG>(reinterpret_cast<const double2 *>(Qr + j * kQ + kQbC));  // (bC, pi)
+        const double y = w[j] + cp.y * Y;  // Y = 0 in the first block
+        const double x = y - cp.x * xprev;
+        w[j] = x;
+        xprev = x;
+    }
+    xs[(P + p) * kLanes + lane] = xprev;
+    __syncthreads();
+
+    // ---- suffix of block-start values, correction ---------------------------------------
+    double X = 0.0;
+    for (int k = P - 1; k > p; k--) X = xs[(P + k) * kLanes + lane] + ldc<LDG>(Qt + (size_t)(k * RPB) * kQ + kQrho) * X;
+#pragma unroll
+    for (int j = 0; j < RPB; j++) {
+        const double rho = ldc<LDG>(Qr + j * kQ + kQrho);
+        w[j] = (PER && j == 0 && p == 0) ? w[0] : w[j] + rho * X;  // X = 0 in the last block
+    }
+}
+
+// Line of a tile lane: start offset inside a field, element stride, line index.
+struct LineRef {
+    long long base, s;
+    int L;
+    bool valid;
+};
+
+template <bool XD>
+__device__ __forceinline__ LineRef line_of(const SweepArgs &a, int tile, int lane)
+{
+    LineRef r;
+    if (XD) {
+        r.L = tile * kLanes + lane;
+        r.valid = r.L < a.nlines;
+        r.base = (long long)r.L * a.N;
+        r.s = 1;
+    } else {
+        const int o = tile / a.tiles_per_row;
+        const int i = (tile % a.tiles_per_row) * kLanes + lane;
+        r.valid = i < a.nx;
+        r.base = i + (long long)o * a.os;
+        r.s = a.es;
+        r.L = i + a.nx * o;
+    }
+    return r;
+}
+
+// Store the solved block (optionally blended with the input values `orig(j)`).
+template <bool XD, int RPB, typename Orig>
+__device__ __forceinline__ void store_block(double *w, double *Gl, long long s, int sp, bool blend_on, double blend,
+                                            Orig orig)
+{
+    if (XD) {
+#pragma unroll
+        for (int q = 0; q < RPB / 4; q++) {
+            double *v = &w[4 * q];
+            if (blend_on) {
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const double o = orig(4 * q + k);
+                    v[k] = o + blend * (v[k] - o);
+                }
+            }
+            st4(Gl + sp + 4 * q, v);
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < RPB; j++) {
+            double v = w[j];
+            if (blend_on) {
+                const double o = orig(j);
+                v = o + blend * (v - o);
+            }
+            Gl[(long long)(sp + j) * s] = v;
+        }
+    }
+}
+
+// Halo row r of a line held at `ln` with element stride `st`: wraps for cyclic lines, zero
+// outside a non-cyclic line (its band coefficients are zero there).
+template <bool PER, typename Ld>
+__device__ __forceinline__ double halo_row(int r, int N, Ld ld)
+{
+    if (PER) {
+        r += r < 0 ? N : 0;
+        r -= r >= N ? N : 0;
+    } else if (r < 0 || r >= N) {
+        return 0.0;
+    }
+    return ld(r);
+}
+
+// ---- one tile per CTA, rows from global memory ----------------------------------------
+template <bool XD, bool PER, int NR, int RPB>
+__global__ void __launch_bounds__(32 * kMaxP) k_rsweep(const SweepArgs a)
+{
+    constexpr int H = NR - 1;
+    constexpr int WP = (2 * NR - 1 + 3) / 4 * 4;
+    constexpr int NW = RPB + 2 * H;
+    extern __shared__ __align__(16) double rxs[];  // [3][P][32]
+    const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
+    const int P = a.P;
+    const int N = a.N;
+    const int sp = p * RPB;
+    const LineRef lr = line_of<XD>(a, blockIdx.x, lane);
+    const double *Fl = a.in + (long long)blockIdx.z * a.in_bstride + (long long)a.in_slot[blockIdx.y] * a.npts + lr.base;
+    double *Gl = a.out + (long long)blockIdx.z * a.out_bstride + (long long)a.out_slot[blockIdx.y] * a.npts + lr.base;
+    const long long s = lr.s;
+    const int t = lr.valid ? a.ltype[lr.L] : 0;
+    const double *Qt = a.Q + (size_t)t * N * kQ;
+    const double *Rr = a.Rm + ((size_t)t * N + sp) * WP;
+    const double *Qr = Qt + (size_t)sp * kQ;
+
+    auto ldg = [&](int r) { return ld_stream(Fl + (long long)r * s); };
+    double w[NW];
+    if (lr.valid) {
+        if (XD) {
+#pragma unroll
+            for (int q = 0; q < RPB / 4; q++) ld4_stream(Fl + sp + 4 * q, &w[H + 4 * q]);
+#pragma unroll
+            for (int k = 0; k < H; k++) {
+                w[k] = halo_row<PER>(sp - H + k, N, ldg);
+                w[H + RPB + k] = halo_row<PER>(sp + RPB + k, N, ldg);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < NW; k++)
+                w[k] = (k >= H && k < H + RPB) ? ldg(sp - H + k) : halo_row<PER>(sp - H + k, N, ldg);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < NW; k++) w[k] = 0.0;
+    }
+    solve_block<PER, NR, RPB, true>(w, Rr, Qt, Qr, rxs, lane, p, P);
+    if (!lr.valid) return;
+    const bool blend_on = a.epi == EPI_BLEND;
+    const double blend = blend_on ? sweep_blend(a) : 0.0;
+    store_block<XD, RPB>(w, Gl, s, sp, blend_on, blend, [&](int j) { return ldg(sp + j); });
+}
+
+// ---- persistent CTAs, TMA-fed two-stage ring --------------------------------------------
+// Job j = tile + ntiles * (field + nf * member); CTA b takes jobs b, b + G, b + 2G, ...
+// y/z tiles: one tensor box {x: 32, line: N} of the 5-D map (x, y, z, field slot, member);
+// x tiles: one bulk copy per line into a [32][N+2] stage (the pad keeps 16-byte reads of
+// two rows conflict-free).
+template <bool XD, bool PER, int NR, int RPB>
+__global__ void __launch_bounds__(32 * kMaxP) k_psweep(const SweepArgs a, const __grid_constant__ CUtensorMap tmap)
+{
+    constexpr int H = NR - 1;
+    constexpr int WP = (2 * NR - 1 + 3) / 4 * 4;
+    constexpr int NW = RPB + 2 * H;
+    extern __shared__ __align__(128) double psm[];
+    const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
+    const int P = a.P;
+    const int N = a.N;
+    const int sp = p * RPB;
+    const size_t stage_d = psweep_stage_doubles(XD, N);
+    double *xs = psm + kStages * stage_d;
+    double *sRm = xs + 3 * P * kLanes;                   // coefficient copy, all line types
+    double *sQ = sRm + (size_t)a.ntypes * N * WP;
+    const uint32_t st0 = smem_u32(psm);
+    const uint32_t bar0 = smem_u32(sQ + (size_t)a.ntypes * N * kQ);
+    const int G = gridDim.x;
+    if (st0 & 127u) {  // tensor copies need 128-byte aligned stages
+        if (threadIdx.x == 0) *(volatile int *)a.err = 2;
+        return;
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; s++) mbar_init(bar0 + 8 * s, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    auto issue = [&](int j, int s) {
+        const int tile = j % a.ntiles, fb = j / a.ntiles, f = fb % a.nf, b = fb / a.nf;
+        const uint32_t bar = bar0 + 8 * s, dst = st0 + (uint32_t)(s * stage_d * sizeof(double));
+        if (XD) {
+            if (threadIdx.x < kLanes) {
+                const int L0 = tile * kLanes;
+                const int nv = min(kLanes, a.nlines - L0);
+                fence_proxy_async();
+                if (lane == 0) mbar_expect_tx(bar, (uint32_t)(nv * N * sizeof(double)));
+                __syncwarp();
+                if (lane < nv)
+                    bulk_g2s(dst + lane * (N + 2) * (uint32_t)sizeof(double),
+                             a.in + (long long)b * a.in_bstride + (long long)a.in_slot[f] * a.npts +
+                                 (long long)(L0 + lane) * N,
+                             (uint32_t)(N * sizeof(double)), bar);
+            }
+        } else if (threadIdx.x == 0) {
+            fence_proxy_async();
+            mbar_expect_tx(bar, (uint32_t)(N * kLanes * sizeof(double)));
+            const int o = tile / a.tiles_per_row, x0 = (tile % a.tiles_per_row) * kLanes;
+            tma_load_5d(dst, &tmap, x0, a.dir == 1 ? 0 : o, a.dir == 1 ? o : 0, a.in_slot[f], b, bar);
+        }
+    };
+    for (int s = 0; s < kStages; s++)
+        if (blockIdx.x + s * G < a.njobs) issue(blockIdx.x + s * G, s);
+    // the coefficient records are read by every tile: copy them once while the first tiles land
+    {
+        const int nR2 = a.ntypes * N * WP / 2, nQ2 = a.ntypes * N * kQ / 2;
+        const double2 *gR = reinterpret_cast<const double2 *>(a.Rm);
+        const double2 *gQ = reinterpret_cast<const double2 *>(a.Q);
+        for (int i = threadIdx.x; i < nR2; i += blockDim.x) reinterpret_cast<double2 *>(sRm)[i] = __ldg(gR + i);
+        for (int i = threadIdx.x; i < nQ2; i += blockDim.x) reinterpret_cast<double2 *>(sQ)[i] = __ldg(gQ + i);
+    }
+    __syncthreads();
+
+    const bool blend_on = a.epi == EPI_BLEND;
+    const double blend = blend_on ? sweep_blend(a) : 0.0;
+    int k = 0;
+    for (int j = blockIdx.x; j < a.njobs; j += G, k++) {
+        const int s = k % kStages;
+        const uint32_t par = (uint32_t)(k / kStages) & 1u;
+        const int tile = j % a.ntiles, fb = j / a.ntiles, f = fb % a.nf, b = fb / a.nf;
+        const LineRef lr = line_of<XD>(a, tile, lane);
+        const int t = lr.valid ? a.ltype[lr.L] : 0;
+        const double *Qt = sQ + (size_t)t * N * kQ;
+        const double *Rr = sRm + ((size_t)t * N + sp) * WP;
+        const double *Qr = Qt + (size_t)sp * kQ;
+        const double *stg = psm + s * stage_d;
+        const bool late = !mbar_wait(bar0 + 8 * s, par);
+
+        // window rows from the stage
+        double w[NW];
+        const double *ln = XD ? stg + lane * (N + 2) : stg + lane;
+        const int ls = XD ? 1 : kLanes;
+        auto lds = [&](int r) { return ln[r * ls]; };
+        if (XD) {
+#pragma unroll
+            for (int q = 0; q < RPB / 2; q++) {
+                const double2 v = *reinterpret_cast<const double2 *>(ln + sp + 2 * q);
+                w[H + 2 * q] = v.x;
+                w[H + 2 * q + 1] = v.y;
+            }
+#pragma unroll
+            for (int kk = 0; kk < H; kk++) {
+                w[kk] = halo_row<PER>(sp - H + kk, N, lds);
+                w[H + RPB + kk] = halo_row<PER>(sp + RPB + kk, N, lds);
+            }
+        } else {
+#pragma unroll
+            for (int kk = 0; kk < NW; kk++)
+                w[kk] = (kk >= H && kk < H + RPB) ? lds(sp - H + kk) : halo_row<PER>(sp - H + kk, N, lds);
+        }
+        if (__syncthreads_or(late)) {
+            // give up: report, let the other stage's copy land (bounded), leave
+            if (threadIdx.x == 0) {
+                *(volatile int *)a.err = 1;
+                if (j + G < a.njobs) mbar_wait(bar0 + 8 * ((k + 1) % kStages), (uint32_t)((k + 1) / kStages) & 1u);
+            }
+            __syncthreads();
+            return;
+        }
+        // every warp has its rows: refill this stage (blend keeps it for the epilogue)
+        if (!blend_on && j + kStages * G < a.njobs) issue(j + kStages * G, s);
+
+        solve_block<PER, NR, RPB, false>(w, Rr, Qt, Qr, xs, lane, p, P);
+        if (lr.valid) {
+            double *Gl = a.out + (long long)b * a.out_bstride + (long long)a.out_slot[f] * a.npts + lr.base;
+            store_block<XD, RPB>(w, Gl, lr.s, sp, blend_on, blend, [&](int jj) { return lds(sp + jj); });
+        }
+        if (blend_on) {
+            __syncthreads();
+            if (j + kStages * G < a.njobs) issue(j + kStages * G, s);
+        }
+    }
+}
+
+}  // namespace gatt

@@ -41,7 +41,8 @@ enum SweepEpi { EPI_STORE = 0, EPI_BLEND = 1 };
 // plus the cyclic dot row D, the block propagators pi / rho, and (row 0 of a cyclic
 // type) the corner couplings A(1) = LHS(1,N) and C(1) = LHS(N,1).
 constexpr int kQ = 8;
-constexpr int kQfA = 0, kQfB = 1, kQbC = 2, kQD = 3, kQpi = 4, kQrho = 5, kQcA = 6, kQcC = 7;
+// Pairs read together sit at even offsets: (fA, fB), (bC, pi), (cA, cC).
+constexpr int kQfA = 0, kQfB = 1, kQbC = 2, kQpi = 3, kQD = 4, kQrho = 5, kQcA = 6, kQcC = 7;
 
 struct SweepArgs {
     const double *in;        // base of the input field set
@@ -67,6 +68,13 @@ struct SweepArgs {
     double blend_fct;
     int epi;                 // SweepEpi
     int P;                   // row blocks per line (1 .. kMaxP); CTA = 32*P threads
+    // pipelined solver (k_psweep) only
+    int dir;                 // 0 x, 1 y, 2 z
+    int nf;                  // fields per launch
+    int ntiles;              // tiles per field
+    int njobs;               // ntiles * nf * members
+    int ntypes;              // line types of the coefficient set
+    int *err;                // set to 1 when a pipeline wait gives up (host-mapped)
 };
 
 __device__ __forceinline__ double sweep_blend(const SweepArgs &a)
@@ -258,15 +266,18 @@ __global__ void __launch_bounds__(BIG ? 32 * kMaxP : 128) k_sweep(const SweepArg
     // full chunks: every incoming row i+NR is a row of this block (i + NR <= ep)
     const int nfull = (ep - NR + 1 - sp) / RB;
     for (int c = 0; c < nfull; c++) {
-        double rc[RB][NV * 4], qc[RB][4], inc[RB];
+        double rc[RB][NV * 4], qc[RB][2], inc[RB];
 #pragma unroll
         for (int u = 0; u < RB; u++) {
             const double2 *r2 = reinterpret_cast<const double2 *>(rp + u * Wp);
 #pragma unroll
             for (int v = 0; v < NV * 2; v++) { const double2 x = r2[v]; rc[u][2 * v] = x.x; rc[u][2 * v + 1] = x.y; }
-            const double2 *q2 = reinterpret_cast<const double2 *>(qp + u * kQ);
-            const double2 qa = q2[0], qb = q2[1];
-            qc[u][0] = qa.x; qc[u][1] = qa.y; qc[u][2] = qb.x; qc[u][3] = qb.y;
+            if (!PER) {
+                const double2 qa = *reinterpret_cast<const double2 *>(qp + u * kQ + kQfA);
+                qc[u][kQfA] = qa.x; qc[u][kQfB] = qa.y;
+            } else {
+                qc[u][0] = qp[u * kQ + kQD];
+            }
             inc[u] = cp[(u + NR) * kLanes];
         }
 #pragma unroll
@@ -280,7 +291,7 @@ __global__ void __launch_bounds__(BIG ? 32 * kMaxP : 128) k_sweep(const SweepArg
                 yprev = y;
             } else {
                 cp[u * kLanes] = acc;
-                dot = (i + u == sp) ? acc * qc[u][kQD] : dot + acc * qc[u][kQD];
+                dot = (i + u == sp) ? acc * qc[u][0] : dot + acc * qc[u][0];
             }
 #pragma unroll
             for (int k = 0; k < W - 1; k++) w[k] = w[k + 1];
@@ -290,14 +301,17 @@ __global__ void __launch_bounds__(BIG ? 32 * kMaxP : 128) k_sweep(const SweepArg
     }
     // tail rows: the incoming row may come from the right halo
     for (; i <= ep; i++, rp += Wp, qp += kQ, cp += kLanes) {
-        double rc[NV * 4], qc[4];
+        double rc[NV * 4], qc[2];
         {
             const double2 *r2 = reinterpret_cast<const double2 *>(rp);
 #pragma unroll
             for (int v = 0; v < NV * 2; v++) { const double2 x = r2[v]; rc[2 * v] = x.x; rc[2 * v + 1] = x.y; }
-            const double2 *q2 = reinterpret_cast<const double2 *>(qp);
-            const double2 qa = q2[0], qb = q2[1];
-            qc[0] = qa.x; qc[1] = qa.y; qc[2] = qb.x; qc[3] = qb.y;
+            if (!PER) {
+                const double2 qa = *reinterpret_cast<const double2 *>(qp + kQfA);
+                qc[kQfA] = qa.x; qc[kQfB] = qa.y;
+            } else {
+                qc[0] = qp[kQD];
+            }
         }
         const int r = i + NR;
         const double inc = r <= ep ? cp[NR * kLanes] : (r - ep - 1 < NR - 1 ? halo[(r - ep - 1) * kLanes] : 0.0);
@@ -310,7 +324,7 @@ __global__ void __launch_bounds__(BIG ? 32 * kMaxP : 128) k_sweep(const SweepArg
             yprev = y;
         } else {
             *cp = acc;
-            dot = (i == sp) ? acc * qc[kQD] : dot + acc * qc[kQD];
+            dot = (i == sp) ? acc * qc[0] : dot + acc * qc[0];
         }
 #pragma unroll
         for (int k = 0; k < W - 1; k++) w[k] = w[k + 1];

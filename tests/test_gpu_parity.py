@@ -45,6 +45,13 @@ def get_case(name):
         elif name == "cavity3d":
             _CASES[name] = cs.cavity_channel(nx=24, ny=20, nz=8, adiabatic_corners=True,
                                              sfd={"X": 0.05, "Delta": 10.0, "buffer": 6})
+        elif name == "box64":
+            _CASES[name] = cs.periodic_box(n=64)
+        elif name == "lid64":
+            _CASES[name] = cs.lid_driven(n=64)
+        elif name == "cavity3d_32":
+            _CASES[name] = cs.cavity_channel(nx=32, ny=32, nz=16, adiabatic_corners=True,
+                                             sfd={"X": 0.05, "Delta": 10.0, "buffer": 6})
         elif name == "long_x":
             _CASES[name] = cs.lid_driven(nxy=(900, 12))
     return _CASES[name]
@@ -66,9 +73,15 @@ def pair(name):
     return c, GattDNS(c), Oracle(c)
 
 
-@pytest.mark.parametrize("name", ["box", "box_aniso", "lid", "lid_tanh", "cavity2d", "cavity3d", "long_x"])
+@pytest.mark.parametrize("name", ["box", "box_aniso", "box64", "lid", "lid64", "lid_tanh", "cavity2d", "cavity3d",
+                                  "cavity3d_32", "long_x"])
 @pytest.mark.parametrize("kind", ["deriv", "filter"])
-def test_line_solves(libs, name, kind):
+@pytest.mark.parametrize("solver", ["pipe", "reg", "tile"])
+def test_line_solves(libs, monkeypatch, name, kind, solver):
+    """The three line-solve kernel families (register rows fed by the TMA ring, register rows
+    loaded from global memory, shared-memory tile) against the oracle; GATT_SWEEP is read
+    when matrices are set."""
+    monkeypatch.setenv("GATT_SWEEP", solver)
     c, g, o = pair(name)
     rng = np.random.default_rng(11)
     F = np.asfortranarray(rng.standard_normal((c.nx, c.ny, c.nz)))
@@ -79,7 +92,8 @@ def test_line_solves(libs, name, kind):
     g.close()
 
 
-@pytest.mark.parametrize("name", ["box", "box_aniso", "lid", "lid_tanh", "cavity2d", "cavity3d"])
+@pytest.mark.parametrize("name", ["box", "box_aniso", "box64", "lid", "lid64", "lid_tanh", "cavity2d", "cavity3d",
+                                  "cavity3d_32"])
 def test_rhs(libs, name):
     c, g, o = pair(name)
     f = flow_for(c)
@@ -116,7 +130,8 @@ def test_filter_in_place(libs, name):
     g.close()
 
 
-@pytest.mark.parametrize("name", ["box", "box_aniso", "lid", "lid_tanh", "cavity2d", "cavity3d"])
+@pytest.mark.parametrize("name", ["box", "box_aniso", "box64", "lid", "lid64", "lid_tanh", "cavity2d", "cavity3d",
+                                  "cavity3d_32"])
 def test_step(libs, name):
     c, g, o = pair(name)
     f = flow_for(c, seed=2)
