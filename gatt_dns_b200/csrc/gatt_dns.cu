@@ -383,9 +383,20 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
 {
     const int N = m.N;
     const bool xd = d == 0;
-    const size_t smem = psweep_smem_bytes(xd, N, m.P, m.nTypes, m.Wp);
     void *k = reg_kernel(true, xd, m.periodic != 0, m.nR);
-    if (!k || smem > kMaxSmem) return GATT_ERR_STATE;
+    if (!k) return GATT_ERR_STATE;
+    // ring depth: the deepest ring that keeps the most CTAs resident (one stage suffices
+    // when a tile's solve outlasts the next tile's copy)
+    int nst = 0, per_sm = 0;
+    size_t smem = 0;
+    for (int st = kMaxStages; st >= 1; st--) {
+        const size_t b = psweep_smem_bytes(xd, N, m.P, m.nTypes, m.Wp, st);
+        if (b > kMaxSmem) continue;
+        const int r = resident_ctas(k, 32 * m.P, b);
+        if (r > per_sm) { per_sm = r; nst = st; smem = b; }
+    }
+    if (nst == 0 || per_sm < 1) return GATT_ERR_STATE;
+    a.nst = nst;
     // 16-byte aligned field starts and line starts (bulk copies), even strides (tensor map)
     if ((reinterpret_cast<uintptr_t>(a.in) & 15) || (c->npts & 1) || (a.in_bstride & 1)) return GATT_ERR_STATE;
     CUtensorMap map;
@@ -408,8 +419,6 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return GATT_ERR_STATE;
     }
-    const int per_sm = resident_ctas(k, 32 * m.P, smem);
-    if (per_sm < 1) return GATT_ERR_STATE;
     const int grid = std::min(a.njobs, per_sm * c->nsm);
     void *args[] = {&a, &map};
     TRY(before_launch(c, cls));

@@ -13,7 +13,7 @@
 // Two kernels feed the registers:
 //  * k_rsweep: one tile per CTA, rows loaded straight from global memory (halo rows are
 //    the neighbouring block's rows, L2 hits);
-//  * k_psweep: persistent CTAs with a two-stage shared-memory ring filled by the Tensor
+//  * k_psweep: persistent CTAs with a one- or two-stage shared-memory ring filled by the Tensor
 //    Memory Accelerator -- one cp.async.bulk.tensor box {32 x N} per y/z tile (it lands
 //    as [row][lane]) or 32 one-dimensional cp.async.bulk line copies per x tile -- so the
 //    next tile streams in while the current one is solved from registers and stored.
@@ -28,23 +28,23 @@ namespace gatt {
 
 // Largest band half-width + 1 the register kernels are instantiated for.
 constexpr int kMaxNRreg = 7;
-// Shared-memory ring depth of k_psweep.
-constexpr int kStages = 2;
+// Deepest shared-memory ring of k_psweep (the host picks 1 or 2 stages per launch).
+constexpr int kMaxStages = 2;
 // Longest mbarrier wait (ns) before a pipeline gives up.
 constexpr unsigned long long kWaitNs = 1000000000ull;
 
-// Shared memory of k_psweep in bytes: kStages tiles, the block exchange, the coefficient
+// Shared memory of k_psweep in bytes: nst ring stages, the block exchange, the coefficient
 // records of every line type (band rows [nTypes][N][Wp], records [nTypes][N][kQ]), the
 // mbarriers.
 __host__ __device__ __forceinline__ size_t psweep_stage_doubles(bool xd, int N)
 {
     return xd ? (size_t)kLanes * (N + 2) : (size_t)N * kLanes;
 }
-__host__ __device__ __forceinline__ size_t psweep_smem_bytes(bool xd, int N, int P, int ntypes, int Wp)
+__host__ __device__ __forceinline__ size_t psweep_smem_bytes(bool xd, int N, int P, int ntypes, int Wp, int nst)
 {
-    return (kStages * psweep_stage_doubles(xd, N) + 3 * (size_t)P * kLanes + (size_t)ntypes * N * (Wp + kQ)) *
+    return (nst * psweep_stage_doubles(xd, N) + 3 * (size_t)P * kLanes + (size_t)ntypes * N * (Wp + kQ)) *
                sizeof(double) +
-           kStages * 8;
+           nst * 8;
 }
 
 // Coefficient load: read-only data path (global records) or plain (shared-memory copy).
@@ -346,7 +346,8 @@ __global__ void __launch_bounds__(32 * kMaxP) k_psweep(const SweepArgs a, const 
     const int N = a.N;
     const int sp = p * RPB;
     const size_t stage_d = psweep_stage_doubles(XD, N);
-    double *xs = psm + kStages * stage_d;
+    const int nst = a.nst;
+    double *xs = psm + nst * stage_d;
     double *sRm = xs + 3 * P * kLanes;                   // coefficient copy, all line types
     double *sQ = sRm + (size_t)a.ntypes * N * WP;
     const uint32_t st0 = smem_u32(psm);
@@ -357,7 +358,7 @@ __global__ void __launch_bounds__(32 * kMaxP) k_psweep(const SweepArgs a, const 
         return;
     }
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; s++) mbar_init(bar0 + 8 * s, 1);
+        for (int s = 0; s < nst; s++) mbar_init(bar0 + 8 * s, 1);
         fence_mbar_init();
     }
     __syncthreads();
@@ -385,7 +386,7 @@ __global__ void __launch_bounds__(32 * kMaxP) k_psweep(const SweepArgs a, const 
             tma_load_5d(dst, &tmap, x0, a.dir == 1 ? 0 : o, a.dir == 1 ? o : 0, a.in_slot[f], b, bar);
         }
     };
-    for (int s = 0; s < kStages; s++)
+    for (int s = 0; s < nst; s++)
         if (blockIdx.x + s * G < a.njobs) issue(blockIdx.x + s * G, s);
     // the coefficient records are read by every tile: copy them once while the first tiles land
     {
@@ -401,8 +402,8 @@ __global__ void __launch_bounds__(32 * kMaxP) k_psweep(const SweepArgs a, const 
     const double blend = blend_on ? sweep_blend(a) : 0.0;
     int k = 0;
     for (int j = blockIdx.x; j < a.njobs; j += G, k++) {
-        const int s = k % kStages;
-        const uint32_t par = (uint32_t)(k / kStages) & 1u;
+        const int s = k % nst;
+        const uint32_t par = (uint32_t)(k / nst) & 1u;
         const int tile = j % a.ntiles, fb = j / a.ntiles, f = fb % a.nf, b = fb / a.nf;
         const LineRef lr = line_of<XD>(a, tile, lane);
         const int t = lr.valid ? a.ltype[lr.L] : 0;
@@ -438,13 +439,13 @@ __global__ void __launch_bounds__(32 * kMaxP) k_psweep(const SweepArgs a, const 
             // give up: report, let the other stage's copy land (bounded), leave
             if (threadIdx.x == 0) {
                 *(volatile int *)a.err = 1;
-                if (j + G < a.njobs) mbar_wait(bar0 + 8 * ((k + 1) % kStages), (uint32_t)((k + 1) / kStages) & 1u);
+                if (nst > 1 && j + G < a.njobs) mbar_wait(bar0 + 8 * ((k + 1) % nst), (uint32_t)((k + 1) / nst) & 1u);
             }
             __syncthreads();
             return;
         }
         // every warp has its rows: refill this stage (blend keeps it for the epilogue)
-        if (!blend_on && j + kStages * G < a.njobs) issue(j + kStages * G, s);
+        if (!blend_on && j + nst * G < a.njobs) issue(j + nst * G, s);
 
         solve_block<PER, NR, RPB, false>(w, Rr, Qt, Qr, xs, lane, p, P);
         if (lr.valid) {
@@ -453,7 +454,7 @@ __global__ void __launch_bounds__(32 * kMaxP) k_psweep(const SweepArgs a, const 
         }
         if (blend_on) {
             __syncthreads();
-            if (j + kStages * G < a.njobs) issue(j + kStages * G, s);
+            if (j + nst * G < a.njobs) issue(j + nst * G, s);
         }
     }
 }

@@ -74,6 +74,7 @@ struct SweepArgs {
     int ntiles;              // tiles per field
     int njobs;               // ntiles * nf * members
     int ntypes;              // line types of the coefficient set
+    int nst;                 // ring stages (1 .. kMaxStages)
     int *err;                // set to 1 when a pipeline wait gives up (host-mapped)
 };
 
