@@ -32,6 +32,10 @@ STAGES = 4
 # Sweep-model bytes per 3-D point-stage: 27 derivative sweeps x 16 B + 5 fields x 32 B of
 # RK state traffic + 15 filter sweeps x 16 B / 4 stages.
 BYTES_PER_POINT_STAGE = 27 * 16 + 5 * 32 + 15 * 16 / 4
+# Fields the 3-D assembly + RK update moves per point, averaged over the four stages: stage
+# input 5, gradients 15, second-sweep terms 12, step start 5 (stages 2-4; in stage 1 it is
+# the stage input), RK increment read 5 (stages 2-4) and written 5 (stages 1-3), output 5.
+ASSEMBLE_FIELDS = (5 + 15 + 12 + 5) + (3 * 5 + 3 * 5 + 3 * 5) / 4.0 + 5 - 5 / 4.0
 
 
 def parse():
@@ -265,7 +269,7 @@ def main():
     alg = {"sweep_d1_x": 5 * 16, "sweep_d1_y": 5 * 16, "sweep_d1_z": 5 * 16,
            "sweep_d2_x": 4 * 16, "sweep_d2_y": 4 * 16, "sweep_d2_z": 4 * 16,
            "filter_x": 5 * 16, "filter_y": 5 * 16, "filter_z": 5 * 16,
-           "visc": (13 + 9) * 8, "assemble_rk": (5 + 15 + 6 + 12 + 5 + 5 + 5 + 5) * 8, "maxchange": 10 * 8}
+           "visc": (13 + 9) * 8, "assemble_rk": ASSEMBLE_FIELDS * 8, "maxchange": 10 * 8}
     per_step = {k: v[0] * v[1] for k, v in prof.items()}
     dom = max(per_step, key=per_step.get)
     peak, peak_kind = measured_peaks()

@@ -527,7 +527,7 @@ int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet
         TRY(sweep(c, 2, 0, tq, btq, iz, d2, bd2, sz, 4, nmem, 0, nullptr, PC_D2Z));
         TRY(before_launch(c, PC_ASSEMBLE));
         k_assemble3d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(
-            c->ph, q, q0, out, fset(c, delta, 5), fset(c, d1, D3_N), fset(c, tq, T3_N), fset(c, d2, S3_N), n, mode, sp);
+            c->ph, q, q0, out, fset(c, delta, 5), fset(c, d1, D3_N), fset(c, d2, S3_N), n, mode, sp);
         return after_launch(c);
     }
     const long long bd1 = D2_N * n, btq = T2_N * n, bd2 = S2_N * n;

@@ -62,22 +62,43 @@ __device__ __forceinline__ double sutherland_mu(const Phys &ph, double E)
     return mu1 * mu2 * sqrt(mu2);
 }
 
+// Viscous stresses from the velocity gradients, 3-D (nseq.F90:225-236).  One definition for
+// k_visc3d (which stores them for the second sweeps) and k_assemble3d (which recomputes them
+// from the gradients it reads anyway instead of reading six stored fields back).
+struct Stress3 {
+    double xx, yy, zz, xy, xz, yz;
+};
+__device__ __forceinline__ Stress3 stress3d(double c, double dux, double duy, double duz, double dvx, double dvy,
+                                            double dvz, double dwx, double dwy, double dwz)
+{
+    const double tzz = -2.0 / 3.0 * (dux + dvy + dwz);
+    Stress3 t;
+    t.xx = c * (2.0 * dux + tzz);
+    t.yy = c * (2.0 * dvy + tzz);
+    t.zz = c * (2.0 * dwz + tzz);
+    t.xy = c * (duy + dvx);
+    t.xz = c * (duz + dwx);
+    t.yz = c * (dvz + dwy);
+    return t;
+}
+
 // Stresses and heat fluxes, 3-D (nseq.F90:225-239, 286-288)
-__global__ void k_visc3d(Phys ph, StateSet q, FieldSet d1, FieldSet tq, long long n)
+__global__ void __launch_bounds__(256) k_visc3d(Phys ph, StateSet q, FieldSet d1, FieldSet tq, long long n)
 {
     const int b = blockIdx.y;
     const double *E = q.v[4] + b * q.bstride;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
         const double mu = sutherland_mu(ph, E[p]);
-        const double dux = d1.f(b, D3_UX)[p], dvy = d1.f(b, D3_VY)[p], dwz = d1.f(b, D3_WZ)[p];
-        const double tzz = -2.0 / 3.0 * (dux + dvy + dwz);
         const double c = 1.0 / ph.Re * mu;
-        tq.f(b, T3_XX)[p] = c * (2.0 * dux + tzz);
-        tq.f(b, T3_YY)[p] = c * (2.0 * dvy + tzz);
-        tq.f(b, T3_ZZ)[p] = c * (2.0 * dwz + tzz);
-        tq.f(b, T3_XY)[p] = c * (d1.f(b, D3_UY)[p] + d1.f(b, D3_VX)[p]);
-        tq.f(b, T3_XZ)[p] = c * (d1.f(b, D3_UZ)[p] + d1.f(b, D3_WX)[p]);
-        tq.f(b, T3_YZ)[p] = c * (d1.f(b, D3_VZ)[p] + d1.f(b, D3_WY)[p]);
+        const Stress3 t = stress3d(c, d1.f(b, D3_UX)[p], d1.f(b, D3_UY)[p], d1.f(b, D3_UZ)[p], d1.f(b, D3_VX)[p],
+                                   d1.f(b, D3_VY)[p], d1.f(b, D3_VZ)[p], d1.f(b, D3_WX)[p], d1.f(b, D3_WY)[p],
+                                   d1.f(b, D3_WZ)[p]);
+        tq.f(b, T3_XX)[p] = t.xx;
+        tq.f(b, T3_YY)[p] = t.yy;
+        tq.f(b, T3_ZZ)[p] = t.zz;
+        tq.f(b, T3_XY)[p] = t.xy;
+        tq.f(b, T3_XZ)[p] = t.xz;
+        tq.f(b, T3_YZ)[p] = t.yz;
         const double h = -ph.gamma / ph.Re / ph.Pr * mu;
         tq.f(b, T3_QX)[p] = h * d1.f(b, D3_EX)[p];
         tq.f(b, T3_QY)[p] = h * d1.f(b, D3_EY)[p];
@@ -117,9 +138,10 @@ __device__ __forceinline__ void rk_update(int mode, double dt, double k, double 
 
 // Assembly of dR, dU, dV, dW, dE (nseq.F90:310-318) fused with the RK4 stage update.
 // q: stage input; q0: step start; out: stage output (may alias q: pointwise in place).
-__global__ void k_assemble3d(Phys ph, StateSet q, StateSet q0, StateSet out, FieldSet delta,
-                             FieldSet d1, FieldSet tq, FieldSet d2, long long n, int mode,
-                             const StepParams *sp)
+// The stresses are recomputed from the gradients (stress3d) rather than read back.
+__global__ void __launch_bounds__(256, 3) k_assemble3d(Phys ph, StateSet q, StateSet q0, StateSet out, FieldSet delta,
+                                                       FieldSet d1, FieldSet d2, long long n, int mode,
+                                                       const StepParams *sp)
 {
     const int b = blockIdx.y;
     const double dt = sp ? sp->dt : 0.0;
@@ -144,10 +166,11 @@ __global__ void k_assemble3d(Phys ph, StateSet q, StateSet q0, StateSet out, Fie
         const double kU = -(dux * u + duy * v + duz * w) + (vtx - DPx) / r;
         const double kV = -(dvx * u + dvy * v + dvz * w) + (vty - DPy) / r;
         const double kW = -(dwx * u + dwy * v + dwz * w) + (vtz - DPz) / r;
+        const Stress3 t = stress3d(1.0 / ph.Re * sutherland_mu(ph, e), dux, duy, duz, dvx, dvy, dvz, dwx, dwy, dwz);
         const double kE = -(dex * u + dey * v + dez * w)
-                        + (-P * (dux + dvy + dwz) + tq.f(b, T3_XX)[p] * dux + tq.f(b, T3_YY)[p] * dvy
-                           + tq.f(b, T3_ZZ)[p] * dwz + tq.f(b, T3_XY)[p] * (dvx + duy)
-                           + tq.f(b, T3_XZ)[p] * (dwx + duz) + tq.f(b, T3_YZ)[p] * (dwy + dvz)
+                        + (-P * (dux + dvy + dwz) + t.xx * dux + t.yy * dvy
+                           + t.zz * dwz + t.xy * (dvx + duy)
+                           + t.xz * (dwx + duz) + t.yz * (dwy + dvz)
                            - d2.f(b, S3_HTX)[p] - d2.f(b, S3_HTY)[p] - d2.f(b, S3_HTZ)[p]) / r;
         const double k[5] = {kU, kV, kW, kR, kE};
 #pragma unroll
@@ -155,7 +178,7 @@ __global__ void k_assemble3d(Phys ph, StateSet q, StateSet q0, StateSet out, Fie
             double *dl = delta.p ? delta.f(b, f) + p : nullptr;
             double q0v = (mode != RK_STORE_RHS) ? q0.v[f][b * q0.bstride + p] : 0.0;
             double res;
-            double dtmp = dl ? *dl : 0.0;
+            double dtmp = (dl && mode >= RK_STAGE2) ? *dl : 0.0;  // stage 1 overwrites delta
             rk_update(mode, dt, k[f], q0v, &dtmp, &res);
             if (dl && mode != RK_STAGE4 && mode != RK_STORE_RHS) *dl = dtmp;
             out.v[f][b * out.bstride + p] = res;
@@ -197,7 +220,7 @@ __global__ void k_assemble2d(Phys ph, StateSet q, StateSet q0, StateSet out, Fie
             double *dl = delta.p ? delta.f(b, f) + p : nullptr;
             double q0v = (mode != RK_STORE_RHS) ? q0.v[f][b * q0.bstride + p] : 0.0;
             double res;
-            double dtmp = dl ? *dl : 0.0;
+            double dtmp = (dl && mode >= RK_STAGE2) ? *dl : 0.0;  // stage 1 overwrites delta
             rk_update(mode, dt, k[f], q0v, &dtmp, &res);
             if (dl && mode != RK_STAGE4 && mode != RK_STORE_RHS) *dl = dtmp;
             out.v[f][b * out.bstride + p] = res;
