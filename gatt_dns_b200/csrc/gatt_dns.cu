@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/gatt_dns.h"
+#include "arnoldi.cuh"
 #include "bc.cuh"
 #include "pointwise.cuh"
 #include "rsweep.cuh"
@@ -118,6 +119,13 @@ struct gatt_ctx {
     double *qA = nullptr, *qB = nullptr, *delta = nullptr, *mean = nullptr;
     double *d1 = nullptr, *tq = nullptr, *d2 = nullptr, *P = nullptr, *tmp = nullptr;
     double *tin = nullptr, *tout = nullptr;  // host-facing scratch (rhs / deriv entry points)
+    // Jacobian-free Arnoldi (gatt_arnoldi): basis [b][j][v][p], B, base and base-run states,
+    // reduction partials, Hessenberg columns, region mask
+    double *arn_zeta = nullptr, *arn_B = nullptr, *arn_base = nullptr, *arn_um = nullptr;
+    double *arn_part = nullptr, *arn_h = nullptr;
+    uint8_t *arn_region = nullptr;
+    int arn_m = 0;       // basis vectors held: m + 1 per member
+    bool arn_have_region = false;
     bool mean_init = false;                  // SFD mean uploaded or copied from the state
     int cur = 0;
     unsigned long long *acc = nullptr;
@@ -907,6 +915,148 @@ int noalloc_scratch(unsigned long long **out)
     return GATT_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Jacobian-free Arnoldi (calcInstability.m:304-400, first-order variant), nbatch problems
+// ---------------------------------------------------------------------------
+
+int arn_nv(const gatt_ctx *c) { return c->is3d ? 5 : 4; }
+
+int arn_alloc(gatt_ctx *c, int m)
+{
+    const long long len = (long long)arn_nv(c) * c->npts;
+    if (c->arn_m < m) {
+        cudaFree(c->arn_zeta);
+        c->arn_zeta = nullptr;
+        c->arn_m = 0;
+        CU(cudaMalloc(&c->arn_zeta, sizeof(double) * (size_t)c->nb * (m + 1) * len));
+        cudaFree(c->arn_part);
+        c->arn_part = nullptr;
+        CU(cudaMalloc(&c->arn_part, sizeof(double) * (size_t)c->nb * (m + 2) * kRedBlocks));
+        cudaFree(c->arn_h);
+        c->arn_h = nullptr;
+        CU(cudaMalloc(&c->arn_h, sizeof(double) * (size_t)c->nb * (m + 2)));
+        c->arn_m = m;
+    }
+    if (!c->arn_B) CU(cudaMalloc(&c->arn_B, sizeof(double) * (size_t)c->nb * len));
+    if (!c->arn_base) CU(cudaMalloc(&c->arn_base, sizeof(double) * 5 * (size_t)c->npts));
+    if (!c->arn_um) CU(cudaMalloc(&c->arn_um, sizeof(double) * 5 * (size_t)c->npts));
+    if (!c->arn_region) CU(cudaMalloc(&c->arn_region, (size_t)c->npts));
+    return GATT_OK;
+}
+
+// Sum the partials of nvec vectors per member into arn_h[b][0..nvec) (sqrt when asked)
+int arn_sum(gatt_ctx *c, int part_stride, int nvec, double *h, int h_stride, bool take_sqrt)
+{
+    TRY(before_launch(c, PC_OTHER));
+    k_arn_sum<<<c->nb, (nvec + 31) / 32 * 32, 0, c->stream>>>(c->arn_part, part_stride, nvec, h, h_stride, take_sqrt);
+    return after_launch(c);
+}
+
+int arnoldi(gatt_ctx *c, int m, int nsteps, double t0, double dt, double eps, const double *base,
+            const double *v0, const unsigned char *region, double *H)
+{
+    TRY(check_ready(c, true));
+    if (m < 1 || m > kMaxKrylov) return fail(GATT_ERR_BADARG, "Krylov dimension must be 1 .. " + std::to_string(kMaxKrylov));
+    if (nsteps < 1) return fail(GATT_ERR_BADARG, "nsteps < 1");
+    if (!(dt > 0) || !std::isfinite(dt) || !(eps > 0) || !std::isfinite(eps))
+        return fail(GATT_ERR_BADARG, "dt and eps must be positive and finite");
+    if (!base || !v0 || !H) return fail(GATT_ERR_BADARG, "null base, v0 or H");
+    const long long n = c->npts;
+    const int nv = arn_nv(c);
+    const long long len = (long long)nv * n;
+    TRY(arn_alloc(c, m));
+    const long long zs = (long long)(c->arn_m + 1) * len;  // basis stride between members
+    const int ps = (c->arn_m + 2) * kRedBlocks, hs = c->arn_m + 2;
+    // flow region: the points whose values enter the vectors (calcInstability.m:137-141)
+    long long nreg = n;
+    if (region) {
+        nreg = 0;
+        for (long long p = 0; p < n; p++) nreg += region[p] != 0;
+        if (nreg == 0) return fail(GATT_ERR_BADARG, "empty flow region");
+        CU(cudaMemcpyAsync(c->arn_region, region, (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    }
+    const uint8_t *reg = region ? c->arn_region : nullptr;
+    const double sqrtN = std::sqrt((double)nv * (double)nreg);
+    const double den = eps * sqrtN;
+    CU(cudaMemcpyAsync(c->arn_base, base, sizeof(double) * 5 * n, cudaMemcpyHostToDevice, c->stream));
+    // zeta_1 = v0 restricted to the region (flow2vec), normalised
+    {
+        std::vector<double> tmp((size_t)n);
+        for (int b = 0; b < c->nb; b++)
+            for (int f = 0; f < 5; f++) {
+                const int v = c->is3d ? f : (f == 2 ? -1 : (f < 2 ? f : f - 1));
+                if (v < 0) continue;
+                const double *src = v0 + ((size_t)b * 5 + f) * n;
+                for (long long p = 0; p < n; p++) tmp[p] = (!region || region[p]) ? src[p] : 0.0;
+                CU(cudaMemcpyAsync(c->arn_zeta + b * zs + v * n, tmp.data(), sizeof(double) * n,
+                                   cudaMemcpyHostToDevice, c->stream));
+                CU(cudaStreamSynchronize(c->stream));  // tmp is reused
+            }
+    }
+    const dim3 rgrid(kRedBlocks, c->nb);
+    TRY(before_launch(c, PC_OTHER));
+    k_arn_dots<<<rgrid, kRedThreads, 0, c->stream>>>(c->arn_zeta, zs, c->arn_zeta, zs, 0, len, c->arn_part, ps);
+    TRY(after_launch(c));
+    TRY(arn_sum(c, ps, 1, c->arn_h, hs, true));
+    TRY(before_launch(c, PC_OTHER));
+    k_arn_scale<<<dim3(grid_for(c, len), c->nb), kBlock, 0, c->stream>>>(c->arn_zeta, zs, c->arn_h, hs, 0, len);
+    TRY(after_launch(c));
+
+    auto evolve = [&](int k, double e) -> int {
+        // state = base + (zeta_k * e) * sqrt(N); SFD mean restarts from it (main.F90:158-163)
+        TRY(before_launch(c, PC_OTHER));
+        k_arn_perturb<<<dim3(grid_for(c, n), c->nb), kBlock, 0, c->stream>>>(state_set(c, 0), c->arn_base,
+                                                                             c->arn_zeta + k * len, zs, reg, e,
+                                                                             sqrtN, c->is3d, n);
+        TRY(after_launch(c));
+        c->mean_init = false;
+        return run_steps(c, nsteps, t0, dt, nullptr, true);
+    };
+    // UM: the base flow's own run (calcInstability.m:327-340); every member runs the base
+    // (a zero disturbance), member 0's result is kept
+    TRY(evolve(0, 0.0));
+    {
+        const StateSet q = state_set(c, 0);
+        for (int f = 0; f < 5; f++)
+            CU(cudaMemcpyAsync(c->arn_um + f * n, q.v[f], sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    memset(H, 0, sizeof(double) * (size_t)c->nb * (m + 1) * m);
+    std::vector<double> hc((size_t)c->nb * hs);
+    for (int k = 0; k < m; k++) {
+        // B = (Phi(base + disturbance) - UM) / (eps sqrt(N))
+        TRY(evolve(k, eps));
+        TRY(before_launch(c, PC_OTHER));
+        k_arn_diff<<<dim3(grid_for(c, n), c->nb), kBlock, 0, c->stream>>>(state_set(c, 0), c->arn_um, c->arn_B, len, nv,
+                                                                          reg, den, c->is3d, n);
+        TRY(after_launch(c));
+        // classical Gram-Schmidt: H(j,k) = zeta_j . B, uPrime = B - sum H(j,k) zeta_j
+        TRY(before_launch(c, PC_OTHER));
+        k_arn_dots<<<rgrid, kRedThreads, 0, c->stream>>>(c->arn_zeta, zs, c->arn_B, len, k, len, c->arn_part, ps);
+        TRY(after_launch(c));
+        TRY(arn_sum(c, ps, k + 1, c->arn_h, hs, false));
+        TRY(before_launch(c, PC_OTHER));
+        k_arn_orth<<<rgrid, kRedThreads, 0, c->stream>>>(c->arn_zeta, zs, c->arn_B, len, c->arn_h, hs, k, len,
+                                                          c->arn_part, ps);
+        TRY(after_launch(c));
+        // H(k+1,k) = |uPrime|, zeta_{k+1} = uPrime / H(k+1,k)
+        TRY(arn_sum(c, ps, 1, c->arn_h + k + 1, hs, true));
+        TRY(before_launch(c, PC_OTHER));
+        k_arn_scale<<<dim3(grid_for(c, len), c->nb), kBlock, 0, c->stream>>>(c->arn_zeta, zs, c->arn_h + k + 1, hs,
+                                                                             k + 1, len);
+        TRY(after_launch(c));
+        CU(cudaMemcpyAsync(hc.data(), c->arn_h, sizeof(double) * hc.size(), cudaMemcpyDeviceToHost, c->stream));
+        TRY(sync_stream(c));
+        for (int b = 0; b < c->nb; b++)
+            for (int i = 0; i <= k + 1; i++) {
+                const double h = hc[(size_t)b * hs + i];
+                if (!std::isfinite(h)) return fail(GATT_ERR_DIVERGED, "non-finite Hessenberg entry (member " +
+                                                                          std::to_string(b) + ")");
+                H[(size_t)b * (m + 1) * m + (size_t)k * (m + 1) + i] = h;
+            }
+    }
+    return GATT_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -997,7 +1147,9 @@ void gatt_destroy(gatt_ctx *c)
         cudaFree(c->ltype[d]);
     }
     double *bufs[] = {c->qA, c->qB, c->delta, c->mean, c->d1, c->tq, c->d2, c->P, c->tmp, c->tin, c->tout, c->chi, c->hist,
-                      c->d_coef1, c->d_coef2, c->d_xs};
+                      c->d_coef1, c->d_coef2, c->d_xs, c->arn_zeta, c->arn_B, c->arn_base, c->arn_um,
+                      c->arn_part, c->arn_h};
+    cudaFree(c->arn_region);
     for (double *p : bufs) cudaFree(p);
     cudaFree(c->d_ops); cudaFree(c->acc); cudaFree(c->d_params);
     if (c->h_params) cudaFreeHost(c->h_params);
@@ -1426,6 +1578,29 @@ int gatt_max_velocity(gatt_ctx *c, double *vmax)
     CU(cudaMemcpyAsync(h.data(), c->acc, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost, c->stream));
     TRY(sync_stream(c));
     for (size_t i = 0; i < h.size(); i++) memcpy(&vmax[i], &h[i], sizeof(double));
+    return GATT_OK;
+}
+
+int gatt_arnoldi(gatt_ctx *c, int m, int nsteps, double t0, double dt, double eps, const double *base,
+                 const double *v0, const unsigned char *region, double *H)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    return arnoldi(c, m, nsteps, t0, dt, eps, base, v0, region, H);
+}
+
+int gatt_arnoldi_vector(gatt_ctx *c, int b, int j, double *out)
+{
+    if (!c || !out) return fail(GATT_ERR_BADARG, "null argument");
+    TRY(check_member(c, b));
+    if (!c->arn_zeta || j < 0 || j > c->arn_m) return fail(GATT_ERR_BADARG, "no such basis vector");
+    const long long n = c->npts, len = (long long)arn_nv(c) * n;
+    const double *z = c->arn_zeta + (long long)b * (c->arn_m + 1) * len + (long long)j * len;
+    for (int f = 0; f < 5; f++) {
+        const int v = c->is3d ? f : (f == 2 ? -1 : (f < 2 ? f : f - 1));
+        if (v < 0) memset(out + f * n, 0, sizeof(double) * n);
+        else CU(cudaMemcpyAsync(out + f * n, z + v * n, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    }
+    TRY(sync_stream(c));
     return GATT_OK;
 }
 

@@ -195,6 +195,36 @@ class GattDNS:
         _lib.check(self.lib.gatt_run(self.h, nsteps, t0, dt, _dp(mc)), "gatt_run")
         return mc.reshape(self.nbatch, 5)
 
+    def arnoldi(self, base, v0, m, nsteps, dt, eps=1e-7, t0=0.0, region=None):
+        """Jacobian-free Arnoldi (calcInstability.m:304-400, first order) for every member.
+
+        base: flow dict (the base flow, shared); v0: list of nbatch flow dicts (initial
+        disturbances); region: boolean (nx, ny, nz) flow region or None.  Returns H of shape
+        (nbatch, m+1, m); the Ritz values of member b are eig(H[b, :m, :m]) and the growth
+        rates log(lambda)/T as calcInstability.m:411 computes them.
+        """
+        keys = ("U", "V", "W", "R", "E")
+        if len(v0) != self.nbatch:
+            raise ValueError("need one initial disturbance per member")
+        bvec = np.concatenate([_f64(base[k]).ravel(order="F") for k in keys])
+        v = np.concatenate([_f64(d[k]).ravel(order="F") for d in v0 for k in keys])
+        reg = None
+        if region is not None:
+            reg = np.ascontiguousarray(np.asarray(region, dtype=bool).ravel(order="F").astype(np.uint8))
+        H = np.zeros(self.nbatch * (m + 1) * m)
+        _lib.check(self.lib.gatt_arnoldi(self.h, m, nsteps, t0, dt, eps, _dp(bvec), _dp(v),
+                                         reg.ctypes.data_as(ctypes.c_void_p) if reg is not None else None,
+                                         _dp(H)), "gatt_arnoldi")
+        return H.reshape(self.nbatch, m, m + 1).transpose(0, 2, 1).copy()
+
+    def arnoldi_vector(self, b, j):
+        """Basis vector zeta_{j+1} of member b after arnoldi(), as a flow dict."""
+        s = (self.case.nx, self.case.ny, self.case.nz)
+        out = np.zeros(5 * self.case.nx * self.case.ny * self.case.nz)
+        _lib.check(self.lib.gatt_arnoldi_vector(self.h, b, j, _dp(out)), "gatt_arnoldi_vector")
+        n = out.size // 5
+        return {k: out[i * n:(i + 1) * n].reshape(s, order="F") for i, k in enumerate(("U", "V", "W", "R", "E"))}
+
     def max_velocity(self):
         v = np.zeros(3 * self.nbatch)
         _lib.check(self.lib.gatt_max_velocity(self.h, _dp(v)), "gatt_max_velocity")

@@ -150,6 +150,31 @@ int gatt_step(gatt_ctx *ctx, double t, double dt, double *maxChange);
  * synchronisation per step; maxChange receives the last step's 5*nbatch values. */
 int gatt_run(gatt_ctx *ctx, int nsteps, double t0, double dt, double *maxChange);
 
+/* Jacobian-free Arnoldi, first-order variant of calcInstability.m:304-400, run for the
+ * context's nbatch members as nbatch independent problems side by side (the Krylov index is
+ * sequential within a problem; the batch advances every problem's step k together, each
+ * member's arithmetic identical to a run of that member alone).
+ *   base   host, 5*npts: U, V, W, R, E of the base flow, shared by all problems
+ *   v0     host, nbatch*5*npts (member-major, then U, V, W, R, E): initial disturbances;
+ *          zeta_1 = v0 restricted to the region and normalised (the reference passes its
+ *          Gaussian bump unnormalised, calcInstability.m:309)
+ *   region host npts bytes, nonzero = point in the flow region (calcInstability.m:137-141),
+ *          or NULL for every point
+ *   H      host, nbatch*(m+1)*m, column-major per member: H(i,k) at [b*(m+1)*m + k*(m+1) + i]
+ * Vectors hold U, V, W, R, E (3-D) or U, V, R, E (2-D) over the region, N entries.  One
+ * base run UM = Phi(base) (:327-340), then for k = 1..m: Phi(base + zeta_k*eps*sqrt(N))
+ * over nsteps steps of dt from t0, B = (that - UM)/(eps*sqrt(N)), classical Gram-Schmidt
+ * H(j,k) = zeta_j.B, H(k+1,k) = |B - sum H(j,k) zeta_j|, zeta_{k+1} (:364-400).  Leaves the
+ * state at the last run's end; the basis stays on the device for gatt_arnoldi_vector.
+ * m <= 512; device memory for the basis: nbatch*(m+1)*N doubles. */
+int gatt_arnoldi(gatt_ctx *ctx, int m, int nsteps, double t0, double dt, double eps, const double *base,
+                 const double *v0, const unsigned char *region, double *H);
+
+/* Basis vector zeta_{j+1} (0 <= j <= m) of member b after gatt_arnoldi, as five host fields
+ * U, V, W, R, E of npts each (W zero in 2-D, zero outside the region): the psiA = zeta*psiH
+ * mode reconstruction of calcInstability.m:419 is left to the caller. */
+int gatt_arnoldi_vector(gatt_ctx *ctx, int b, int j, double *out);
+
 /* max|U|, max|V|, max|W| of every member (main.F90:196-204), for the caller's CFL. */
 int gatt_max_velocity(gatt_ctx *ctx, double *vmax);
 

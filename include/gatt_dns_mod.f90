@@ -195,6 +195,22 @@ module gatt_dns
             real(c_double), dimension(*) :: maxChange
             integer(c_int) :: gatt_run
         end function
+        function gatt_arnoldi(ctx, m, nsteps, t0, dt, eps, base, v0, region, H) bind(C, name='gatt_arnoldi')
+            import :: c_int, c_ptr, c_double, c_signed_char
+            type(c_ptr), value :: ctx
+            integer(c_int), value :: m, nsteps
+            real(c_double), value :: t0, dt, eps
+            real(c_double), dimension(*) :: base, v0, H
+            integer(c_signed_char), dimension(*) :: region
+            integer(c_int) :: gatt_arnoldi
+        end function
+        function gatt_arnoldi_vector(ctx, b, j, out) bind(C, name='gatt_arnoldi_vector')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: ctx
+            integer(c_int), value :: b, j
+            real(c_double), dimension(*) :: out
+            integer(c_int) :: gatt_arnoldi_vector
+        end function
         function gatt_max_velocity(ctx, vmax) bind(C, name='gatt_max_velocity')
             import :: c_int, c_ptr, c_double
             type(c_ptr), value :: ctx
