@@ -33,9 +33,14 @@ STAGES = 4
 # RK state traffic + 15 filter sweeps x 16 B / 4 stages.
 BYTES_PER_POINT_STAGE = 27 * 16 + 5 * 32 + 15 * 16 / 4
 # Fields the 3-D assembly + RK update moves per point, averaged over the four stages: stage
-# input 5, gradients 15, second-sweep terms 12, step start 5 (stages 2-4; in stage 1 it is
-# the stage input), RK increment read 5 (stages 2-4) and written 5 (stages 1-3), output 5.
-ASSEMBLE_FIELDS = (5 + 15 + 12 + 5) + (3 * 5 + 3 * 5 + 3 * 5) / 4.0 + 5 - 5 / 4.0
+# input 5, gradients 15, second-sweep terms 12 and output 5 in every stage; step start 5
+# (stages 2-4; in stage 1 it is the stage input), RK increment read 5 (stages 2-4) and
+# written 5 (stages 1-3).  Stages 1..4: 42, 52, 52, 47 fields; mean 48.25.
+ASSEMBLE_FIELDS = (5 + 15 + 12 + 5) + 3 * (3 * 5) / 4.0
+# DRAM traffic of the assembly from ncu (profiles/k_assemble3d_periodic_box_128.md): a
+# stage-3 launch moved 876.3 MB (read + write) for 52 algorithmic fields of 128^3 points;
+# scaled to the four-stage mean by algorithmic fields, for n = 128 only.
+ASSEMBLE_TRAFFIC_STAGE3_128 = 876.3e6
 
 
 def parse():
@@ -46,6 +51,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--n", type=int, default=N_GRID)
     p.add_argument("--no-clocks", action="store_true")
+    p.add_argument("--no-arnoldi", action="store_true")
     return p.parse_args()
 
 
@@ -175,6 +181,64 @@ def cpu_baseline_sample(c, seconds=10.0):
                       "OpenMP over lines)" % (n, c.nx, el)}
 
 
+def arnoldi_sample(cs, GattDNS, case, base, members, m, nsteps, seed, label):
+    """Batched vs serial Jacobian-free Arnoldi on one GPU (bounded sample).
+
+    Batched: one context of `members` members, one gatt_arnoldi call (every kernel launch
+    covers all members).  Serial: one single-member context reused for the same problems one
+    after another.  Both include the host<->device transfers of the calls; each side's
+    graphs are captured in an untimed warm-up call first.
+    """
+    import torch
+    rng = np.random.default_rng(seed)
+    s = (case.nx, case.ny, case.nz)
+    v0 = []
+    for _ in range(members):
+        d = {k: np.zeros(s, order="F") for k in "UVWRE"}
+        d["U"][...] = 1e-6 * rng.standard_normal(s)
+        d["V"][...] = 1e-6 * rng.standard_normal(s)
+        v0.append(d)
+    dt = case.cfl_dt(base["U"], base["V"], base["W"], 0.5)
+    gb = GattDNS(case, nbatch=members)
+    gb.arnoldi(base, v0, 1, 1, dt)                      # warm-up: graph capture, buffers
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Hb = gb.arnoldi(base, v0, m, nsteps, dt)
+    torch.cuda.synchronize()
+    tb = time.perf_counter() - t0
+    step_b = time_steps(gb, dt, 10) / members          # ms per member-step, batched
+    gb.close()
+    g1 = GattDNS(case, nbatch=1)
+    g1.arnoldi(base, v0[:1], 1, 1, dt)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    same = True
+    for b in range(members):
+        Hs = g1.arnoldi(base, [v0[b]], m, nsteps, dt)[0]
+        same = same and bool(np.array_equal(Hs, Hb[b]))
+    torch.cuda.synchronize()
+    ts = time.perf_counter() - t0
+    step_1 = time_steps(g1, dt, 10)                    # ms per step, one member
+    g1.close()
+    return {"workload": label, "members": members, "krylov_steps": m, "rk4_steps_per_run": nsteps,
+            "runs_per_member": m + 1, "batched_s": tb, "serial_s": ts, "serial_over_batched": ts / tb,
+            "H_batched_equals_serial": same,
+            "rk4_step_ms_per_member_batched": step_b, "rk4_step_ms_single": step_1,
+            "full_config_serial_over_batched_est": step_1 / step_b,
+            "sample": "%d Krylov steps of %d RK4 steps each (plus the base run) per problem; the full "
+                      "config runs 32 Krylov steps of 500, where the RK4 steps dominate: its ratio is "
+                      "estimated from the time per member-step (10 synchronised steps)" % (m, nsteps)}
+
+
+def time_steps(g, dt, k):
+    """ms per step of k back-to-back gatt_run steps (gatt_run returns after synchronising the
+    context's own stream, so the wall time brackets the device work)."""
+    g.run(2, 0.0, dt)
+    t0 = time.perf_counter()
+    g.run(k, 0.0, dt)
+    return (time.perf_counter() - t0) * 1e3 / k
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -294,7 +358,10 @@ def main():
                     "path": "gatt_upload from pinned host, K x gatt_step (host maxChange each step), gatt_download"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "frac": (achieved / peak) if achieved else None,
+                         "traffic": (ASSEMBLE_TRAFFIC_STAGE3_128 * ASSEMBLE_FIELDS / 52.0
+                                     if dom == "assemble_rk" and args.n == 128 else None),
+                         "traffic_bytes_algorithmic": dom_bytes,
                          "peak_source": peak_kind,
                          "step_sweep_model_gbs": stage_model, "step_sweep_model_frac": stage_model / peak},
             "kernels_ms_per_launch": {k: round(v[0], 5) for k, v in prof.items() if v[1] > 0},
@@ -303,6 +370,14 @@ def main():
         line["clocks"] = clocks
     if rank == 0 and world == 1:
         line["cpu_baseline"] = cpu_baseline_sample(c)
+        if not args.no_arnoldi:
+            g.close()
+            lid = cs.lid_driven(n=128)
+            line["arnoldi"] = [
+                arnoldi_sample(cs, GattDNS, c, f, 32, 2, 10, 4321,
+                               "32 problems on the %d^3 periodic box base flow" % args.n),
+                arnoldi_sample(cs, GattDNS, lid, cs.uniform_flow(lid), 32, 2, 100, 4321,
+                               "32 problems on the 128^2 lid-driven cavity (rest state base)")]
     if rank == 0:
         print(json.dumps(line), flush=True)
     g.close()
