@@ -258,6 +258,7 @@ def main():
         dist.barrier()
     from gatt_dns_b200 import case as cs
     from gatt_dns_b200.solver import GattDNS
+    from gatt_dns_b200.shard import max_over_ranks
 
     c = cs.periodic_box(n=args.n)
     f = cs.solenoidal_turbulence(c, seed=1234 + rank)
@@ -299,10 +300,7 @@ def main():
     launches = g.kernel_launches() - l0
     ms = ev0.elapsed_time(ev1)
     t += args.steps * dt
-    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    ms_max = max_over_ranks(ms, dist if world > 1 else None, device="cuda")
     value = world * npts * STAGES * args.steps / (ms_max / 1e3) / 1e6
 
     # ---- end-to-end through the C-ABI with host buffers ------------------------------
@@ -319,10 +317,8 @@ def main():
     torch.cuda.synchronize()
     wall = time.perf_counter() - w0
     e_ms = max(e0.elapsed_time(e1), wall * 1e3)
-    et = torch.tensor([e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(et, op=dist.ReduceOp.MAX)
-    e2e_value = world * npts * STAGES * args.steps / (float(et.item()) / 1e3) / 1e6
+    e2e_value = world * npts * STAGES * args.steps / (max_over_ranks(e_ms, dist if world > 1 else None,
+                                                                     device="cuda") / 1e3) / 1e6
     field_bytes = 5 * npts * 8
     h2d = (field_bytes + args.steps * 24) / args.steps
     d2h = (field_bytes + args.steps * 5 * 8) / args.steps
