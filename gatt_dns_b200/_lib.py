@@ -50,6 +50,10 @@ SIGNATURES = {
     "gatt_arnoldi": (_c_int, [_c_void_p, _c_int, _c_int, _c_double, _c_double, _c_double, _pd, _pd,
                               ctypes.c_void_p, _pd]),
     "gatt_arnoldi_vector": (_c_int, [_c_void_p, _c_int, _c_int, _pd]),
+    "gatt_rhs_jvp": (_c_int, [_c_void_p, _pd, _pd, _pd]),
+    "gatt_rhs_vjp": (_c_int, [_c_void_p, _pd, _pd, _pd]),
+    "gatt_jvp": (_c_int, [_c_void_p, _c_int, _c_double, _c_double, _pd, _pd]),
+    "gatt_vjp": (_c_int, [_c_void_p, _c_int, _c_double, _c_double, _c_int, _pd, _pd]),
     "gatt_synchronize": (_c_int, [_c_void_p]),
     "gatt_kernel_launches": (ctypes.c_longlong, [_c_void_p]),
     "gatt_profile_kernels": (_c_int, [_c_void_p, _c_double, _c_double, _c_int, _pd, _pd]),

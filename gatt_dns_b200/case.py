@@ -442,7 +442,9 @@ def build_matrices(X, Y, Z, flow_region, periodic, fix_periodic, domain_ends, de
         m = mx.prepare_thomas(L, R, fL, fR, tmap)
         blocks = mx.get_matrix_type_blocks(tmap, 1, 1)[0]
         m.blocks = blocks
-        out.append(m.rounded() if round_fortran else m)
+        m = m.rounded() if round_fortran else m
+        m.adj = mx.adjoint_sets(L, R, fL, fR, tmap)
+        out.append(m)
     return out
 
 

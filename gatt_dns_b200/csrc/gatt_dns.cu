@@ -19,6 +19,7 @@
 
 #include "../../include/gatt_dns.h"
 #include "arnoldi.cuh"
+#include "tangent.cuh"
 #include "bc.cuh"
 #include "pointwise.cuh"
 #include "rsweep.cuh"
@@ -53,6 +54,10 @@ int fail(int code, const std::string &msg)
 // Line-solve kernel families: shared-memory tile (any N), register-resident rows loaded
 // from global memory, register-resident rows fed by a TMA ring (persistent CTAs).
 enum SweepFamily { FAM_TILE = 0, FAM_REG = 1, FAM_PIPE = 2 };
+
+// Matrix kinds per direction: 0 derivative, 1 filter, 2/3 derivative transpose (LHS^T solve,
+// then R^T band), 4/5 filter transpose (same split); see gatt_set_matrices.
+constexpr int kMatKinds = 6;
 
 struct DevDir {
     bool set = false;
@@ -94,7 +99,7 @@ struct gatt_ctx {
     bool is3d;
     Phys ph{};
     bool phys_set = false;
-    DevDir mat[3][2];
+    DevDir mat[3][kMatKinds];  // kinds: derivative, filter, and the four transposed operators
     uint8_t *ltype[3] = {nullptr, nullptr, nullptr};
     bool lt_set[3] = {false, false, false};
     int lt_max[3] = {0, 0, 0};  // largest 0-based type in each direction's map
@@ -126,6 +131,15 @@ struct gatt_ctx {
     uint8_t *arn_region = nullptr;
     int arn_m = 0;       // basis vectors held: m + 1 per member
     bool arn_have_region = false;
+    // tangent-linear / adjoint work arrays (5-field sets unless noted), allocated on first use
+    double *dx[5] = {};                  // base states: step start and stage states
+    double *dy[3] = {};                  // tangent states
+    double *t_delta = nullptr, *t_d1 = nullptr, *t_tq = nullptr, *t_d2 = nullptr;  // tangent RK increment, 15, 9, 12
+    double *a_lam = nullptr, *a_acc = nullptr, *a_arg = nullptr, *a_prev = nullptr, *a_g = nullptr;
+    double *a_lq = nullptr, *a_ld1 = nullptr, *a_ltau = nullptr, *a_lvt = nullptr;  // 5, 15, 9, 4
+    double *a_s1 = nullptr, *a_s2 = nullptr, *a_scr = nullptr;                       // 15, 12, 5
+    double *a_ckpt = nullptr, *a_seg = nullptr;
+    int a_nckpt = 0, a_nseg = 0;
     bool mean_init = false;                  // SFD mean uploaded or copied from the state
     int cur = 0;
     unsigned long long *acc = nullptr;
@@ -507,7 +521,7 @@ int sweep(gatt_ctx *c, int d, int kind, const double *in, long long in_bs, const
 
 // nseq2d/nseq3d on stage input q, fused with the RK4 update into out (mode).
 int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet &out, int mode, int nmem,
-              double *d1, double *tq, double *d2, double *delta)
+              double *d1, double *tq, double *d2, double *delta, bool assemble = true)
 {
     const long long n = c->npts;
     const double *qin = q.v[0];
@@ -533,6 +547,7 @@ int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet
         TRY(sweep(c, 0, 0, tq, btq, ix, d2, bd2, sx, 4, nmem, 0, nullptr, PC_D2X));
         TRY(sweep(c, 1, 0, tq, btq, iy, d2, bd2, sy, 4, nmem, 0, nullptr, PC_D2Y));
         TRY(sweep(c, 2, 0, tq, btq, iz, d2, bd2, sz, 4, nmem, 0, nullptr, PC_D2Z));
+        if (!assemble) return GATT_OK;  // the gradients and second sweeps only (tangent / adjoint)
         TRY(before_launch(c, PC_ASSEMBLE));
         k_assemble3d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(
             c->ph, q, q0, out, fset(c, delta, 5), fset(c, d1, D3_N), fset(c, d2, S3_N), n, mode, sp);
@@ -1057,6 +1072,328 @@ int arnoldi(gatt_ctx *c, int m, int nsteps, double t0, double dt, double eps, co
     return GATT_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// Tangent-linear and adjoint of the 3-D step (no counterpart in the reference)
+// ---------------------------------------------------------------------------
+
+StateSet set5(const gatt_ctx *c, double *p)
+{
+    StateSet s;
+    for (int f = 0; f < 5; f++) s.v[f] = p + f * c->npts;
+    s.bstride = 5 * c->npts;
+    return s;
+}
+
+int copy_set5(gatt_ctx *c, double *dst, const double *src)
+{
+    CU(cudaMemcpyAsync(dst, src, sizeof(double) * 5 * (size_t)c->npts * c->nb, cudaMemcpyDeviceToDevice, c->stream));
+    return GATT_OK;
+}
+
+// copy between a context state slot (separate per-variable pointers) and a 5-field set
+int state_to_set(gatt_ctx *c, const StateSet &q, double *dst, bool to_set)
+{
+    for (int b = 0; b < c->nb; b++)
+        for (int f = 0; f < 5; f++) {
+            double *sp = q.v[f] + b * q.bstride, *dp = dst + ((size_t)b * 5 + f) * c->npts;
+            if (to_set) CU(cudaMemcpyAsync(dp, sp, sizeof(double) * c->npts, cudaMemcpyDeviceToDevice, c->stream));
+            else CU(cudaMemcpyAsync(sp, dp, sizeof(double) * c->npts, cudaMemcpyDeviceToDevice, c->stream));
+        }
+    return GATT_OK;
+}
+
+// The tangent and the adjoint are built for 3-D cases whose step is RK4 + filter: no
+// boundary-condition program, no disturbances, no SFD.
+int check_diff(gatt_ctx *c, bool adjoint)
+{
+    TRY(check_ready(c, true));
+    if (!c->is3d) return fail(GATT_ERR_STATE, "tangent and adjoint are built for 3-D cases");
+    if (c->sfd_type > 0) return fail(GATT_ERR_STATE, "tangent and adjoint are built for cases without SFD");
+    if (c->bc_dirty) TRY(build_bc_program(c));
+    if (c->nops > 0)
+        return fail(GATT_ERR_STATE, "tangent and adjoint are built for cases without boundary conditions");
+    if (adjoint)
+        for (int d = 0; d < 3; d++) {
+            if (!c->mat[d][2].set || !c->mat[d][3].set)
+                return fail(GATT_ERR_STATE, "transposed derivative matrices (kinds 2, 3) missing");
+            if (c->filt[d] && (!c->mat[d][4].set || !c->mat[d][5].set))
+                return fail(GATT_ERR_STATE, "transposed filter matrices (kinds 4, 5) missing");
+        }
+    return GATT_OK;
+}
+
+int diff_alloc(gatt_ctx *c, bool adjoint)
+{
+    for (double *&p : c->dx) if (!p) TRY(alloc_fields(c, &p, 5, c->nb));
+    if (!adjoint) {
+        for (double *&p : c->dy) if (!p) TRY(alloc_fields(c, &p, 5, c->nb));
+        if (!c->t_delta) TRY(alloc_fields(c, &c->t_delta, 5, c->nb));
+        if (!c->t_d1) TRY(alloc_fields(c, &c->t_d1, D3_N, c->nb));
+        if (!c->t_tq) TRY(alloc_fields(c, &c->t_tq, T3_N, c->nb));
+        if (!c->t_d2) TRY(alloc_fields(c, &c->t_d2, S3_N, c->nb));
+        return GATT_OK;
+    }
+    double **five[] = {&c->a_lam, &c->a_acc, &c->a_arg, &c->a_prev, &c->a_g, &c->a_lq, &c->a_scr};
+    for (double **p : five) if (!*p) TRY(alloc_fields(c, p, 5, c->nb));
+    if (!c->a_ld1) TRY(alloc_fields(c, &c->a_ld1, D3_N, c->nb));
+    if (!c->a_ltau) TRY(alloc_fields(c, &c->a_ltau, T3_N, c->nb));
+    if (!c->a_lvt) TRY(alloc_fields(c, &c->a_lvt, 4, c->nb));
+    if (!c->a_s1) TRY(alloc_fields(c, &c->a_s1, 15, c->nb));
+    if (!c->a_s2) TRY(alloc_fields(c, &c->a_s2, 12, c->nb));
+    return GATT_OK;
+}
+
+int set_params(gatt_ctx *c, int slot, double t, double dt)
+{
+    TRY(ensure_hist(c, slot + 1));
+    c->h_params[slot].t = t; c->h_params[slot].dt = dt; c->h_params[slot].slot = slot;
+    CU(cudaMemcpyAsync(c->d_params, &c->h_params[slot], sizeof(StepParams), cudaMemcpyHostToDevice, c->stream));
+    return GATT_OK;
+}
+
+// Tangent of one RK stage (mode 1..4, or RK_STORE_RHS for the bare RHS): the base stage
+// xin -> xout (the forward kernels), then the tangent yin -> yout.
+int tl_stage(gatt_ctx *c, const StateSet &xin, const StateSet &x0, const StateSet &xout, const StateSet &yin,
+             const StateSet &y0, const StateSet &yout, int mode)
+{
+    const int nm = c->nb;
+    const long long n = c->npts;
+    TRY(rhs_stage(c, xin, x0, xout, mode, nm, c->d1, c->tq, c->d2, c->delta));
+    const long long bd1 = D3_N * n, btq = T3_N * n, bd2 = S3_N * n;
+    const int fin[5] = {0, 1, 2, 3, 4};
+    const int ox[5] = {D3_UX, D3_VX, D3_WX, D3_RX, D3_EX};
+    const int oy[5] = {D3_UY, D3_VY, D3_WY, D3_RY, D3_EY};
+    const int oz[5] = {D3_UZ, D3_VZ, D3_WZ, D3_RZ, D3_EZ};
+    TRY(sweep(c, 0, 0, yin.v[0], yin.bstride, fin, c->t_d1, bd1, ox, 5, nm, 0, nullptr, PC_D1X));
+    TRY(sweep(c, 1, 0, yin.v[0], yin.bstride, fin, c->t_d1, bd1, oy, 5, nm, 0, nullptr, PC_D1Y));
+    TRY(sweep(c, 2, 0, yin.v[0], yin.bstride, fin, c->t_d1, bd1, oz, 5, nm, 0, nullptr, PC_D1Z));
+    TRY(before_launch(c, PC_VISC));
+    k_tl_tau3d<<<dim3(grid_for(c, n), nm), kBlock, 0, c->stream>>>(c->ph, xin, fset(c, c->d1, D3_N), yin,
+                                                                  fset(c, c->t_d1, D3_N), fset(c, c->t_tq, T3_N), n);
+    TRY(after_launch(c));
+    const int ix[4] = {T3_XX, T3_XY, T3_XZ, T3_QX}, sx[4] = {S3_TXXX, S3_TXYX, S3_TXZX, S3_HTX};
+    const int iy[4] = {T3_XY, T3_YY, T3_YZ, T3_QY}, sy[4] = {S3_TXYY, S3_TYYY, S3_TYZY, S3_HTY};
+    const int iz[4] = {T3_XZ, T3_YZ, T3_ZZ, T3_QZ}, sz[4] = {S3_TXZZ, S3_TYZZ, S3_TZZZ, S3_HTZ};
+    TRY(sweep(c, 0, 0, c->t_tq, btq, ix, c->t_d2, bd2, sx, 4, nm, 0, nullptr, PC_D2X));
+    TRY(sweep(c, 1, 0, c->t_tq, btq, iy, c->t_d2, bd2, sy, 4, nm, 0, nullptr, PC_D2Y));
+    TRY(sweep(c, 2, 0, c->t_tq, btq, iz, c->t_d2, bd2, sz, 4, nm, 0, nullptr, PC_D2Z));
+    TRY(before_launch(c, PC_ASSEMBLE));
+    k_tl_assemble3d<<<dim3(grid_for(c, n), nm), kBlock, 0, c->stream>>>(
+        c->ph, xin, fset(c, c->d1, D3_N), fset(c, c->d2, S3_N), yin, fset(c, c->t_d1, D3_N), fset(c, c->t_d2, S3_N),
+        y0, yout, fset(c, c->t_delta, 5), n, mode, c->d_params);
+    return after_launch(c);
+}
+
+// One step of base and tangent: dx[0], dy[0] = step start -> step end (same arrays)
+int tl_step(gatt_ctx *c)
+{
+    const StateSet X0 = set5(c, c->dx[0]), XA = set5(c, c->dx[1]), XB = set5(c, c->dx[2]);
+    const StateSet Y0 = set5(c, c->dy[0]), YA = set5(c, c->dy[1]), YB = set5(c, c->dy[2]);
+    TRY(tl_stage(c, X0, X0, XA, Y0, Y0, YA, RK_STAGE1));
+    TRY(tl_stage(c, XA, X0, XB, YA, Y0, YB, RK_STAGE2));
+    TRY(tl_stage(c, XB, X0, XA, YB, Y0, YA, RK_STAGE3));
+    TRY(tl_stage(c, XA, X0, XB, YA, Y0, YB, RK_STAGE4));
+    // the filter is linear: the same sweeps act on the tangent (main.F90:357-378)
+    const double *bdt = c->fct > 0 ? &c->d_params->dt : nullptr;
+    TRY(filter_set(c, XB, c->nb, 0.0, bdt));
+    TRY(filter_set(c, YB, c->nb, 0.0, bdt));
+    TRY(copy_set5(c, c->dx[0], c->dx[2]));
+    return copy_set5(c, c->dy[0], c->dy[2]);
+}
+
+// transposed line operator L^T = R^T (LHS^T)^-1 of direction d over nf fields: kind k0 (the
+// LHS^T solve) into the scratch, then kind k0+1 (the R^T band) into the output slots
+int sweep_T(gatt_ctx *c, int d, int k0, const double *in, long long in_bs, const int *in_slots, double *out,
+            long long out_bs, const int *out_slots, int nf)
+{
+    int sl[16];
+    for (int f = 0; f < nf; f++) sl[f] = f;
+    TRY(sweep(c, d, k0, in, in_bs, in_slots, c->a_scr, 5 * c->npts, sl, nf, c->nb, 0.0, nullptr, PC_OTHER));
+    return sweep(c, d, k0 + 1, c->a_scr, 5 * c->npts, sl, out, out_bs, out_slots, nf, c->nb, 0.0, nullptr, PC_OTHER);
+}
+
+// G = F'(q)^T a (the adjoint of the RHS at state q)
+int adj_rhs(gatt_ctx *c, const StateSet &q, const StateSet &a, const StateSet &G)
+{
+    const int nm = c->nb;
+    const long long n = c->npts;
+    TRY(rhs_stage(c, q, q, q, RK_STORE_RHS, nm, c->d1, c->tq, c->d2, nullptr, false));
+    TRY(before_launch(c, PC_OTHER));
+    k_adj_asm3d<<<dim3(grid_for(c, n), nm), kBlock, 0, c->stream>>>(
+        c->ph, q, fset(c, c->d1, D3_N), fset(c, c->d2, S3_N), a, fset(c, c->a_lq, 5), fset(c, c->a_ld1, D3_N),
+        fset(c, c->a_ltau, T3_N), fset(c, c->a_lvt, 4), n);
+    TRY(after_launch(c));
+    // transposed second sweeps: (vtx, vty, vtz, ht) -> stress / heat-flux contributions
+    const int v4[4] = {0, 1, 2, 3};
+    for (int d = 0; d < 3; d++) {
+        const int o4[4] = {4 * d, 4 * d + 1, 4 * d + 2, 4 * d + 3};
+        TRY(sweep_T(c, d, 2, c->a_lvt, 4 * n, v4, c->a_s2, 12 * n, o4, 4));
+    }
+    TRY(before_launch(c, PC_OTHER));
+    k_adj_tau3d<<<dim3(grid_for(c, n), nm), kBlock, 0, c->stream>>>(c->ph, q, fset(c, c->d1, D3_N),
+                                                                   fset(c, c->a_ltau, T3_N), fset(c, c->a_s2, 12),
+                                                                   fset(c, c->a_ld1, D3_N), fset(c, c->a_lq, 5), n);
+    TRY(after_launch(c));
+    // transposed first sweeps: gradient lambdas -> state lambdas
+    for (int d = 0; d < 3; d++) {
+        const int i5[5] = {D3_UX + d, D3_VX + d, D3_WX + d, D3_RX + d, D3_EX + d};
+        const int o5[5] = {5 * d, 5 * d + 1, 5 * d + 2, 5 * d + 3, 5 * d + 4};
+        TRY(sweep_T(c, d, 2, c->a_ld1, (long long)D3_N * n, i5, c->a_s1, 15 * n, o5, 5));
+    }
+    TRY(before_launch(c, PC_OTHER));
+    k_adj_q3d<<<dim3(grid_for(c, n), nm), kBlock, 0, c->stream>>>(fset(c, c->a_lq, 5), fset(c, c->a_s1, 15), G, n);
+    return after_launch(c);
+}
+
+int axpby5(gatt_ctx *c, double *out, const double *x, const double *y, double alpha, double beta)
+{
+    TRY(before_launch(c, PC_OTHER));
+    k_axpby5<<<dim3(grid_for(c, c->npts), c->nb), kBlock, 0, c->stream>>>(
+        set5(c, out), set5(c, const_cast<double *>(x)), set5(c, const_cast<double *>(y ? y : x)), alpha, beta,
+        y != nullptr, c->npts);
+    return after_launch(c);
+}
+
+// Adjoint of one step: a_lam holds lambda at the step end; dx[0] the step's start state.
+// Reverse of: 4 RK stages (timeIntegration.F90:338-498), then the x -> y -> z filter.
+int adj_step(gatt_ctx *c, double dt)
+{
+    const StateSet X[5] = {set5(c, c->dx[0]), set5(c, c->dx[1]), set5(c, c->dx[2]), set5(c, c->dx[3]),
+                           set5(c, c->dx[4])};
+    // recompute the stage inputs q1, q2, q3 (q4, the pre-filter state, is not needed)
+    for (int s = 1; s <= 3; s++) TRY(rhs_stage(c, X[s - 1], X[0], X[s], s, c->nb, c->d1, c->tq, c->d2, c->delta));
+    // filter^T, z -> y -> x; with the time blend lam = lam + b (F^T lam - lam)
+    const int f5[5] = {0, 1, 2, 3, 4};
+    for (int d = 2; d >= 0; d--) {
+        if (!c->filt[d]) continue;
+        if (c->fct > 0) {
+            TRY(sweep_T(c, d, 4, c->a_lam, 5 * c->npts, f5, c->a_g, 5 * c->npts, f5, 5));
+            TRY(before_launch(c, PC_OTHER));
+            k_adj_blend5<<<dim3(grid_for(c, c->npts), c->nb), kBlock, 0, c->stream>>>(
+                set5(c, c->a_lam), set5(c, c->a_g), c->d_params, c->fct, c->npts);
+            TRY(after_launch(c));
+        } else {
+            TRY(sweep_T(c, d, 4, c->a_lam, 5 * c->npts, f5, c->a_lam, 5 * c->npts, f5, 5));
+        }
+    }
+    // RK4: q4 = q0 + dt/6 k1 + dt/3 k2 + dt/3 k3 + dt/6 k4, q1 = q0 + dt/2 k1,
+    // q2 = q0 + dt/2 k2, q3 = q0 + dt k3, k_s = F(q_{s-1})
+    const StateSet A = set5(c, c->a_arg), G = set5(c, c->a_g);
+    TRY(copy_set5(c, c->a_acc, c->a_lam));
+    const double wl[4] = {dt / 6.0, dt / 3.0, dt / 3.0, dt / 6.0};  // weight of lambda4 in a_s (s = 4..1)
+    const double wp[4] = {0.0, dt, dt / 2.0, dt / 2.0};             // weight of lambda_{q_s}
+    for (int i = 0; i < 4; i++) {
+        const int s = 3 - i;  // stage state q_s feeds k_{s+1}
+        TRY(axpby5(c, c->a_arg, c->a_lam, i ? c->a_prev : nullptr, wl[i], wp[i]));
+        TRY(adj_rhs(c, X[s], A, G));
+        TRY(axpby5(c, c->a_acc, c->a_acc, c->a_g, 1.0, 1.0));
+        if (s > 0) TRY(copy_set5(c, c->a_prev, c->a_g));
+    }
+    return copy_set5(c, c->a_lam, c->a_acc);
+}
+
+int upload5(gatt_ctx *c, double *dst, const double *host)
+{
+    CU(cudaMemcpyAsync(dst, host, sizeof(double) * 5 * (size_t)c->npts * c->nb, cudaMemcpyHostToDevice, c->stream));
+    return GATT_OK;
+}
+
+int download5(gatt_ctx *c, double *host, const double *src)
+{
+    CU(cudaMemcpyAsync(host, src, sizeof(double) * 5 * (size_t)c->npts * c->nb, cudaMemcpyDeviceToHost, c->stream));
+    return sync_stream(c);
+}
+
+int rhs_jvp(gatt_ctx *c, const double *q, const double *dq, double *dk)
+{
+    TRY(check_diff(c, false));
+    TRY(diff_alloc(c, false));
+    TRY(upload5(c, c->dx[0], q));
+    TRY(upload5(c, c->dy[0], dq));
+    const StateSet X0 = set5(c, c->dx[0]), Y0 = set5(c, c->dy[0]);
+    TRY(tl_stage(c, X0, X0, set5(c, c->dx[1]), Y0, Y0, set5(c, c->dy[1]), RK_STORE_RHS));
+    return download5(c, dk, c->dy[1]);
+}
+
+int rhs_vjp(gatt_ctx *c, const double *q, const double *a, double *lam)
+{
+    TRY(check_diff(c, true));
+    TRY(diff_alloc(c, true));
+    TRY(upload5(c, c->dx[0], q));
+    TRY(upload5(c, c->a_arg, a));
+    TRY(adj_rhs(c, set5(c, c->dx[0]), set5(c, c->a_arg), set5(c, c->a_g)));
+    return download5(c, lam, c->a_g);
+}
+
+int jvp(gatt_ctx *c, int nsteps, double t0, double dt, const double *dq0, double *dqN)
+{
+    TRY(check_diff(c, false));
+    if (nsteps < 1 || !(dt > 0) || !dq0 || !dqN) return fail(GATT_ERR_BADARG, "bad nsteps, dt or arrays");
+    TRY(diff_alloc(c, false));
+    TRY(state_to_set(c, state_set(c, 0), c->dx[0], true));
+    TRY(upload5(c, c->dy[0], dq0));
+    double t = t0;
+    for (int s = 0; s < nsteps; s++) {
+        TRY(set_params(c, 0, t, dt));
+        TRY(tl_step(c));
+        TRY(sync_stream(c));  // the parameter slot is reused
+        t = t + dt;
+    }
+    TRY(state_to_set(c, state_set(c, 0), c->dx[0], false));
+    return download5(c, dqN, c->dy[0]);
+}
+
+// Checkpointed reverse sweep: states every `every` steps are kept on the forward pass; each
+// segment is recomputed from its checkpoint (storing every step's start state), then its
+// steps are reversed.  Leaves the context state at the end of the forward run.
+int vjp(gatt_ctx *c, int nsteps, double t0, double dt, int every, const double *lamN, double *lam0)
+{
+    TRY(check_diff(c, true));
+    if (nsteps < 1 || every < 1 || !(dt > 0) || !lamN || !lam0) return fail(GATT_ERR_BADARG, "bad nsteps, dt or arrays");
+    TRY(diff_alloc(c, true));
+    const int nck = (nsteps + every - 1) / every, seg = std::min(every, nsteps);
+    const size_t st = 5 * (size_t)c->npts * c->nb;
+    if (c->a_nckpt < nck + 1) {
+        cudaFree(c->a_ckpt);
+        c->a_ckpt = nullptr;
+        c->a_nckpt = 0;
+        CU(cudaMalloc(&c->a_ckpt, sizeof(double) * st * (nck + 1)));
+        c->a_nckpt = nck + 1;
+    }
+    if (c->a_nseg < seg) {
+        cudaFree(c->a_seg);
+        c->a_seg = nullptr;
+        c->a_nseg = 0;
+        CU(cudaMalloc(&c->a_seg, sizeof(double) * st * seg));
+        c->a_nseg = seg;
+    }
+    // forward: checkpoints at steps 0, every, 2*every, ...; slot nck keeps the final state
+    for (int k = 0; k < nck; k++) {
+        TRY(state_to_set(c, state_set(c, 0), c->a_ckpt + st * k, true));
+        const int len = std::min(every, nsteps - k * every);
+        TRY(run_steps(c, len, t0 + (double)(k * every) * dt, dt, nullptr, false));
+    }
+    TRY(state_to_set(c, state_set(c, 0), c->a_ckpt + st * nck, true));
+    TRY(upload5(c, c->a_lam, lamN));
+    for (int k = nck - 1; k >= 0; k--) {
+        const int len = std::min(every, nsteps - k * every);
+        TRY(state_to_set(c, state_set(c, 0), c->a_ckpt + st * k, false));
+        for (int i = 0; i < len; i++) {
+            TRY(state_to_set(c, state_set(c, 0), c->a_seg + st * i, true));
+            if (i + 1 < len) TRY(run_steps(c, 1, t0 + (double)(k * every + i) * dt, dt, nullptr, false));
+        }
+        for (int i = len - 1; i >= 0; i--) {
+            TRY(copy_set5(c, c->dx[0], c->a_seg + st * i));
+            TRY(set_params(c, 0, t0 + (double)(k * every + i) * dt, dt));
+            TRY(adj_step(c, dt));
+            TRY(sync_stream(c));
+        }
+    }
+    TRY(state_to_set(c, state_set(c, 0), c->a_ckpt + st * nck, false));
+    return download5(c, lam0, c->a_lam);
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1139,7 +1476,7 @@ void gatt_destroy(gatt_ctx *c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     invalidate_graphs(c);
     for (int d = 0; d < 3; d++) {
-        for (int k = 0; k < 2; k++) {
+        for (int k = 0; k < kMatKinds; k++) {
             DevDir &m = c->mat[d][k];
             cudaFree(m.Rm);
             cudaFree(m.Q);
@@ -1150,6 +1487,11 @@ void gatt_destroy(gatt_ctx *c)
                       c->d_coef1, c->d_coef2, c->d_xs, c->arn_zeta, c->arn_B, c->arn_base, c->arn_um,
                       c->arn_part, c->arn_h};
     cudaFree(c->arn_region);
+    for (double *p : c->dx) cudaFree(p);
+    for (double *p : c->dy) cudaFree(p);
+    double *dbufs[] = {c->t_delta, c->t_d1, c->t_tq, c->t_d2, c->a_lam, c->a_acc, c->a_arg, c->a_prev, c->a_g,
+                       c->a_lq, c->a_ld1, c->a_ltau, c->a_lvt, c->a_s1, c->a_s2, c->a_scr, c->a_ckpt, c->a_seg};
+    for (double *p : dbufs) cudaFree(p);
     for (double *p : bufs) cudaFree(p);
     cudaFree(c->d_ops); cudaFree(c->acc); cudaFree(c->d_params);
     if (c->h_params) cudaFreeHost(c->h_params);
@@ -1191,7 +1533,8 @@ int gatt_set_matrices(gatt_ctx *c, int dir, int kind, int periodic, int nRHS, in
                       const int *blocks)
 {
     if (!c) return fail(GATT_ERR_BADARG, "null context");
-    if (dir < 1 || dir > 3 || kind < 0 || kind > 1) return fail(GATT_ERR_BADARG, "dir must be 1..3 and kind 0..1");
+    if (dir < 1 || dir > 3 || kind < 0 || kind >= kMatKinds)
+        return fail(GATT_ERR_BADARG, "dir must be 1..3 and kind 0..5");
     const int d = dir - 1;
     const int N = line_len(c, d);
     if (periodic != 0 && periodic != 1) return fail(GATT_ERR_BADARG, "periodic must be 0 or 1");
@@ -1509,7 +1852,7 @@ int gatt_apply_bc(gatt_ctx *c, double t)
 int gatt_deriv_dir(gatt_ctx *c, int dir, int kind, const double *F, double *dF)
 {
     if (!c) return fail(GATT_ERR_BADARG, "null context");
-    if (dir < 1 || dir > 3 || kind < 0 || kind > 1 || !F || !dF) return fail(GATT_ERR_BADARG, "bad arguments");
+    if (dir < 1 || dir > 3 || kind < 0 || kind >= kMatKinds || !F || !dF) return fail(GATT_ERR_BADARG, "bad arguments");
     if (line_len(c, dir - 1) < 2) return fail(GATT_ERR_BADARG, "direction has a single node");
     TRY(ensure_host_scratch(c));
     CU(cudaMemcpyAsync(c->tin, F, sizeof(double) * c->npts, cudaMemcpyHostToDevice, c->stream));
@@ -1602,6 +1945,30 @@ int gatt_arnoldi_vector(gatt_ctx *c, int b, int j, double *out)
     }
     TRY(sync_stream(c));
     return GATT_OK;
+}
+
+int gatt_rhs_jvp(gatt_ctx *c, const double *q, const double *dq, double *dk)
+{
+    if (!c || !q || !dq || !dk) return fail(GATT_ERR_BADARG, "null argument");
+    return rhs_jvp(c, q, dq, dk);
+}
+
+int gatt_rhs_vjp(gatt_ctx *c, const double *q, const double *a, double *lam)
+{
+    if (!c || !q || !a || !lam) return fail(GATT_ERR_BADARG, "null argument");
+    return rhs_vjp(c, q, a, lam);
+}
+
+int gatt_jvp(gatt_ctx *c, int nsteps, double t0, double dt, const double *dq0, double *dqN)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    return jvp(c, nsteps, t0, dt, dq0, dqN);
+}
+
+int gatt_vjp(gatt_ctx *c, int nsteps, double t0, double dt, int checkpoint_every, const double *lamN, double *lam0)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    return vjp(c, nsteps, t0, dt, checkpoint_every, lamN, lam0);
 }
 
 int gatt_synchronize(gatt_ctx *c)

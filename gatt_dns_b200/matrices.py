@@ -352,6 +352,7 @@ class DirectionMatrices:
     nRHSf: int
     types: np.ndarray = field(default=None)      # per-line type map (1-based), 2-D
     blocks: np.ndarray = field(default=None)     # (nBlocks, 5) 1-based
+    adj: list = field(default=None)              # transposed operators (adjoint_sets), or None
 
     def rounded(self):
         """Copy with every coefficient passed through the ``%.20f`` text format."""
@@ -444,6 +445,59 @@ def prepare_thomas(LHS, RHS, fLHS, fRHS, types):
     return DirectionMatrices(periodic=int(bool(is_periodic)), nTypes=ntypes, A=A, B=B, C=C, D=D, R=R, nRHS=nR,
                              Af=Af, Bf=Bf, Cf=Cf, Df=Df, Rf=Rf, nRHSf=nRf,
                              types=np.asarray(types))
+
+
+@dataclass
+class OperatorSet:
+    """One compact line operator x = LHS^-1 (R f) in the factored form the C-ABI takes
+    (the arrays of one ``gatt_set_matrices`` call)."""
+    periodic: int
+    nTypes: int
+    A: np.ndarray
+    B: np.ndarray
+    C: np.ndarray
+    D: np.ndarray
+    R: np.ndarray
+    nRHS: int
+
+
+def _identity_factors(N, ntypes, periodic):
+    """Thomas factors of the identity LHS (cyclic form when periodic: D = e_1, no corners)."""
+    if periodic:
+        D = np.zeros((N, ntypes))
+        D[0, :] = 1.0
+        return np.zeros((N - 1, ntypes)), np.ones((N - 1, ntypes)), np.zeros((N - 1, ntypes)), D
+    return np.zeros((N - 1, ntypes)), np.ones((N, ntypes)), np.zeros((N - 1, ntypes)), np.zeros((N, ntypes))
+
+
+def _identity_band(N, ntypes):
+    R = np.zeros((N, 3, ntypes))
+    R[:, 1, :] = 1.0
+    return R
+
+
+def adjoint_sets(LHS, RHS, fLHS, fRHS, types):
+    """Transposes of the derivative and filter line operators, each as two operators the
+    forward kernels run: L^T = (LHS^-1 R)^T = R^T (LHS^T)^-1 is a solve with LHS^T and an
+    identity band, then a band product with R^T and an identity LHS.  Returns
+    [deriv LHS^T solve, deriv R^T band, filter LHS^T solve, filter R^T band]
+    (``gatt_set_matrices`` kinds 2..5)."""
+    ntypes = int(np.max(types))
+    N = LHS[0].shape[0]
+    eye = [np.eye(N) for _ in range(ntypes)]
+    lt = prepare_thomas([m.T.copy() for m in LHS], eye, [m.T.copy() for m in fLHS], eye, types)
+    per = lt.periodic
+    out = []
+    for A, B, C, D, Rt in ((lt.A, lt.B, lt.C, lt.D, RHS), (lt.Af, lt.Bf, lt.Cf, lt.Df, fRHS)):
+        out.append(OperatorSet(per, ntypes, A, B, C, D if per else np.zeros((N, ntypes)), _identity_band(N, ntypes), 2))
+        stack = np.stack([np.asarray(Rt[t], dtype=np.float64).T for t in range(ntypes)], axis=2)
+        band, nd = _rhs_diagonals(stack, filter_rule=True)
+        if nd < 2:
+            band = np.concatenate([np.zeros((N, 1, ntypes)), band, np.zeros((N, 1, ntypes))], axis=1)
+            nd = 2
+        iA, iB, iC, iD = _identity_factors(N, ntypes, per)
+        out.append(OperatorSet(per, ntypes, iA, iB, iC, iD, band, nd))
+    return out
 
 
 # ---------------------------------------------------------------------------

@@ -71,6 +71,12 @@ class GattDNS:
                 _lib.check(L.gatt_set_matrices(self.h, d + 1, kind, m.periodic, nR, m.nTypes, _dp(A), _dp(B), _dp(C),
                                                _dp(D) if m.periodic else None, _dp(R), nb, _ip(blocks)),
                            "gatt_set_matrices")
+            # transposed operators for the adjoint (kinds 2..5), when the emitter produced them
+            for k, s in enumerate(m.adj or []):
+                A, B, C, D, R = _f64(s.A), _f64(s.B), _f64(s.C), _f64(s.D), _f64(s.R)
+                _lib.check(L.gatt_set_matrices(self.h, d + 1, 2 + k, s.periodic, s.nRHS, s.nTypes, _dp(A), _dp(B),
+                                               _dp(C), _dp(D) if s.periodic else None, _dp(R), 0, None),
+                           "gatt_set_matrices")
         fd = c.filterDirections
         _lib.check(L.gatt_set_filter(self.h, fd[0], fd[1], fd[2], c.filterCharTime), "gatt_set_filter")
         bc = c.bc
@@ -161,11 +167,17 @@ class GattDNS:
         return ctypes.cast(p, ctypes.c_void_p).value
 
     # -- reference operations ----------------------------------------------
+    KINDS = {"deriv": 0, "filter": 1, "deriv_lhsT": 2, "deriv_rT": 3, "filter_lhsT": 4, "filter_rT": 5}
+
     def calc_derivs(self, F, direction, kind="deriv"):
-        """solveSystem{X,Y,Z}[per] of one field (derivs.F90:556-948)."""
+        """solveSystem{X,Y,Z}[per] of one field (derivs.F90:556-948); kind also names the
+        transposed operators: "deriv_T" / "filter_T" apply both halves (L^T)."""
         F = _f64(F)
+        if kind in ("deriv_T", "filter_T"):
+            base = kind[:-2]
+            return self.calc_derivs(self.calc_derivs(F, direction, base + "_lhsT"), direction, base + "_rT")
         out = np.zeros_like(F, order="F")
-        _lib.check(self.lib.gatt_deriv_dir(self.h, direction, 0 if kind == "deriv" else 1, _dp(F), _dp(out)),
+        _lib.check(self.lib.gatt_deriv_dir(self.h, direction, self.KINDS[kind], _dp(F), _dp(out)),
                    "gatt_deriv_dir")
         return out
 
@@ -224,6 +236,50 @@ class GattDNS:
         _lib.check(self.lib.gatt_arnoldi_vector(self.h, b, j, _dp(out)), "gatt_arnoldi_vector")
         n = out.size // 5
         return {k: out[i * n:(i + 1) * n].reshape(s, order="F") for i, k in enumerate(("U", "V", "W", "R", "E"))}
+
+    # -- tangent-linear / adjoint (3-D, no boundary conditions, no SFD) ------------------
+    def _pack(self, flows):
+        """list (one per member) of flow dicts -> contiguous nbatch*5*npts vector"""
+        if isinstance(flows, dict):
+            flows = [flows]
+        return np.concatenate([_f64(f[k]).ravel(order="F") for f in flows for k in ("U", "V", "W", "R", "E")])
+
+    def _unpack(self, vec):
+        s = (self.case.nx, self.case.ny, self.case.nz)
+        n = self.case.nx * self.case.ny * self.case.nz
+        out = []
+        for b in range(self.nbatch):
+            out.append({k: vec[(b * 5 + i) * n:(b * 5 + i + 1) * n].reshape(s, order="F")
+                        for i, k in enumerate(("U", "V", "W", "R", "E"))})
+        return out if self.nbatch > 1 else out[0]
+
+    def rhs_jvp(self, q, dq):
+        """F'(q) dq of the right-hand side (nseq3d linearised)."""
+        qv, dv = self._pack(q), self._pack(dq)
+        out = np.zeros_like(qv)
+        _lib.check(self.lib.gatt_rhs_jvp(self.h, _dp(qv), _dp(dv), _dp(out)), "gatt_rhs_jvp")
+        return self._unpack(out)
+
+    def rhs_vjp(self, q, a):
+        """F'(q)^T a."""
+        qv, av = self._pack(q), self._pack(a)
+        out = np.zeros_like(qv)
+        _lib.check(self.lib.gatt_rhs_vjp(self.h, _dp(qv), _dp(av), _dp(out)), "gatt_rhs_vjp")
+        return self._unpack(out)
+
+    def jvp(self, dq0, nsteps, t0, dt):
+        """Tangent over nsteps steps from the current state (which advances, as run())."""
+        dv = self._pack(dq0)
+        out = np.zeros_like(dv)
+        _lib.check(self.lib.gatt_jvp(self.h, nsteps, t0, dt, _dp(dv), _dp(out)), "gatt_jvp")
+        return self._unpack(out)
+
+    def vjp(self, lamN, nsteps, t0, dt, checkpoint_every=20):
+        """Adjoint over nsteps steps from the current state, checkpointed."""
+        lv = self._pack(lamN)
+        out = np.zeros_like(lv)
+        _lib.check(self.lib.gatt_vjp(self.h, nsteps, t0, dt, checkpoint_every, _dp(lv), _dp(out)), "gatt_vjp")
+        return self._unpack(out)
 
     def max_velocity(self):
         v = np.zeros(3 * self.nbatch)

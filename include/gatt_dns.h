@@ -70,7 +70,12 @@ int gatt_set_physics(gatt_ctx *ctx, double Re, double Ma, double Pr, double gamm
  *   else may be NULL), R(N, 2*nRHS-1, nTypes); blocks(nBlocks,5) = derivBlocks? with
  *   1-based (type, a1, a2, b1, b2) line ranges.  The blocks must cover every line of the
  *   direction exactly once.  The filter uses the derivative blocks (main.F90:360), so
- *   kind 1 may pass nBlocks = 0 to reuse them. */
+ *   kind 1 may pass nBlocks = 0 to reuse them.
+ * Kinds 2..5 (no counterpart in the reference) hold the transposed operators the adjoint
+ * needs, in the same factored form: a line operator L = LHS^-1 R has
+ * L^T = R^T (LHS^T)^-1, so kind 2 = derivative LHS^T with an identity band, kind 3 =
+ * identity LHS with the derivative R^T band, kinds 4 / 5 the same for the filter
+ * (gatt_dns_b200/matrices.py: adjoint_sets emits them); they reuse the blocks. */
 int gatt_set_matrices(gatt_ctx *ctx, int dir, int kind, int periodic, int nRHS, int nTypes,
                       const double *A, const double *B, const double *C, const double *D,
                       const double *R, int nBlocks, const int *blocks);
@@ -127,7 +132,8 @@ int gatt_state_device_ptr(gatt_ctx *ctx, int b, int var, double **dptr);
 int gatt_apply_bc(gatt_ctx *ctx, double t);
 
 /* One compact line solve -- solveSystem{X,Y,Z}[per] (derivs.F90:556-948) -- of the host
- * field F into dF with the derivative (kind 0) or filter (kind 1) coefficients of dir. */
+ * field F into dF with the derivative (kind 0) or filter (kind 1) coefficients of dir, or
+ * with one of the transposed-operator kinds 2..5. */
 int gatt_deriv_dir(gatt_ctx *ctx, int dir, int kind, const double *F, double *dF);
 
 /* Navier-Stokes right-hand side -- nseq2d / nseq3d (nseq.F90:10-323) -- of host fields;
@@ -174,6 +180,24 @@ int gatt_arnoldi(gatt_ctx *ctx, int m, int nsteps, double t0, double dt, double 
  * U, V, W, R, E of npts each (W zero in 2-D, zero outside the region): the psiA = zeta*psiH
  * mode reconstruction of calcInstability.m:419 is left to the caller. */
 int gatt_arnoldi_vector(gatt_ctx *ctx, int b, int j, double *out);
+
+/* Tangent-linear and adjoint of the 3-D RHS and time step (no counterpart in the reference;
+ * the reference linearises only by finite differences, calcInstability.m:353-390).  They
+ * cover 3-D cases whose step is RK4 + filter: no boundary-condition lists, no disturbances,
+ * no SFD (GATT_ERR_STATE otherwise); the adjoint also needs matrix kinds 2..5.  Arrays are
+ * host, nbatch*5*npts (member-major, then U, V, W, R, E).
+ *   gatt_rhs_jvp: dk = F'(q) dq of nseq3d (nseq.F90:142-323)
+ *   gatt_rhs_vjp: lam = F'(q)^T a
+ *   gatt_jvp:     dqN = (dPhi/dq) dq0 over nsteps steps of dt from the context state (which
+ *                 advances to the end state, as gatt_run)
+ *   gatt_vjp:     lam0 = (dPhi/dq)^T lamN over nsteps steps from the context state, keeping a
+ *                 checkpoint every checkpoint_every steps and recomputing each segment's
+ *                 states for the reverse sweep; the context state ends at the end state. */
+int gatt_rhs_jvp(gatt_ctx *ctx, const double *q, const double *dq, double *dk);
+int gatt_rhs_vjp(gatt_ctx *ctx, const double *q, const double *a, double *lam);
+int gatt_jvp(gatt_ctx *ctx, int nsteps, double t0, double dt, const double *dq0, double *dqN);
+int gatt_vjp(gatt_ctx *ctx, int nsteps, double t0, double dt, int checkpoint_every, const double *lamN,
+             double *lam0);
 
 /* max|U|, max|V|, max|W| of every member (main.F90:196-204), for the caller's CFL. */
 int gatt_max_velocity(gatt_ctx *ctx, double *vmax);

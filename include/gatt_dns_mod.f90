@@ -211,6 +211,34 @@ module gatt_dns
             real(c_double), dimension(*) :: out
             integer(c_int) :: gatt_arnoldi_vector
         end function
+        function gatt_rhs_jvp(ctx, q, dq, dk) bind(C, name='gatt_rhs_jvp')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: ctx
+            real(c_double), dimension(*) :: q, dq, dk
+            integer(c_int) :: gatt_rhs_jvp
+        end function
+        function gatt_rhs_vjp(ctx, q, a, lam) bind(C, name='gatt_rhs_vjp')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: ctx
+            real(c_double), dimension(*) :: q, a, lam
+            integer(c_int) :: gatt_rhs_vjp
+        end function
+        function gatt_jvp(ctx, nsteps, t0, dt, dq0, dqN) bind(C, name='gatt_jvp')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: ctx
+            integer(c_int), value :: nsteps
+            real(c_double), value :: t0, dt
+            real(c_double), dimension(*) :: dq0, dqN
+            integer(c_int) :: gatt_jvp
+        end function
+        function gatt_vjp(ctx, nsteps, t0, dt, checkpoint_every, lamN, lam0) bind(C, name='gatt_vjp')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: ctx
+            integer(c_int), value :: nsteps, checkpoint_every
+            real(c_double), value :: t0, dt
+            real(c_double), dimension(*) :: lamN, lam0
+            integer(c_int) :: gatt_vjp
+        end function
         function gatt_max_velocity(ctx, vmax) bind(C, name='gatt_max_velocity')
             import :: c_int, c_ptr, c_double
             type(c_ptr), value :: ctx

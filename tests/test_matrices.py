@@ -145,3 +145,53 @@ def test_derivative_regions_of_a_cavity():
     assert set(np.unique(reg["typeMapY"])) == {1, 2}
     # x lines: the fully solid row j=1 maps to the largest type
     assert reg["typeMapX"][0, 0] == reg["typeMapX"].max()
+
+
+def _apply_factored(A, B, C, D, R, nR, periodic, t, f):
+    """One line through a factored operator, in the kernels' row semantics (numpy)."""
+    N = f.size
+    rhs = np.zeros(N)
+    for i in range(N):
+        for l in range(2 * nR - 1):
+            rhs[i] += R[i, l, t] * f[(i + l - (nR - 1)) % N]
+    x = np.zeros(N)
+    if periodic:
+        x1 = D[:, t] @ rhs
+        rhs[1] -= A[0, t] * x1
+        rhs[N - 1] -= C[0, t] * x1
+        y = 0.0
+        for r in range(1, N):
+            y = (rhs[r] - (A[r - 1, t] if r >= 2 else 0.0) * y) * B[r - 1, t]
+            x[r] = y
+        xp = 0.0
+        for r in range(N - 1, 0, -1):
+            xp = x[r] - (C[r, t] if r <= N - 2 else 0.0) * xp
+            x[r] = xp
+        x[0] = x1
+    else:
+        y = 0.0
+        for r in range(N):
+            y = (rhs[r] - (A[r - 1, t] if r >= 1 else 0.0) * y) * B[r, t]
+            x[r] = y
+        xp = 0.0
+        for r in range(N - 1, -1, -1):
+            xp = x[r] - (C[r, t] if r <= N - 2 else 0.0) * xp
+            x[r] = xp
+    return x
+
+
+@pytest.mark.parametrize("which", ["periodic", "walls"])
+def test_adjoint_sets_are_transposes(which):
+    """Kinds 2+3 (and 4+5) applied in turn are the transposes of the derivative (filter)."""
+    from gatt_dns_b200 import case as cs
+    c = cs.periodic_box(n=12) if which == "periodic" else cs.lid_driven(n=14)
+    m = c.mats[0]
+    N = c.nx
+    fwd = [(m.A, m.B, m.C, m.D, m.R, m.nRHS), (m.Af, m.Bf, m.Cf, m.Df, m.Rf, m.nRHSf)]
+    for kind in range(2):
+        Lf = np.stack([_apply_factored(*fwd[kind], m.periodic, 0, e) for e in np.eye(N)], axis=1)
+        s1, s2 = m.adj[2 * kind], m.adj[2 * kind + 1]
+        Lt = np.stack([_apply_factored(s2.A, s2.B, s2.C, s2.D, s2.R, s2.nRHS, s2.periodic, 0,
+                                       _apply_factored(s1.A, s1.B, s1.C, s1.D, s1.R, s1.nRHS, s1.periodic, 0, e))
+                       for e in np.eye(N)], axis=1)
+        assert np.max(np.abs(Lt - Lf.T)) < 1e-12 * np.max(np.abs(Lf)), (which, kind)
