@@ -42,6 +42,7 @@ struct BcOp {
     int aux;        // divisor for corner averages
     int xoff;       // offset of the box's x coordinates (OP_LID)
     double val;
+    long long tape; // adjoint tape: offset of this op's recorded base values (-1: none)
 };
 
 struct BcProgram {
@@ -135,6 +136,246 @@ __global__ void k_bc(BcProgram pg, StateSet q, double *Pbase, long long pstride)
             }
         }
         // every item may read what the previous one wrote
+        __syncthreads();
+    }
+}
+
+// ---- tangent-linear and adjoint of the program (no counterpart in the reference) -------
+//
+// The program is a sequence of in-place box updates; the nonlinear ones (pressure Dirichlet,
+// P = R E, R = P / E, R = R / E / aux) need the base values they saw.  The tangent runs
+// base and tangent side by side; the adjoint runs the ops in reverse with those base values
+// read from a tape that k_bc_rec wrote while applying the program to the base state.
+// Values recorded per box point, in the box's loop order: OP_DIR_P: E; OP_P_LOAD: R, E;
+// OP_R_FROM_P: P, E; OP_R_DIV_E: R, E.
+
+__host__ __device__ __forceinline__ int bc_tape_width(int code)
+{
+    return code == OP_DIR_P ? 1 : (code == OP_P_LOAD || code == OP_R_FROM_P || code == OP_R_DIV_E) ? 2 : 0;
+}
+
+// Face point q of a Neumann op: the face node and the unit step into the domain.
+__device__ __forceinline__ void neumann_geom(const int *b, int dir, int len, long long q, int n1, int &i, int &j,
+                                             int &k, int &di, int &dj, int &dk)
+{
+    int a0, c0;
+    if (dir <= 2) { a0 = b[2]; c0 = b[4]; }
+    else if (dir <= 4) { a0 = b[0]; c0 = b[4]; }
+    else { a0 = b[0]; c0 = b[2]; }
+    const int a = a0 + (int)(q % n1), cc = c0 + (int)(q / n1);
+    const bool lo = (dir & 1);
+    const int s = lo ? 1 : -1;
+    di = dj = dk = 0;
+    if (dir <= 2) { i = lo ? b[0] : b[0] + len; di = s; j = a; k = cc; }
+    else if (dir <= 4) { j = lo ? b[2] : b[2] + len; dj = s; i = a; k = cc; }
+    else { k = lo ? b[4] : b[4] + len; dk = s; i = a; j = cc; }
+}
+
+__device__ __forceinline__ void neumann_extent(const int *b, int dir, int &n1, int &n2)
+{
+    if (dir <= 2) { n1 = b[3] - b[2] + 1; n2 = b[5] - b[4] + 1; }
+    else if (dir <= 4) { n1 = b[1] - b[0] + 1; n2 = b[5] - b[4] + 1; }
+    else { n1 = b[1] - b[0] + 1; n2 = b[3] - b[2] + 1; }
+}
+
+// the forward program on the base, recording the tape (same arithmetic as k_bc)
+__global__ void k_bc_rec(BcProgram pg, StateSet q, double *Pbase, long long pstride, double *tape, long long tstride)
+{
+    const int b = blockIdx.x;
+    double *F[5];
+#pragma unroll
+    for (int f = 0; f < 5; f++) F[f] = q.v[f] + b * q.bstride;
+    double *P = Pbase + b * pstride;
+    double *Rr = F[3], *Ee = F[4];
+    double *tp = tape + b * tstride;
+    for (int o = 0; o < pg.nops; o++) {
+        const BcOp op = pg.ops[o];
+        if (op.code == OP_NEU || op.code == OP_P_NEU) {
+            double *u = (op.code == OP_NEU) ? F[op.var] : P;
+            neumann_face(pg, u, op.box, op.dir, op.len, op.coef ? pg.coef2 : pg.coef1);
+            __syncthreads();
+            continue;
+        }
+        const int ni = op.box[1] - op.box[0] + 1, nj = op.box[3] - op.box[2] + 1, nk = op.box[5] - op.box[4] + 1;
+        const long long total = (long long)ni * nj * nk;
+        const int tw = bc_tape_width(op.code);
+        for (long long q2 = threadIdx.x; q2 < total; q2 += blockDim.x) {
+            const int i = op.box[0] + (int)(q2 % ni);
+            const int j = op.box[2] + (int)((q2 / ni) % nj);
+            const int k = op.box[4] + (int)(q2 / ((long long)ni * nj));
+            const long long p = bidx(pg, i, j, k);
+            double *t = tp + op.tape + tw * q2;
+            switch (op.code) {
+            case OP_SET: F[op.var][p] = op.val; break;
+            case OP_DIR_P: t[0] = Ee[p]; Rr[p] = op.val / (pg.gamma - 1.0) / Ee[p]; break;
+            case OP_P_LOAD: t[0] = Rr[p]; t[1] = Ee[p]; P[p] = Rr[p] * Ee[p]; break;
+            case OP_R_FROM_P: t[0] = P[p]; t[1] = Ee[p]; Rr[p] = P[p] / Ee[p]; break;
+            case OP_CORNER_E0: Ee[p] = 0.0; break;
+            case OP_P_FROM_E: P[p] = Ee[p]; break;
+            case OP_E_ADD_P: Ee[p] = Ee[p] + P[p]; break;
+            case OP_E_DIV: Ee[p] = Ee[p] / (double)op.aux; break;
+            case OP_R0: Rr[p] = 0.0; break;
+            case OP_R_ADD_P: Rr[p] = Rr[p] + P[p]; break;
+            case OP_R_DIV_E: t[0] = Rr[p]; t[1] = Ee[p]; Rr[p] = Rr[p] / Ee[p] / (double)op.aux; break;
+            case OP_LID: {
+                const double *x = pg.xs + op.xoff;
+                const double sx = 2 * (x[i - op.box[0]] - x[0]) / (x[ni - 1] - x[0]) - 1;
+                const double s2 = sx * sx, s4 = s2 * s2, s8 = s4 * s4, s16 = s8 * s8;
+                const double pp = 1 - s16 * s2;
+                F[op.var][p] = op.val * (pp * pp);
+                break;
+            }
+            default: break;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// tangent: base q (updated as k_bc does) and tangent dq (P, dP scratch)
+__global__ void k_bc_tl(BcProgram pg, StateSet q, double *Pbase, StateSet dq, double *dPbase, long long pstride)
+{
+    const int b = blockIdx.x;
+    double *F[5], *dF[5];
+#pragma unroll
+    for (int f = 0; f < 5; f++) { F[f] = q.v[f] + b * q.bstride; dF[f] = dq.v[f] + b * dq.bstride; }
+    double *P = Pbase + b * pstride, *dP = dPbase + b * pstride;
+    double *Rr = F[3], *Ee = F[4], *dR = dF[3], *dE = dF[4];
+    for (int o = 0; o < pg.nops; o++) {
+        const BcOp op = pg.ops[o];
+        if (op.code == OP_NEU || op.code == OP_P_NEU) {
+            const double *cf = op.coef ? pg.coef2 : pg.coef1;
+            neumann_face(pg, op.code == OP_NEU ? F[op.var] : P, op.box, op.dir, op.len, cf);
+            neumann_face(pg, op.code == OP_NEU ? dF[op.var] : dP, op.box, op.dir, op.len, cf);
+            __syncthreads();
+            continue;
+        }
+        const int ni = op.box[1] - op.box[0] + 1, nj = op.box[3] - op.box[2] + 1, nk = op.box[5] - op.box[4] + 1;
+        const long long total = (long long)ni * nj * nk;
+        for (long long q2 = threadIdx.x; q2 < total; q2 += blockDim.x) {
+            const int i = op.box[0] + (int)(q2 % ni);
+            const int j = op.box[2] + (int)((q2 / ni) % nj);
+            const int k = op.box[4] + (int)(q2 / ((long long)ni * nj));
+            const long long p = bidx(pg, i, j, k);
+            switch (op.code) {
+            case OP_SET: F[op.var][p] = op.val; dF[op.var][p] = 0.0; break;
+            case OP_DIR_P: {
+                const double e = Ee[p], rn = op.val / (pg.gamma - 1.0) / e;
+                dR[p] = -rn / e * dE[p];
+                Rr[p] = rn;
+                break;
+            }
+            case OP_P_LOAD: dP[p] = dR[p] * Ee[p] + Rr[p] * dE[p]; P[p] = Rr[p] * Ee[p]; break;
+            case OP_R_FROM_P: {
+                const double e = Ee[p], pv = P[p];
+                dR[p] = dP[p] / e - pv * dE[p] / (e * e);
+                Rr[p] = pv / e;
+                break;
+            }
+            case OP_CORNER_E0: Ee[p] = 0.0; dE[p] = 0.0; break;
+            case OP_P_FROM_E: P[p] = Ee[p]; dP[p] = dE[p]; break;
+            case OP_E_ADD_P: Ee[p] = Ee[p] + P[p]; dE[p] = dE[p] + dP[p]; break;
+            case OP_E_DIV: Ee[p] = Ee[p] / (double)op.aux; dE[p] = dE[p] / (double)op.aux; break;
+            case OP_R0: Rr[p] = 0.0; dR[p] = 0.0; break;
+            case OP_R_ADD_P: Rr[p] = Rr[p] + P[p]; dR[p] = dR[p] + dP[p]; break;
+            case OP_R_DIV_E: {
+                const double r = Rr[p], e = Ee[p], aux = (double)op.aux;
+                dR[p] = dR[p] / e / aux - r * dE[p] / (e * e) / aux;
+                Rr[p] = r / e / aux;
+                break;
+            }
+            case OP_LID: {
+                const double *x = pg.xs + op.xoff;
+                const double sx = 2 * (x[i - op.box[0]] - x[0]) / (x[ni - 1] - x[0]) - 1;
+                const double s2 = sx * sx, s4 = s2 * s2, s8 = s4 * s4, s16 = s8 * s8;
+                const double pp = 1 - s16 * s2;
+                F[op.var][p] = op.val * (pp * pp);
+                dF[op.var][p] = 0.0;
+                break;
+            }
+            default: break;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// adjoint of a Neumann face: g = lam[face]; lam[face] = 0; lam[face + m s] += c_{m-1} g
+__device__ void neumann_face_adj(const BcProgram &pg, double *lam, const int *b, int dir, int len, const double *c)
+{
+    int n1, n2;
+    neumann_extent(b, dir, n1, n2);
+    const long long total = (long long)n1 * n2;
+    for (long long q = threadIdx.x; q < total; q += blockDim.x) {
+        int i, j, k, di, dj, dk;
+        neumann_geom(b, dir, len, q, n1, i, j, k, di, dj, dk);
+        const long long pf = bidx(pg, i, j, k);
+        const double g = lam[pf];
+        lam[pf] = 0.0;
+        for (int m = 1; m <= len; m++) lam[bidx(pg, i + m * di, j + m * dj, k + m * dk)] += c[m - 1] * g;
+    }
+}
+
+// adjoint: lam (the five variables) and lP (the scratch's lambda, zero on entry), ops in reverse
+__global__ void k_bc_adj(BcProgram pg, StateSet lam, double *lPbase, long long pstride, const double *tape,
+                         long long tstride)
+{
+    const int b = blockIdx.x;
+    double *L[5];
+#pragma unroll
+    for (int f = 0; f < 5; f++) L[f] = lam.v[f] + b * lam.bstride;
+    double *lP = lPbase + b * pstride;
+    double *lR = L[3], *lE = L[4];
+    const double *tp = tape + b * tstride;
+    for (int o = pg.nops - 1; o >= 0; o--) {
+        const BcOp op = pg.ops[o];
+        if (op.code == OP_NEU || op.code == OP_P_NEU) {
+            neumann_face_adj(pg, op.code == OP_NEU ? L[op.var] : lP, op.box, op.dir, op.len,
+                             op.coef ? pg.coef2 : pg.coef1);
+            __syncthreads();
+            continue;
+        }
+        const int ni = op.box[1] - op.box[0] + 1, nj = op.box[3] - op.box[2] + 1, nk = op.box[5] - op.box[4] + 1;
+        const long long total = (long long)ni * nj * nk;
+        const int tw = bc_tape_width(op.code);
+        for (long long q2 = threadIdx.x; q2 < total; q2 += blockDim.x) {
+            const int i = op.box[0] + (int)(q2 % ni);
+            const int j = op.box[2] + (int)((q2 / ni) % nj);
+            const int k = op.box[4] + (int)(q2 / ((long long)ni * nj));
+            const long long p = bidx(pg, i, j, k);
+            const double *t = tp + op.tape + tw * q2;
+            switch (op.code) {
+            case OP_SET: L[op.var][p] = 0.0; break;
+            case OP_DIR_P: {
+                const double e = t[0], rn = op.val / (pg.gamma - 1.0) / e;
+                lE[p] += -rn / e * lR[p];
+                lR[p] = 0.0;
+                break;
+            }
+            case OP_P_LOAD: lR[p] += t[1] * lP[p]; lE[p] += t[0] * lP[p]; lP[p] = 0.0; break;
+            case OP_R_FROM_P: {
+                const double pv = t[0], e = t[1];
+                lP[p] += lR[p] / e;
+                lE[p] += -pv / (e * e) * lR[p];
+                lR[p] = 0.0;
+                break;
+            }
+            case OP_CORNER_E0: lE[p] = 0.0; break;
+            case OP_P_FROM_E: lE[p] += lP[p]; lP[p] = 0.0; break;
+            case OP_E_ADD_P: lP[p] += lE[p]; break;
+            case OP_E_DIV: lE[p] = lE[p] / (double)op.aux; break;
+            case OP_R0: lR[p] = 0.0; break;
+            case OP_R_ADD_P: lP[p] += lR[p]; break;
+            case OP_R_DIV_E: {
+                const double r = t[0], e = t[1], aux = (double)op.aux;
+                lE[p] += -r / (e * e) / aux * lR[p];
+                lR[p] = lR[p] / e / aux;
+                break;
+            }
+            case OP_LID: L[op.var][p] = 0.0; break;
+            default: break;
+            }
+        }
         __syncthreads();
     }
 }

@@ -140,6 +140,9 @@ struct gatt_ctx {
     double *a_s1 = nullptr, *a_s2 = nullptr, *a_scr = nullptr;                       // 15, 12, 5
     double *a_ckpt = nullptr, *a_seg = nullptr;
     int a_nckpt = 0, a_nseg = 0;
+    long long tape_len = 0;              // doubles of the boundary-program tape per member
+    double *t_P = nullptr, *a_lP = nullptr, *a_tape = nullptr, *a_tmp = nullptr;
+    long long a_tape_cap = 0;
     bool mean_init = false;                  // SFD mean uploaded or copied from the state
     int cur = 0;
     unsigned long long *acc = nullptr;
@@ -697,6 +700,15 @@ int build_bc_program(gatt_ctx *c)
         TRY(check_box(c, d.ind));
         BcOp o = mk(OP_LID, d.var, d.ind); o.xoff = d.xoff; o.val = d.par; ops.push_back(o);
     }
+    // adjoint tape offsets (base values of the nonlinear ops, per box point)
+    long long tape = 0;
+    for (BcOp &o : ops) {
+        const int tw = bc_tape_width(o.code);
+        o.tape = tape;
+        if (o.code != OP_NEU && o.code != OP_P_NEU && tw > 0)
+            tape += (long long)tw * (o.box[1] - o.box[0] + 1) * (o.box[3] - o.box[2] + 1) * (o.box[5] - o.box[4] + 1);
+    }
+    c->tape_len = tape;
     cudaFree(c->d_ops); c->d_ops = nullptr;
     cudaFree(c->d_coef1); c->d_coef1 = nullptr;
     cudaFree(c->d_coef2); c->d_coef2 = nullptr;
@@ -1103,16 +1115,14 @@ int state_to_set(gatt_ctx *c, const StateSet &q, double *dst, bool to_set)
     return GATT_OK;
 }
 
-// The tangent and the adjoint are built for 3-D cases whose step is RK4 + filter: no
-// boundary-condition program, no disturbances, no SFD.
+// The tangent and the adjoint are built for 3-D cases whose step is RK4 + filter +
+// boundary conditions (no SFD).
 int check_diff(gatt_ctx *c, bool adjoint)
 {
     TRY(check_ready(c, true));
     if (!c->is3d) return fail(GATT_ERR_STATE, "tangent and adjoint are built for 3-D cases");
     if (c->sfd_type > 0) return fail(GATT_ERR_STATE, "tangent and adjoint are built for cases without SFD");
     if (c->bc_dirty) TRY(build_bc_program(c));
-    if (c->nops > 0)
-        return fail(GATT_ERR_STATE, "tangent and adjoint are built for cases without boundary conditions");
     if (adjoint)
         for (int d = 0; d < 3; d++) {
             if (!c->mat[d][2].set || !c->mat[d][3].set)
@@ -1127,6 +1137,7 @@ int diff_alloc(gatt_ctx *c, bool adjoint)
 {
     for (double *&p : c->dx) if (!p) TRY(alloc_fields(c, &p, 5, c->nb));
     if (!adjoint) {
+        if (!c->t_P) TRY(alloc_fields(c, &c->t_P, 1, c->nb));
         for (double *&p : c->dy) if (!p) TRY(alloc_fields(c, &p, 5, c->nb));
         if (!c->t_delta) TRY(alloc_fields(c, &c->t_delta, 5, c->nb));
         if (!c->t_d1) TRY(alloc_fields(c, &c->t_d1, D3_N, c->nb));
@@ -1141,7 +1152,56 @@ int diff_alloc(gatt_ctx *c, bool adjoint)
     if (!c->a_lvt) TRY(alloc_fields(c, &c->a_lvt, 4, c->nb));
     if (!c->a_s1) TRY(alloc_fields(c, &c->a_s1, 15, c->nb));
     if (!c->a_s2) TRY(alloc_fields(c, &c->a_s2, 12, c->nb));
+    if (!c->a_lP) TRY(alloc_fields(c, &c->a_lP, 1, c->nb));
+    if (!c->a_tmp) TRY(alloc_fields(c, &c->a_tmp, 5, c->nb));
+    // five boundary-program tapes per step (after each stage and after the filter)
+    const long long need = 5 * std::max(1LL, c->tape_len) * c->nb;
+    if (c->a_tape_cap < need) {
+        cudaFree(c->a_tape);
+        c->a_tape = nullptr;
+        c->a_tape_cap = 0;
+        CU(cudaMalloc(&c->a_tape, sizeof(double) * (size_t)need));
+        c->a_tape_cap = need;
+    }
     return GATT_OK;
+}
+
+BcProgram bc_program(const gatt_ctx *c)
+{
+    BcProgram pg;
+    pg.ops = c->d_ops; pg.nops = c->nops; pg.coef1 = c->d_coef1; pg.coef2 = c->d_coef2; pg.xs = c->d_xs;
+    pg.gamma = c->ph.gamma; pg.nx = c->nx; pg.ny = c->ny; pg.nz = c->nz;
+    return pg;
+}
+
+// boundary program on base x and tangent y together
+int bc_tl(gatt_ctx *c, const StateSet &x, const StateSet &y)
+{
+    if (c->nops == 0) return GATT_OK;
+    TRY(before_launch(c, PC_BC));
+    k_bc_tl<<<c->nb, 512, 0, c->stream>>>(bc_program(c), x, c->P, y, c->t_P, c->npts);
+    return after_launch(c);
+}
+
+// boundary program on base x, recording tape number `which` (0..4)
+int bc_rec(gatt_ctx *c, const StateSet &x, int which)
+{
+    if (c->nops == 0) return GATT_OK;
+    const long long ts = std::max(1LL, c->tape_len);
+    TRY(before_launch(c, PC_BC));
+    k_bc_rec<<<c->nb, 512, 0, c->stream>>>(bc_program(c), x, c->P, c->npts, c->a_tape + which * ts * c->nb, ts);
+    return after_launch(c);
+}
+
+// transposed boundary program on lambda, from tape `which`
+int bc_adj(gatt_ctx *c, const StateSet &lam, int which)
+{
+    if (c->nops == 0) return GATT_OK;
+    const long long ts = std::max(1LL, c->tape_len);
+    CU(cudaMemsetAsync(c->a_lP, 0, sizeof(double) * (size_t)c->npts * c->nb, c->stream));
+    TRY(before_launch(c, PC_BC));
+    k_bc_adj<<<c->nb, 512, 0, c->stream>>>(bc_program(c), lam, c->a_lP, c->npts, c->a_tape + which * ts * c->nb, ts);
+    return after_launch(c);
 }
 
 int set_params(gatt_ctx *c, int slot, double t, double dt)
@@ -1190,14 +1250,20 @@ int tl_step(gatt_ctx *c)
 {
     const StateSet X0 = set5(c, c->dx[0]), XA = set5(c, c->dx[1]), XB = set5(c, c->dx[2]);
     const StateSet Y0 = set5(c, c->dy[0]), YA = set5(c, c->dy[1]), YB = set5(c, c->dy[2]);
+    // boundary conditions after every stage (timeIntegration.F90:406-491) and after the filter
     TRY(tl_stage(c, X0, X0, XA, Y0, Y0, YA, RK_STAGE1));
+    TRY(bc_tl(c, XA, YA));
     TRY(tl_stage(c, XA, X0, XB, YA, Y0, YB, RK_STAGE2));
+    TRY(bc_tl(c, XB, YB));
     TRY(tl_stage(c, XB, X0, XA, YB, Y0, YA, RK_STAGE3));
+    TRY(bc_tl(c, XA, YA));
     TRY(tl_stage(c, XA, X0, XB, YA, Y0, YB, RK_STAGE4));
+    TRY(bc_tl(c, XB, YB));
     // the filter is linear: the same sweeps act on the tangent (main.F90:357-378)
     const double *bdt = c->fct > 0 ? &c->d_params->dt : nullptr;
     TRY(filter_set(c, XB, c->nb, 0.0, bdt));
     TRY(filter_set(c, YB, c->nb, 0.0, bdt));
+    TRY(bc_tl(c, XB, YB));
     TRY(copy_set5(c, c->dx[0], c->dx[2]));
     return copy_set5(c, c->dy[0], c->dy[2]);
 }
@@ -1261,8 +1327,18 @@ int adj_step(gatt_ctx *c, double dt)
 {
     const StateSet X[5] = {set5(c, c->dx[0]), set5(c, c->dx[1]), set5(c, c->dx[2]), set5(c, c->dx[3]),
                            set5(c, c->dx[4])};
-    // recompute the stage inputs q1, q2, q3 (q4, the pre-filter state, is not needed)
-    for (int s = 1; s <= 3; s++) TRY(rhs_stage(c, X[s - 1], X[0], X[s], s, c->nb, c->d1, c->tq, c->d2, c->delta));
+    // recompute the stage states q1..q4 (after their boundary conditions) and the filtered
+    // state, recording the boundary program's tapes: 0..3 after the stages, 4 after the filter
+    for (int s = 1; s <= 4; s++) {
+        TRY(rhs_stage(c, X[s - 1], X[0], X[s], s, c->nb, c->d1, c->tq, c->d2, c->delta));
+        TRY(bc_rec(c, X[s], s - 1));
+    }
+    if (c->nops > 0) {
+        TRY(copy_set5(c, c->a_tmp, c->dx[4]));
+        TRY(filter_set(c, set5(c, c->a_tmp), c->nb, 0.0, c->fct > 0 ? &c->d_params->dt : nullptr));
+        TRY(bc_rec(c, set5(c, c->a_tmp), 4));
+    }
+    TRY(bc_adj(c, set5(c, c->a_lam), 4));
     // filter^T, z -> y -> x; with the time blend lam = lam + b (F^T lam - lam)
     const int f5[5] = {0, 1, 2, 3, 4};
     for (int d = 2; d >= 0; d--) {
@@ -1280,6 +1356,7 @@ int adj_step(gatt_ctx *c, double dt)
     // RK4: q4 = q0 + dt/6 k1 + dt/3 k2 + dt/3 k3 + dt/6 k4, q1 = q0 + dt/2 k1,
     // q2 = q0 + dt/2 k2, q3 = q0 + dt k3, k_s = F(q_{s-1})
     const StateSet A = set5(c, c->a_arg), G = set5(c, c->a_g);
+    TRY(bc_adj(c, set5(c, c->a_lam), 3));  // the boundary conditions after stage 4
     TRY(copy_set5(c, c->a_acc, c->a_lam));
     const double wl[4] = {dt / 6.0, dt / 3.0, dt / 3.0, dt / 6.0};  // weight of lambda4 in a_s (s = 4..1)
     const double wp[4] = {0.0, dt, dt / 2.0, dt / 2.0};             // weight of lambda_{q_s}
@@ -1287,6 +1364,7 @@ int adj_step(gatt_ctx *c, double dt)
         const int s = 3 - i;  // stage state q_s feeds k_{s+1}
         TRY(axpby5(c, c->a_arg, c->a_lam, i ? c->a_prev : nullptr, wl[i], wp[i]));
         TRY(adj_rhs(c, X[s], A, G));
+        if (s > 0) TRY(bc_adj(c, G, s - 1));  // q_s came out of the boundary conditions of stage s
         TRY(axpby5(c, c->a_acc, c->a_acc, c->a_g, 1.0, 1.0));
         if (s > 0) TRY(copy_set5(c, c->a_prev, c->a_g));
     }
@@ -1490,7 +1568,8 @@ void gatt_destroy(gatt_ctx *c)
     for (double *p : c->dx) cudaFree(p);
     for (double *p : c->dy) cudaFree(p);
     double *dbufs[] = {c->t_delta, c->t_d1, c->t_tq, c->t_d2, c->a_lam, c->a_acc, c->a_arg, c->a_prev, c->a_g,
-                       c->a_lq, c->a_ld1, c->a_ltau, c->a_lvt, c->a_s1, c->a_s2, c->a_scr, c->a_ckpt, c->a_seg};
+                       c->a_lq, c->a_ld1, c->a_ltau, c->a_lvt, c->a_s1, c->a_s2, c->a_scr, c->a_ckpt, c->a_seg,
+                       c->t_P, c->a_lP, c->a_tape, c->a_tmp};
     for (double *p : dbufs) cudaFree(p);
     for (double *p : bufs) cudaFree(p);
     cudaFree(c->d_ops); cudaFree(c->acc); cudaFree(c->d_params);

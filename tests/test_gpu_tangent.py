@@ -1,6 +1,7 @@
 """GPU tests of the tangent-linear and adjoint (gatt_rhs_jvp / gatt_rhs_vjp / gatt_jvp / gatt_vjp).
 
-Checks, on the 3-D periodic box:
+Checks, on the 3-D periodic box and on a 3-D cavity channel with walls, corners and open-top
+lists (the boundary program's tangent and its taped adjoint):
 * transposed line operators: <L x, y> = <x, L^T y> per direction, derivative and filter;
 * tangent of the RHS and of the step against central finite differences of the nonlinear
   GPU path (the Jacobian-free linearisation of calcInstability.m:353-390) and of the CPU
@@ -42,16 +43,31 @@ def rand_flow(case, seed, scale=1.0):
     return {k: scale * rng.standard_normal(s) for k in KEYS}
 
 
-@pytest.fixture(scope="module")
-def box():
-    c = cs.periodic_box(n=16)
-    q = cs.solenoidal_turbulence(c, seed=1234)
-    # a thermodynamic perturbation so that every variable's derivative path is exercised
-    rng = np.random.default_rng(3)
-    q = {k: np.array(v, copy=True) for k, v in q.items()}
-    q["R"] = q["R"] * (1.0 + 0.01 * rng.standard_normal(q["R"].shape))
-    q["E"] = q["E"] * (1.0 + 0.01 * rng.standard_normal(q["E"].shape))
-    return c, q
+_CASES = {}
+
+
+def _case(name):
+    if name not in _CASES:
+        if name == "box":
+            c = cs.periodic_box(n=16)
+            q = cs.solenoidal_turbulence(c, seed=1234)
+        else:
+            # walls with isothermal Dirichlet and pressure Neumann lists, adiabatic corners,
+            # an open top with null second derivatives: every op of the boundary program
+            c = cs.cavity_channel(nx=24, ny=20, nz=8, adiabatic_corners=True)
+            q = cs.random_flow(c, seed=5, amp=0.05)
+        # a thermodynamic perturbation so that every variable's derivative path is exercised
+        rng = np.random.default_rng(3)
+        q = {k: np.array(v, copy=True) for k, v in q.items()}
+        q["R"] = q["R"] * (1.0 + 0.01 * rng.standard_normal(q["R"].shape))
+        q["E"] = q["E"] * (1.0 + 0.01 * rng.standard_normal(q["E"].shape))
+        _CASES[name] = (c, q)
+    return _CASES[name]
+
+
+@pytest.fixture(scope="module", params=["box", "cavity3d"])
+def box(request):
+    return _case(request.param)
 
 
 def test_transposed_line_operators(cuda_lib, box):
@@ -184,8 +200,13 @@ def test_energy_gradient(cuda_lib, box):
 def test_unsupported_cases_are_refused(cuda_lib):
     from gatt_dns_b200.solver import GattDNS
     from gatt_dns_b200._lib import GattError
-    c = cs.lid_driven(n=24)  # 2-D with walls
+    c = cs.lid_driven(n=24)  # 2-D
     with GattDNS(c) as g:
         f = cs.uniform_flow(c)
         with pytest.raises(GattError):
             g.rhs_jvp(f, f)
+    c = cs.cavity_channel(nx=24, ny=20, nz=8, sfd={"X": 0.05, "Delta": 10.0, "buffer": 6})  # SFD on
+    with GattDNS(c) as g:
+        f = cs.uniform_flow(c)
+        with pytest.raises(GattError):
+            g.jvp(f, 1, 0.0, 1e-3)
