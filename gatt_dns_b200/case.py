@@ -551,6 +551,95 @@ def cavity_channel(nx=96, ny=64, nz=1, Re=1000.0, Ma=0.5, Pr=0.71, gamma=1.4, T0
     return case
 
 
+def boundary_layer(nx=400, ny=150, nz=64, Lx=6.0, Ly=5.0, Lz=1.0, Re=1000.0, Ma=0.5, Pr=0.71, gamma=1.4,
+                   T0=300.0, filter_alpha=0.49, deriv="SL4", ny_stretch=1.5):
+    """3-D compressible boundary layer over an isothermal flat plate, spanwise periodic.
+
+    The boundary set of source/boundaries/boundaryLayerIsothermal.m for a domain starting
+    at the plate's leading edge (mesh.X(1) = 0): inflow u = 1, v = w = 0, e = E0 with
+    pressure Neumann (:4-66); outflow null second derivatives of u, v, w, e and p = P0
+    (:83-145); outer flow null second derivatives of u, v, w, e, p (:146-207); the plate
+    (j = 1) from findWallsForBoundaries with the wall list of lidDrivenFlow.m (no-slip,
+    e = E0, pressure Neumann).  y is tanh-clustered at the plate; z is periodic.
+    """
+    X = generate_mesh(0.0, Lx, nx)
+    Y = generate_mesh(0.0, Ly, ny, mtype="tanh", par=ny_stretch, local="i")
+    Z = generate_mesh(0.0, Lz, nz, periodic=True, fix_periodic_domain_size=True)
+    fr = np.ones((nx, ny, nz), dtype=bool)
+    fr[:, 0, :] = False
+    fr, walls, corners, inside = find_walls_for_boundaries(fr)
+    E0 = 1.0 / ((gamma ** 2 - gamma) * Ma ** 2)
+    P0 = (gamma - 1) * E0
+    items = wall_boundary_list(walls, inside, P0, E0)
+    inflow = [1, 1, 2, ny, 1, nz]
+    for v, val in (("u", 1.0), ("v", 0.0), ("w", 0.0), ("e", E0)):
+        items.append((v, "dir", "xi", val, list(inflow)))
+    items.append(("p", "neu", "xi", 0.0, list(inflow)))
+    outflow = [nx, nx, 2, ny, 1, nz]
+    for v in ("u", "v", "w", "e"):
+        items.append((v, "sec", "xf", 0.0, list(outflow)))
+    items.append(("p", "dir", "xf", P0, list(outflow)))
+    top = [1, nx, ny, ny, 1, nz]
+    for v in ("u", "v", "w", "e", "p"):
+        items.append((v, "sec", "yf", 0.0, list(top)))
+    n1, n2 = mx.neumann_coefficients(6, 2)
+    bc = init_boundaries(items, corners, mx.fortran_round(n1), mx.fortran_round(n2))
+    mats = build_matrices(X, Y, Z, fr, (False, False, True), (False, False, True), (Lx, Ly, Lz),
+                          deriv=deriv, filter_alpha=filter_alpha, filter_borders="decentered")
+    return Case(name="boundary_layer_%dx%dx%d" % (nx, ny, nz), nx=nx, ny=ny, nz=nz, Re=Re, Ma=Ma, Pr=Pr,
+                gamma=gamma, T0=T0, X=X, Y=Y, Z=Z, mats=mats, bc=bc, flowRegion=fr, dxmin=_dxmin(X, Y, Z))
+
+
+def blasius_profile(eta_max=12.0, n=6001):
+    """Blasius similarity solution f(eta), f'(eta): f''' + f f''/2 = 0, f(0) = f'(0) = 0,
+    f'(inf) = 1, by RK4 shooting on f''(0).  It stands in for the compressible profile of
+    calcCompressibleBL.m."""
+    eta = np.linspace(0.0, eta_max, n)
+    h = eta[1] - eta[0]
+
+    def rhs(y):
+        return np.array([y[1], y[2], -0.5 * y[0] * y[2]])
+
+    def integrate(s):
+        y = np.array([0.0, 0.0, s])
+        out = np.zeros((n, 3))
+        out[0] = y
+        for i in range(1, n):
+            k1 = rhs(y)
+            k2 = rhs(y + 0.5 * h * k1)
+            k3 = rhs(y + 0.5 * h * k2)
+            k4 = rhs(y + h * k3)
+            y = y + h / 6.0 * (k1 + 2 * k2 + 2 * k3 + k4)
+            out[i] = y
+        return out
+
+    lo, hi = 0.2, 0.5
+    for _ in range(50):
+        mid = 0.5 * (lo + hi)
+        if integrate(mid)[-1, 1] > 1.0:
+            hi = mid
+        else:
+            lo = mid
+    sol = integrate(0.5 * (lo + hi))
+    return eta, sol[:, 0], sol[:, 1]
+
+
+def blasius_flow(case: Case, x0=1.0):
+    """Blasius base flow: u = f'(eta), v = (eta f' - f) / (2 sqrt(Re x)) with eta = y sqrt(Re / x)
+    and x measured from a virtual origin x0 upstream of the inflow; R = 1, E = E0."""
+    eta_t, f_t, fp_t = blasius_profile()
+    s = (case.nx, case.ny, case.nz)
+    x = case.X[:, None] + x0
+    eta = case.Y[None, :] * np.sqrt(case.Re / x)
+    f = np.where(eta <= eta_t[-1], np.interp(eta, eta_t, f_t), f_t[-1] + (eta - eta_t[-1]))
+    fp = np.interp(eta, eta_t, fp_t, right=1.0)
+    v = (eta * fp - f) / (2.0 * np.sqrt(case.Re * x))
+    out = uniform_flow(case)
+    out["U"] = np.asfortranarray(np.repeat(fp[:, :, None], s[2], axis=2))
+    out["V"] = np.asfortranarray(np.repeat(v[:, :, None], s[2], axis=2))
+    return out
+
+
 # ---------------------------------------------------------------------------
 # initial flows (synthetic, seeded)
 # ---------------------------------------------------------------------------

@@ -51,6 +51,10 @@ def _case(name):
         if name == "box":
             c = cs.periodic_box(n=16)
             q = cs.solenoidal_turbulence(c, seed=1234)
+        elif name == "bl":
+            # boundary layer: inflow Dirichlet, outflow pressure Dirichlet, open top, plate
+            c = cs.boundary_layer(nx=48, ny=32, nz=16)
+            q = cs.blasius_flow(c)
         else:
             # walls with isothermal Dirichlet and pressure Neumann lists, adiabatic corners,
             # an open top with null second derivatives: every op of the boundary program
@@ -65,7 +69,7 @@ def _case(name):
     return _CASES[name]
 
 
-@pytest.fixture(scope="module", params=["box", "cavity3d"])
+@pytest.fixture(scope="module", params=["box", "cavity3d", "bl"])
 def box(request):
     return _case(request.param)
 
