@@ -52,6 +52,7 @@ def parse():
     p.add_argument("--n", type=int, default=N_GRID)
     p.add_argument("--no-clocks", action="store_true")
     p.add_argument("--no-arnoldi", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true")
     return p.parse_args()
 
 
@@ -230,6 +231,64 @@ def arnoldi_sample(cs, GattDNS, case, base, members, m, nsteps, seed, label):
                       "estimated from the time per member-step (10 synchronised steps)" % (m, nsteps)}
 
 
+def adjoint_sample(cs, GattDNS, nsteps=20, every=5, shape=(400, 150, 64)):
+    """Config 5 on its full grid, bounded sample: gradient of the perturbation kinetic energy
+    J = 1/2 sum |u - u_base|^2 after nsteps steps with respect to the initial perturbation
+    (seed 99, amplitude 1e-6), by the checkpointed adjoint; checked by a central difference
+    along a random direction and by a dot-product test against the tangent."""
+    import torch
+    c = cs.boundary_layer(nx=shape[0], ny=shape[1], nz=shape[2])
+    base = cs.blasius_flow(c)
+    s = (c.nx, c.ny, c.nz)
+    rng = np.random.default_rng(99)
+    pert = {k: 1e-6 * rng.standard_normal(s) for k in "UVWRE"}
+    q0 = {k: base[k] + pert[k] for k in "UVWRE"}
+    dt = c.cfl_dt(base["U"], base["V"], base["W"], 0.5)
+    g = GattDNS(c)
+
+    def run(q):
+        g.upload(q)
+        g.run(nsteps, 0.0, dt)
+        return g.download()
+
+    t0 = time.perf_counter()
+    ub = run(base)
+    t_fwd = time.perf_counter() - t0
+    uN = run(q0)
+
+    def J(u):
+        return 0.5 * float(sum(np.sum((u[k] - ub[k]) ** 2) for k in "UVW"))
+
+    lam = {k: (uN[k] - ub[k]) if k in "UVW" else np.zeros(s) for k in "UVWRE"}
+    g.upload(q0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    grad = g.vjp(lam, nsteps, 0.0, dt, checkpoint_every=every)
+    t_adj = time.perf_counter() - t0
+    v = {k: 1e-6 * rng.standard_normal(s) for k in "UVWRE"}
+    h = 0.1
+    jp = J(run({k: q0[k] + h * v[k] for k in "UVWRE"}))
+    jm = J(run({k: q0[k] - h * v[k] for k in "UVWRE"}))
+    fd = (jp - jm) / (2 * h)
+    ad = float(sum(np.sum(grad[k] * v[k]) for k in "UVWRE"))
+    g.upload(q0)
+    t0 = time.perf_counter()
+    jv = g.jvp(v, nsteps, 0.0, dt)
+    t_tl = time.perf_counter() - t0
+    w = {k: rng.standard_normal(s) for k in "UVWRE"}
+    g.upload(q0)
+    jtw = g.vjp(w, nsteps, 0.0, dt, checkpoint_every=every)
+    a = float(sum(np.sum(jv[k] * w[k]) for k in "UVWRE"))
+    b = float(sum(np.sum(v[k] * jtw[k]) for k in "UVWRE"))
+    g.close()
+    return {"workload": "boundary layer %dx%dx%d, Blasius base, Re 1000, Ma 0.5" % shape, "steps": nsteps,
+            "checkpoint_every": every, "forward_s": t_fwd, "tangent_s": t_tl, "adjoint_s": t_adj,
+            "adjoint_over_forward": t_adj / t_fwd, "gradient_vs_central_difference_rel": abs(ad - fd) / abs(fd),
+            "dot_product_test_rel": abs(a - b) / abs(a),
+            "sample": "%d of the config's 200 steps (checkpoint every %d); times are wall clock of the "
+                      "synchronous C-ABI calls, host transfers included" % (nsteps, every)}
+
+
 def time_steps(g, dt, k):
     """ms per step of k back-to-back gatt_run steps (gatt_run returns after synchronising the
     context's own stream, so the wall time brackets the device work)."""
@@ -374,6 +433,9 @@ def main():
                                "32 problems on the %d^3 periodic box base flow" % args.n),
                 arnoldi_sample(cs, GattDNS, lid, cs.uniform_flow(lid), 32, 2, 100, 4321,
                                "32 problems on the 128^2 lid-driven cavity (rest state base)")]
+        if not args.no_adjoint:
+            g.close()
+            line["adjoint"] = adjoint_sample(cs, GattDNS)
     if rank == 0:
         print(json.dumps(line), flush=True)
     g.close()
