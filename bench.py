@@ -289,6 +289,37 @@ def adjoint_sample(cs, GattDNS, nsteps=20, every=5, shape=(400, 150, 64)):
                       "synchronous C-ABI calls, host transfers included" % (nsteps, every)}
 
 
+def lid_sample(cs, GattDNS, nsteps=1000, cpu_steps=200):
+    """Config 1: the 128^2 lid-driven cavity from rest, nsteps RK4 steps at CFL 0.5 on the GPU
+    (wall clock of one gatt_run), and the CPU oracle on a bounded sample of the same steps."""
+    import oracle
+    c = cs.lid_driven(n=128)
+    f = cs.uniform_flow(c)
+    dt = c.cfl_dt(f["U"], f["V"], f["W"], 0.5)
+    g = GattDNS(c)
+    g.upload(f)
+    g.apply_bound_cond(0.0)
+    g.run(5, 0.0, dt)
+    g.upload(f)
+    g.apply_bound_cond(0.0)
+    t0 = time.perf_counter()
+    g.run(nsteps, 0.0, dt)
+    el = time.perf_counter() - t0
+    g.close()
+    o = oracle.Oracle(c)
+    st = o.new_state(o.apply_bound_cond(f, 0.0))
+    t0 = time.perf_counter()
+    for k in range(cpu_steps):
+        o.step(st, k * dt, dt)
+    cel = (time.perf_counter() - t0) / cpu_steps * nsteps
+    npts = c.nx * c.ny
+    return {"workload": "lid-driven cavity 128^2 from rest, CFL 0.5, %d RK4 steps" % nsteps, "gpu_s": el,
+            "gpu_mpoint_stages_s": npts * STAGES * nsteps / el / 1e6, "cpu_s_est": cel,
+            "cpu_cores": o.lib.orc_num_threads(), "gpu_over_cpu": cel / el,
+            "sample": "GPU: all %d steps in one gatt_run (launch-bound at this size); CPU oracle: %d steps "
+                      "timed, scaled to %d" % (nsteps, cpu_steps, nsteps)}
+
+
 def time_steps(g, dt, k):
     """ms per step of k back-to-back gatt_run steps (gatt_run returns after synchronising the
     context's own stream, so the wall time brackets the device work)."""
@@ -436,6 +467,7 @@ def main():
         if not args.no_adjoint:
             g.close()
             line["adjoint"] = adjoint_sample(cs, GattDNS)
+        line["lid_driven"] = lid_sample(cs, GattDNS)
     if rank == 0:
         print(json.dumps(line), flush=True)
     g.close()
