@@ -2050,6 +2050,29 @@ int gatt_vjp(gatt_ctx *c, int nsteps, double t0, double dt, int checkpoint_every
     return vjp(c, nsteps, t0, dt, checkpoint_every, lamN, lam0);
 }
 
+int gatt_selftest_pipeline_timeout(gatt_ctx *c)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    TRY(check_ready(c, false));
+    TRY(sync_stream(c));
+    // one x-direction first-derivative sweep of member 0's U through the copy ring, every
+    // barrier expecting 16 bytes that never come
+    const DevDir &m = c->mat[0][0];
+    if (!m.set || m.family != FAM_PIPE) return fail(GATT_ERR_STATE, "x lines do not use the pipelined solver");
+    SweepArgs a;
+    memset(&a, 0, sizeof(a));
+    const StateSet q = state_set(c, 0);
+    a.in = q.v[0]; a.out = c->tmp; a.npts = c->npts;
+    a.nx = c->nx; a.ny = c->ny; a.nz = c->nz; a.N = m.N; a.nlines = nlines(c, 0);
+    a.es = 1; a.os = 0; a.tiles_per_row = (c->nx + kLanes - 1) / kLanes;
+    a.Rm = m.Rm; a.Q = m.Q; a.W = m.W; a.Wp = m.Wp; a.P = m.P; a.ltype = c->ltype[0];
+    a.epi = EPI_STORE; a.dir = 0; a.nf = 1; a.ntiles = (a.nlines + kLanes - 1) / kLanes; a.njobs = a.ntiles;
+    a.err = c->d_err; a.ntypes = m.nTypes; a.tx_extra = 16;
+    const int r = launch_psweep(c, m, 0, a, 1, PC_OTHER);
+    if (r != GATT_OK) return r;
+    return sync_stream(c);  // GATT_ERR_TIMEOUT when every wait gave up as intended
+}
+
 int gatt_synchronize(gatt_ctx *c)
 {
     if (!c) return fail(GATT_ERR_BADARG, "null context");

@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(32 * kMaxP) k_psweep(const SweepArgs a, const 
                 const int L0 = tile * kLanes;
                 const int nv = min(kLanes, a.nlines - L0);
                 fence_proxy_async();
-                if (lane == 0) mbar_expect_tx(bar, (uint32_t)(nv * N * sizeof(double)));
+                if (lane == 0) mbar_expect_tx(bar, (uint32_t)(nv * N * sizeof(double) + a.tx_extra));
                 __syncwarp();
                 if (lane < nv)
                     bulk_g2s(dst + lane * (N + 2) * (uint32_t)sizeof(double),
@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(32 * kMaxP) k_psweep(const SweepArgs a, const 
             }
         } else if (threadIdx.x == 0) {
             fence_proxy_async();
-            mbar_expect_tx(bar, (uint32_t)(N * kLanes * sizeof(double)));
+            mbar_expect_tx(bar, (uint32_t)(N * kLanes * sizeof(double) + a.tx_extra));
             const int o = tile / a.tiles_per_row, x0 = (tile % a.tiles_per_row) * kLanes;
             tma_load_5d(dst, &tmap, x0, a.dir == 1 ? 0 : o, a.dir == 1 ? o : 0, a.in_slot[f], b, bar);
         }

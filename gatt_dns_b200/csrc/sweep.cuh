@@ -75,6 +75,8 @@ struct SweepArgs {
     int njobs;               // ntiles * nf * members
     int ntypes;              // line types of the coefficient set
     int nst;                 // ring stages (1 .. kMaxStages)
+    int tx_extra;            // bytes added to every copy barrier's expected count: 0, except in
+                             // gatt_selftest_pipeline_timeout (its waits must run out)
     int *err;                // set to 1 when a pipeline wait gives up (host-mapped)
 };
 

@@ -199,6 +199,14 @@ int gatt_jvp(gatt_ctx *ctx, int nsteps, double t0, double dt, const double *dq0,
 int gatt_vjp(gatt_ctx *ctx, int nsteps, double t0, double dt, int checkpoint_every, const double *lamN,
              double *lam0);
 
+/* Self-test of the pipelined line solver's failure path (no counterpart in the reference):
+ * runs one x-direction sweep whose copy barriers expect 16 bytes more than the copies
+ * deliver, so that every bounded wait gives up (after 1 s; the real copies have landed by
+ * then).  Returns the status the next synchronisation reports -- GATT_ERR_TIMEOUT when the
+ * path works -- and leaves the context usable.  GATT_ERR_STATE when x lines do not use the
+ * pipelined solver. */
+int gatt_selftest_pipeline_timeout(gatt_ctx *ctx);
+
 /* max|U|, max|V|, max|W| of every member (main.F90:196-204), for the caller's CFL. */
 int gatt_max_velocity(gatt_ctx *ctx, double *vmax);
 

@@ -239,6 +239,11 @@ module gatt_dns
             real(c_double), dimension(*) :: lamN, lam0
             integer(c_int) :: gatt_vjp
         end function
+        function gatt_selftest_pipeline_timeout(ctx) bind(C, name='gatt_selftest_pipeline_timeout')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: ctx
+            integer(c_int) :: gatt_selftest_pipeline_timeout
+        end function
         function gatt_max_velocity(ctx, vmax) bind(C, name='gatt_max_velocity')
             import :: c_int, c_ptr, c_double
             type(c_ptr), value :: ctx
