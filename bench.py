@@ -355,6 +355,7 @@ def main():
     dt = c.cfl_dt(f["U"], f["V"], f["W"], 0.5)
     stream = torch.cuda.Stream()
     g = GattDNS(c, stream=stream.cuda_stream)
+    tuned = g.autotune(reps=3)  # line-solve family and row blocks per matrix set
     npts = c.npts
 
     # pinned host buffers for the end-to-end leg
@@ -451,6 +452,9 @@ def main():
                          "peak_source": peak_kind,
                          "step_sweep_model_gbs": stage_model, "step_sweep_model_frac": stage_model / peak},
             "kernels_ms_per_launch": {k: round(v[0], 5) for k, v in prof.items() if v[1] > 0},
+            "autotuned": {"%s/%s" % ("xyz"[d - 1], ("deriv", "filter", "derivT_lhs", "derivT_band", "filterT_lhs",
+                                                   "filterT_band")[k]): [fam, P, round(us, 1)]
+                          for (d, k), (fam, P, us) in tuned.items()},
             "max_change_last": [float(x) for x in mc[0]]}
     if clocks:
         line["clocks"] = clocks

@@ -55,6 +55,7 @@ SIGNATURES = {
     "gatt_jvp": (_c_int, [_c_void_p, _c_int, _c_double, _c_double, _pd, _pd]),
     "gatt_vjp": (_c_int, [_c_void_p, _c_int, _c_double, _c_double, _c_int, _pd, _pd]),
     "gatt_selftest_pipeline_timeout": (_c_int, [_c_void_p]),
+    "gatt_autotune": (_c_int, [_c_void_p, _c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), _pd]),
     "gatt_synchronize": (_c_int, [_c_void_p]),
     "gatt_kernel_launches": (ctypes.c_longlong, [_c_void_p]),
     "gatt_profile_kernels": (_c_int, [_c_void_p, _c_double, _c_double, _c_int, _pd, _pd]),

@@ -64,6 +64,9 @@ struct DevDir {
     int periodic = 0, nR = 0, nTypes = 0, N = 0, W = 0, Wp = 0, P = 1;
     int rpb = 0;           // rows per block of the register-resident solver (0: shared-tile solver)
     int family = 0;        // SweepFamily
+    // the factors as given, repacked [type][row] ([type][row][diag] for R): kept to rebuild
+    // the kernel records for another row-block partition (gatt_autotune)
+    std::vector<double> hA, hB, hC, hD, hR;
     double *Rm = nullptr;  // band coefficients [nTypes][N][Wp]
     double *Q = nullptr;   // row records [nTypes][N][kQ] (see sweep.cuh)
 };
@@ -398,6 +401,56 @@ int set_sweep_attributes()
                 CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
                 CU(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
             }
+    return GATT_OK;
+}
+
+// Kernel row records (sweep.cuh) of a matrix set for a partition into P row blocks: the
+// reference's factors in uniform row semantics plus the block propagators of the partitioned
+// recurrences (long double products).  Allocates the device arrays on first use.
+int upload_records(gatt_ctx *c, DevDir &m, int P)
+{
+    const int N = m.N, W = m.W, Wp = m.Wp, nTypes = m.nTypes;
+    const bool periodic = m.periodic != 0;
+    std::vector<double> hRm((size_t)nTypes * N * Wp, 0.0), hQ((size_t)nTypes * N * kQ, 0.0);
+    for (int t = 0; t < nTypes; t++) {
+        const double *tA = &m.hA[(size_t)t * N], *tB = &m.hB[(size_t)t * N], *tC = &m.hC[(size_t)t * N];
+        double *q = &hQ[(size_t)t * N * kQ];
+        for (int r = 0; r < N; r++) {
+            double *qr = q + (size_t)r * kQ;
+            if (!periodic) {
+                qr[kQfA] = r > 0 ? tA[r - 1] : 0.0;       // derivs.F90:607
+                qr[kQfB] = tB[r];
+                qr[kQbC] = r < N - 1 ? tC[r] : 0.0;       // derivs.F90:610
+            } else {
+                qr[kQfA] = r >= 2 ? tA[r - 1] : 0.0;      // derivs.F90:798
+                qr[kQfB] = r >= 1 ? tB[r - 1] : 0.0;      // derivs.F90:796-798
+                qr[kQbC] = (r >= 1 && r <= N - 2) ? tC[r] : 0.0;  // derivs.F90:801
+                qr[kQD] = m.hD[(size_t)t * N + r];        // derivs.F90:786-789
+            }
+            for (int k = 0; k < W; k++) hRm[((size_t)t * N + r) * Wp + k] = m.hR[((size_t)t * N + r) * W + k];
+        }
+        if (periodic) { q[kQcA] = tA[0]; q[kQcC] = tC[0]; }  // derivs.F90:792-793
+        for (int p = 0; p < P; p++) {
+            const int s0 = block_start(p, N, P), e0 = block_start(p + 1, N, P) - 1;
+            const int rs = (periodic && p == 0) ? 1 : s0;
+            long double prod = 1.0L;
+            for (int r = rs; r <= e0; r++) {
+                prod *= -(long double)q[(size_t)r * kQ + kQfA] * (long double)q[(size_t)r * kQ + kQfB];
+                q[(size_t)r * kQ + kQpi] = (double)prod;
+            }
+            prod = 1.0L;
+            for (int r = e0; r >= rs; r--) {
+                prod *= -(long double)q[(size_t)r * kQ + kQbC];
+                q[(size_t)r * kQ + kQrho] = (double)prod;
+            }
+        }
+    }
+    TRY(sync_stream(c));
+    if (!m.Rm) CU(cudaMalloc(&m.Rm, hRm.size() * sizeof(double)));
+    if (!m.Q) CU(cudaMalloc(&m.Q, hQ.size() * sizeof(double)));
+    CU(cudaMemcpy(m.Rm, hRm.data(), hRm.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(m.Q, hQ.data(), hQ.size() * sizeof(double), cudaMemcpyHostToDevice));
+    m.P = P;
     return GATT_OK;
 }
 
@@ -1472,6 +1525,91 @@ int vjp(gatt_ctx *c, int nsteps, double t0, double dt, int every, const double *
     return download5(c, lam0, c->a_lam);
 }
 
+
+// ---------------------------------------------------------------------------
+// Autotuner: line-solve kernel family and row-block partition per matrix set
+// ---------------------------------------------------------------------------
+
+// Candidates for a matrix set: the two register-resident families (16-row blocks) where the
+// line length allows them, and the shared-tile solver at 8, 16, 32 and 64 rows per block.
+struct TuneCand {
+    int family, rpb, P;
+};
+
+std::vector<TuneCand> tune_candidates(const DevDir &m)
+{
+    std::vector<TuneCand> out;
+    if (m.N % kRPB == 0 && m.N / kRPB <= kMaxP && m.nR >= 2 && m.nR <= kMaxNRreg) {
+        out.push_back({FAM_PIPE, kRPB, m.N / kRPB});
+        out.push_back({FAM_REG, kRPB, m.N / kRPB});
+    }
+    for (int rows : {8, 16, 32, 64}) {
+        int P = 1;
+        while (P * 2 <= kMaxP && m.N / (P * 2) >= rows && m.N / (P * 2) >= m.nR + 1) P *= 2;
+        bool dup = false;
+        for (const TuneCand &t : out) dup |= (t.family == FAM_TILE && t.P == P);
+        if (!dup) out.push_back({FAM_TILE, 0, P});
+    }
+    return out;
+}
+
+// Time every candidate on the context's grid (nf fields of scratch through one sweep, `reps`
+// launches after a warm-up, CUDA events on the context's stream) and keep the fastest.
+int autotune(gatt_ctx *c, int reps, int *family, int *blocks, double *us)
+{
+    TRY(check_ready(c, false));
+    if (reps < 1) reps = 3;
+    const int nf = c->is3d ? 5 : 4, ns = nd1(c);  // inputs in d1 slots 0..nf-1, outputs after them
+    CU(cudaMemsetAsync(c->d1, 0, sizeof(double) * (size_t)ns * c->npts * c->nb, c->stream));
+    int in[5], outs[5];
+    for (int f = 0; f < nf; f++) { in[f] = f; outs[f] = nf + f; }
+    const long long bs = (long long)ns * c->npts;
+    cudaEvent_t e0, e1;
+    CU(cudaEventCreate(&e0));
+    CU(cudaEventCreate(&e1));
+    int rc = GATT_OK;
+    const int ndir = c->is3d ? 3 : 2;
+    for (int d = 0; d < 3 && rc == GATT_OK; d++)
+        for (int k = 0; k < kMatKinds && rc == GATT_OK; k++) {
+            const int slot = d * kMatKinds + k;
+            if (family) family[slot] = -1;
+            if (blocks) blocks[slot] = 0;
+            if (us) us[slot] = 0.0;
+            DevDir &m = c->mat[d][k];
+            if (d >= ndir || !m.set || m.N < 2) continue;
+            TuneCand best{m.family, m.rpb, m.P};
+            float best_ms = -1.0f;
+            for (const TuneCand &t : tune_candidates(m)) {
+                m.family = t.family; m.rpb = t.rpb;
+                rc = upload_records(c, m, t.P);
+                if (rc != GATT_OK) break;
+                rc = sweep(c, d, k, c->d1, bs, in, c->d1, bs, outs, nf, c->nb, 0.0, nullptr);
+                if (rc != GATT_OK) break;
+                cudaEventRecord(e0, c->stream);
+                for (int r = 0; r < reps && rc == GATT_OK; r++)
+                    rc = sweep(c, d, k, c->d1, bs, in, c->d1, bs, outs, nf, c->nb, 0.0, nullptr);
+                cudaEventRecord(e1, c->stream);
+                if (rc != GATT_OK) break;
+                cudaEventSynchronize(e1);
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                ms /= reps;
+                if (best_ms < 0 || ms < best_ms) { best_ms = ms; best = t; }
+            }
+            if (rc != GATT_OK) break;
+            m.family = best.family; m.rpb = best.rpb;
+            rc = upload_records(c, m, best.P);
+            if (family) family[slot] = best.family;
+            if (blocks) blocks[slot] = best.P;
+            if (us) us[slot] = 1e3 * best_ms;
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    invalidate_graphs(c);
+    TRY(rc);
+    return sync_stream(c);
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1676,55 +1814,17 @@ int gatt_set_matrices(gatt_ctx *c, int dir, int kind, int periodic, int nRHS, in
         for (uint8_t t : cur)
             if (t >= nTypes) return fail(GATT_ERR_BADARG, "existing block types exceed nTypes");
     }
-    // Kernel row records (sweep.cuh): the reference's factors in uniform row semantics
-    // plus the block propagators of the partitioned recurrences (long double products).
     const int rpb = choose_rpb(N, nRHS);
     const int P = rpb ? N / rpb : choose_blocks(N, nRHS);
-    const int Wp = (W + 3) / 4 * 4;
-    std::vector<double> hRm((size_t)nTypes * N * Wp, 0.0), hQ((size_t)nTypes * N * kQ, 0.0);
-    for (int t = 0; t < nTypes; t++) {
-        const double *tA = &hA[(size_t)t * N], *tB = &hB[(size_t)t * N], *tC = &hC[(size_t)t * N];
-        double *q = &hQ[(size_t)t * N * kQ];
-        for (int r = 0; r < N; r++) {
-            double *qr = q + (size_t)r * kQ;
-            if (!periodic) {
-                qr[kQfA] = r > 0 ? tA[r - 1] : 0.0;       // derivs.F90:607
-                qr[kQfB] = tB[r];
-                qr[kQbC] = r < N - 1 ? tC[r] : 0.0;       // derivs.F90:610
-            } else {
-                qr[kQfA] = r >= 2 ? tA[r - 1] : 0.0;      // derivs.F90:798
-                qr[kQfB] = r >= 1 ? tB[r - 1] : 0.0;      // derivs.F90:796-798
-                qr[kQbC] = (r >= 1 && r <= N - 2) ? tC[r] : 0.0;  // derivs.F90:801
-                qr[kQD] = hD[(size_t)t * N + r];          // derivs.F90:786-789
-            }
-            for (int k = 0; k < W; k++) hRm[((size_t)t * N + r) * Wp + k] = hR[((size_t)t * N + r) * W + k];
-        }
-        if (periodic) { q[kQcA] = tA[0]; q[kQcC] = tC[0]; }  // derivs.F90:792-793
-        for (int p = 0; p < P; p++) {
-            const int s0 = block_start(p, N, P), e0 = block_start(p + 1, N, P) - 1;
-            const int rs = (periodic && p == 0) ? 1 : s0;
-            long double prod = 1.0L;
-            for (int r = rs; r <= e0; r++) {
-                prod *= -(long double)q[(size_t)r * kQ + kQfA] * (long double)q[(size_t)r * kQ + kQfB];
-                q[(size_t)r * kQ + kQpi] = (double)prod;
-            }
-            prod = 1.0L;
-            for (int r = e0; r >= rs; r--) {
-                prod *= -(long double)q[(size_t)r * kQ + kQbC];
-                q[(size_t)r * kQ + kQrho] = (double)prod;
-            }
-        }
-    }
     TRY(sync_stream(c));
     DevDir &m = c->mat[d][kind];
     cudaFree(m.Rm);
     cudaFree(m.Q);
     m = DevDir();
-    CU(cudaMalloc(&m.Rm, hRm.size() * sizeof(double)));
-    CU(cudaMalloc(&m.Q, hQ.size() * sizeof(double)));
-    CU(cudaMemcpy(m.Rm, hRm.data(), hRm.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(m.Q, hQ.data(), hQ.size() * sizeof(double), cudaMemcpyHostToDevice));
-    m.periodic = periodic; m.nR = nRHS; m.nTypes = nTypes; m.N = N; m.W = W; m.Wp = Wp; m.P = P; m.rpb = rpb;
+    m.periodic = periodic; m.nR = nRHS; m.nTypes = nTypes; m.N = N; m.W = W; m.Wp = (W + 3) / 4 * 4;
+    m.hA = std::move(hA); m.hB = std::move(hB); m.hC = std::move(hC); m.hD = std::move(hD); m.hR = std::move(hR);
+    TRY(upload_records(c, m, P));
+    m.rpb = rpb;
     m.family = rpb ? choose_family() : FAM_TILE;
     m.set = true;
     if (nBlocks > 0) {
@@ -2048,6 +2148,12 @@ int gatt_vjp(gatt_ctx *c, int nsteps, double t0, double dt, int checkpoint_every
 {
     if (!c) return fail(GATT_ERR_BADARG, "null context");
     return vjp(c, nsteps, t0, dt, checkpoint_every, lamN, lam0);
+}
+
+int gatt_autotune(gatt_ctx *c, int reps, int *family, int *blocks, double *us)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    return autotune(c, reps, family, blocks, us);
 }
 
 int gatt_selftest_pipeline_timeout(gatt_ctx *c)

@@ -281,6 +281,16 @@ class GattDNS:
         _lib.check(self.lib.gatt_vjp(self.h, nsteps, t0, dt, checkpoint_every, _dp(lv), _dp(out)), "gatt_vjp")
         return self._unpack(out)
 
+    def autotune(self, reps=3):
+        """Pick the fastest line-solve configuration per matrix set (gatt_autotune).
+        Returns {(dir, kind): (family, row blocks, us per launch)} for the sets present."""
+        fam = np.zeros(18, dtype=np.int32)
+        blk = np.zeros(18, dtype=np.int32)
+        us = np.zeros(18)
+        _lib.check(self.lib.gatt_autotune(self.h, reps, _ip(fam), _ip(blk), _dp(us)), "gatt_autotune")
+        names = ("tile", "reg", "pipe")
+        return {(i // 6 + 1, i % 6): (names[fam[i]], int(blk[i]), float(us[i])) for i in range(18) if fam[i] >= 0}
+
     def max_velocity(self):
         v = np.zeros(3 * self.nbatch)
         _lib.check(self.lib.gatt_max_velocity(self.h, _dp(v)), "gatt_max_velocity")

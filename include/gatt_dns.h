@@ -199,6 +199,16 @@ int gatt_jvp(gatt_ctx *ctx, int nsteps, double t0, double dt, const double *dq0,
 int gatt_vjp(gatt_ctx *ctx, int nsteps, double t0, double dt, int checkpoint_every, const double *lamN,
              double *lam0);
 
+/* Autotuner (no counterpart in the reference): for every matrix set of the context, times
+ * each applicable line-solve configuration on the context's grid -- the TMA-fed and the plain
+ * register-resident solvers (16-row blocks) and the shared-tile solver at 8, 16, 32 and 64
+ * rows per block -- over `reps` launches of one sweep of 5 (3-D) or 4 (2-D) scratch fields,
+ * and keeps the fastest.  Per set (index dir*6 + kind, dir 0..2, kind 0..5), family[] gets
+ * 0 shared tile, 1 register, 2 TMA-fed register (-1: no matrices), blocks[] the row-block
+ * count and us[] the mean microseconds of one launch; any of them may be NULL.  Overwrites
+ * the derivative scratch; call it after the matrices and before the first step. */
+int gatt_autotune(gatt_ctx *ctx, int reps, int *family, int *blocks, double *us);
+
 /* Self-test of the pipelined line solver's failure path (no counterpart in the reference):
  * runs one x-direction sweep whose copy barriers expect 16 bytes more than the copies
  * deliver, so that every bounded wait gives up (after 1 s; the real copies have landed by

@@ -239,6 +239,14 @@ module gatt_dns
             real(c_double), dimension(*) :: lamN, lam0
             integer(c_int) :: gatt_vjp
         end function
+        function gatt_autotune(ctx, reps, family, blocks, us) bind(C, name='gatt_autotune')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: ctx
+            integer(c_int), value :: reps
+            integer(c_int), dimension(*) :: family, blocks
+            real(c_double), dimension(*) :: us
+            integer(c_int) :: gatt_autotune
+        end function
         function gatt_selftest_pipeline_timeout(ctx) bind(C, name='gatt_selftest_pipeline_timeout')
             import :: c_int, c_ptr
             type(c_ptr), value :: ctx

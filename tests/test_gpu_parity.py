@@ -248,3 +248,30 @@ def test_errors_are_reported(libs):
         g.step(0.0, 1e-3)
     assert e.value.code == 4
     g.close()
+
+
+@pytest.mark.parametrize("name", ["box64", "cavity3d_32", "bl", "lid"])
+def test_autotuned_configuration_matches_oracle(libs, name):
+    """gatt_autotune may pick any kernel family and row-block partition per matrix set; the
+    results must stay those of the oracle."""
+    c, g, o = pair(name)
+    choice = g.autotune(reps=2)
+    ndir = 3 if c.is3d else 2
+    assert all((d, k) in choice for d in range(1, ndir + 1) for k in (0, 1))
+    for (d, k), (fam, P, us) in choice.items():
+        assert fam in ("tile", "reg", "pipe") and P >= 1 and us > 0
+    rng = np.random.default_rng(12)
+    F = np.asfortranarray(rng.standard_normal((c.nx, c.ny, c.nz)))
+    for d in range(1, ndir + 1):
+        for kind in ("deriv", "filter"):
+            assert rel(g.calc_derivs(F, d, kind), o.calc_derivs(F, d, kind)) < RHS_TOL, (name, d, kind)
+    f = flow_for(c, seed=4)
+    dt = 0.25 * c.cfl_dt(f["U"], f["V"], f["W"], 1.0)
+    g.upload(f)
+    st = o.new_state(f)
+    g.step(0.0, dt)
+    o.step(st, 0.0, dt)
+    a = g.download()
+    for k in KEYS:
+        assert rel(a[k], st[k]) < STEP_TOL * 10, (name, k)
+    g.close()
