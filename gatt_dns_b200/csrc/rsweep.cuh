@@ -119,6 +119,16 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t
                  : "memory");
 }
 
+// Contiguous shared -> global copy (bulk-group completion) and its group waits.
+__device__ __forceinline__ void bulk_s2g(void *dst, uint32_t src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 // ---- the solve of one row block from registers -------------------------------------------
 // On entry w[k] = row p*RPB - (NR-1) + k of this thread's line; on return w[j] (j < RPB) =
 // the solution at row p*RPB + j.  Every thread of the CTA calls it (three or four barriers).
@@ -370,6 +380,7 @@ __global__ void __launch_bounds__(32 * kMaxP) k_psweep(const SweepArgs a, const 
             if (threadIdx.x < kLanes) {
                 const int L0 = tile * kLanes;
                 const int nv = min(kLanes, a.nlines - L0);
+                bulk_wait_read0();  // this lane's store out of the stage has read it
                 fence_proxy_async();
                 if (lane == 0) mbar_expect_tx(bar, (uint32_t)(nv * N * sizeof(double) + a.tx_extra));
                 __syncwarp();
@@ -441,22 +452,54 @@ __global__ void __launch_bounds__(32 * kMaxP) k_psweep(const SweepArgs a, const 
                 *(volatile int *)a.err = 1;
                 if (nst > 1 && j + G < a.njobs) mbar_wait(bar0 + 8 * ((k + 1) % nst), (uint32_t)((k + 1) / nst) & 1u);
             }
+            if (XD && threadIdx.x < kLanes) bulk_wait0();  // stores already issued
             __syncthreads();
             return;
         }
-        // every warp has its rows: refill this stage (blend keeps it for the epilogue)
-        if (!blend_on && j + nst * G < a.njobs) issue(j + nst * G, s);
+        // y/z: every warp has its rows, refill this stage now (blend keeps it for the epilogue);
+        // x: the stage also carries the results out, it is refilled after the stores
+        if (!XD && !blend_on && j + nst * G < a.njobs) issue(j + nst * G, s);
 
         solve_block<PER, NR, RPB, false>(w, Rr, Qt, Qr, xs, lane, p, P);
-        if (lr.valid) {
-            double *Gl = a.out + (long long)b * a.out_bstride + (long long)a.out_slot[f] * a.npts + lr.base;
-            store_block<XD, RPB>(w, Gl, lr.s, sp, blend_on, blend, [&](int jj) { return lds(sp + jj); });
-        }
-        if (blend_on) {
+        if (XD) {
+            // results back into the stage (its own line, rows sp..), then one contiguous bulk
+            // store per line: 1 KB copies instead of 32-byte pieces scattered over 32 lines
+            double *lw = const_cast<double *>(ln);
+#pragma unroll
+            for (int q = 0; q < RPB / 2; q++) {
+                double2 v = make_double2(w[2 * q], w[2 * q + 1]);
+                if (blend_on) {
+                    const double2 o = *reinterpret_cast<const double2 *>(lw + sp + 2 * q);
+                    v.x = o.x + blend * (v.x - o.x);
+                    v.y = o.y + blend * (v.y - o.y);
+                }
+                *reinterpret_cast<double2 *>(lw + sp + 2 * q) = v;
+            }
+            fence_proxy_async();
             __syncthreads();
+            if (threadIdx.x < kLanes) {
+                const int L0 = tile * kLanes;
+                if (lane < min(kLanes, a.nlines - L0)) {
+                    bulk_s2g(a.out + (long long)b * a.out_bstride + (long long)a.out_slot[f] * a.npts +
+                                 (long long)(L0 + lane) * N,
+                             st0 + (uint32_t)((s * stage_d + lane * (N + 2)) * sizeof(double)),
+                             (uint32_t)(N * sizeof(double)));
+                    bulk_commit();
+                }
+            }
             if (j + nst * G < a.njobs) issue(j + nst * G, s);
+        } else {
+            if (lr.valid) {
+                double *Gl = a.out + (long long)b * a.out_bstride + (long long)a.out_slot[f] * a.npts + lr.base;
+                store_block<XD, RPB>(w, Gl, lr.s, sp, blend_on, blend, [&](int jj) { return lds(sp + jj); });
+            }
+            if (blend_on) {
+                __syncthreads();
+                if (j + nst * G < a.njobs) issue(j + nst * G, s);
+            }
         }
     }
+    if (XD && threadIdx.x < kLanes) bulk_wait0();  // every store has landed before the CTA leaves
 }
 
 }  // namespace gatt
