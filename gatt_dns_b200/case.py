@@ -590,6 +590,96 @@ def boundary_layer(nx=400, ny=150, nz=64, Lx=6.0, Ly=5.0, Lz=1.0, Re=1000.0, Ma=
                 gamma=gamma, T0=T0, X=X, Y=Y, Z=Z, mats=mats, bc=bc, flowRegion=fr, dxmin=_dxmin(X, Y, Z))
 
 
+def sfd_region(shape, buffers, X):
+    """calcSFDregion.m:4-53 with applyX/Y/Z = 2: X * (1 - prod of 0.5 - 0.5 cos ramps over the
+    buffer zones); buffers[d] = (n initial, n final) buffer nodes of direction d."""
+    chi = np.ones(shape)
+    for d, (ni, nf) in enumerate(buffers):
+        for i in range(1, ni + 1):
+            idx = [slice(None)] * 3
+            idx[d] = i - 1
+            chi[tuple(idx)] *= 0.5 - 0.5 * math.cos(math.pi * (i - 1) / ni)
+        for i in range(1, nf + 1):
+            idx = [slice(None)] * 3
+            idx[d] = shape[d] - i
+            chi[tuple(idx)] *= 0.5 - 0.5 * math.cos(math.pi * (i - 1) / nf)
+    return np.asfortranarray(X * (1.0 - chi))
+
+
+def boundary_layer_cavity(nx=800, ny=300, Re=1000.0, Ma=0.5, Pr=0.71, gamma=1.4, T0=300.0, filter_alpha=0.49,
+                          deriv="SL4", cavity=(1.0, 2.0), buffers=((40, 30), (0, 40)), ny_cavity=None,
+                          sfd=(0.02, 15.0)):
+    """2-D compressible boundary layer over a rectangular cavity with buffer zones and SFD.
+
+    Domain x in [-1, 5], y in [-1, 4] (physical part), cavity of depth 1 at 1 < x < 2, the
+    buffer zones of parameters.m:124-142 (sigmoid; inflow 40, outflow 30 and top 40 nodes
+    in the full case) with EX4 derivatives inside them, and the boundary set of
+    boundaryLayerIsothermal.m for mesh.X(1) < 0: Dirichlet inflow u = 1, v = 0, e = E0 with
+    pressure Neumann (:4-66), outflow null second derivatives with p = P0 (:83-145), outer
+    flow null second derivatives (:146-207), no-slip isothermal walls (findWallsForBoundaries
+    + the wall list), and free slip (u Neumann) on the wall upstream of the leading edge x = 0
+    (:408-429).  SFD type 2 on the buffer zones (calcSFDregion.m), X and Delta from `sfd`.
+    nx, ny count all nodes, buffers included.
+    """
+    (bxi, bxf), (byi, byf) = buffers
+    sig = lambda n, st: {"n": n, "type": "sigmoid", "stretching": st, "transition": 0.2}
+    X = generate_mesh(-1.0, 5.0, nx - bxi - bxf, buffer_i=sig(bxi, 30) if bxi else None,
+                      buffer_f=sig(bxf, 15) if bxf else None)
+    ny_phys = ny - byi - byf
+    nyc = ny_cavity or max(4, ny_phys // 6)
+    yc = np.linspace(-1.0, 0.0, nyc)
+    yu = generate_mesh(0.0, 4.0, ny_phys - nyc + 1, mtype="tanh", par=1.5, local="i",
+                       buffer_f=sig(byf, 30) if byf else None)
+    Y = np.concatenate([yc[:-1], yu])
+    Z = np.array([0.0])
+    x0, x1 = cavity
+    # solid at and below y = 0 (the plate surface row is wall), except the cavity's inside
+    fr = (Y[None, :, None] > 0) | ((X[:, None, None] > x0) & (X[:, None, None] < x1))
+    fr = np.array(fr, copy=True)
+    fr[:, 0, :] = False
+    fr, walls, corners, inside = find_walls_for_boundaries(fr)
+    E0 = 1.0 / ((gamma ** 2 - gamma) * Ma ** 2)
+    P0 = (gamma - 1) * E0
+    # the reference's order: inflow, outflow and outer flow over whole boundary planes, then
+    # the walls, whose Dirichlet values override those planes at solid nodes
+    items = []
+    inflow = [1, 1, 1, ny, 1, 1]
+    for v, val in (("u", 1.0), ("v", 0.0), ("e", E0)):
+        items.append((v, "dir", "xi", val, list(inflow)))
+    items.append(("p", "neu", "xi", 0.0, list(inflow)))
+    outflow = [nx, nx, 1, ny, 1, 1]
+    for v in ("u", "v", "e"):
+        items.append((v, "sec", "xf", 0.0, list(outflow)))
+    items.append(("p", "dir", "xf", P0, list(outflow)))
+    top = [1, nx, ny, ny, 1, 1]
+    for v in ("u", "v", "e", "p"):
+        items.append((v, "sec", "yf", 0.0, list(top)))
+    items += wall_boundary_list(walls, inside, P0, E0)
+    j0 = int(np.argmin(np.abs(Y))) + 1                    # 1-based row of y = 0
+    # the solid nodes of the inflow and outflow planes keep the wall values (no slip, E0)
+    for i in (1, nx):
+        box = [i, i, 1, j0, 1, 1]
+        for v, val in (("u", 0.0), ("v", 0.0), ("e", E0)):
+            items.append((v, "dir", "yi", val, list(box)))
+    # free slip on the plate row upstream of the leading edge x = 0 (:408-429)
+    ile = int(np.argmin(np.abs(X)))                       # 0-based node of the leading edge
+    items.append(("u", "neu", "yi", 0.0, [1, max(1, ile), j0, j0, 1, 1]))
+    n1, n2 = mx.neumann_coefficients(6, 2)
+    bc = init_boundaries(items, corners, mx.fortran_round(n1), mx.fortran_round(n2))
+    bufs = [{"i": sig(bxi, 30) if bxi else {"n": 0}, "f": sig(bxf, 15) if bxf else {"n": 0}},
+            {"i": {"n": 0}, "f": sig(byf, 30) if byf else {"n": 0}},
+            {"i": {"n": 0}, "f": {"n": 0}}]
+    mats = build_matrices(X, Y, Z, fr, (False, False, False), (False, False, False), (6.0, 5.0, 1.0),
+                          deriv=deriv, deriv_buffer="EX4", filter_alpha=filter_alpha, filter_borders="decentered",
+                          buffers=bufs)
+    case = Case(name="bl_cavity_%dx%d" % (nx, ny), nx=nx, ny=ny, nz=1, Re=Re, Ma=Ma, Pr=Pr, gamma=gamma, T0=T0,
+                X=X, Y=Y, Z=Z, mats=mats, bc=bc, flowRegion=fr, dxmin=_dxmin(X, Y, Z))
+    if sfd:
+        case.sfd_type, case.sfd_X, case.sfd_delta = 2, sfd[0], sfd[1]
+        case.sfd_chi = sfd_region((nx, ny, 1), ((bxi, bxf), (byi, byf), (0, 0)), sfd[0])
+    return case
+
+
 def blasius_profile(eta_max=12.0, n=6001):
     """Blasius similarity solution f(eta), f'(eta): f''' + f f''/2 = 0, f(0) = f'(0) = 0,
     f'(inf) = 1, by RK4 shooting on f''(0).  It stands in for the compressible profile of
@@ -626,11 +716,13 @@ def blasius_profile(eta_max=12.0, n=6001):
 
 def blasius_flow(case: Case, x0=1.0):
     """Blasius base flow: u = f'(eta), v = (eta f' - f) / (2 sqrt(Re x)) with eta = y sqrt(Re / x)
-    and x measured from a virtual origin x0 upstream of the inflow; R = 1, E = E0."""
+    and x measured from a virtual origin x0 upstream of the leading edge x = 0 (upstream of
+    it the leading-edge profile is repeated; below y = 0 the fluid is at rest); R = 1, E = E0."""
     eta_t, f_t, fp_t = blasius_profile()
     s = (case.nx, case.ny, case.nz)
-    x = case.X[:, None] + x0
+    x = np.maximum(case.X, 0.0)[:, None] + x0
     eta = case.Y[None, :] * np.sqrt(case.Re / x)
+    eta = np.maximum(eta, 0.0)
     f = np.where(eta <= eta_t[-1], np.interp(eta, eta_t, f_t), f_t[-1] + (eta - eta_t[-1]))
     fp = np.interp(eta, eta_t, fp_t, right=1.0)
     v = (eta * fp - f) / (2.0 * np.sqrt(case.Re * x))

@@ -364,22 +364,27 @@ int choose_rpb(int N, int nR)
     return (N % kRPB == 0 && N / kRPB <= kMaxP) ? kRPB : 0;
 }
 
-size_t sweep_smem(int N, int P, int nR, int Wp) { return sweep_smem_doubles(N, P, nR, Wp) * sizeof(double); }
+size_t sweep_smem(int N, int P, int nR, int Wp, bool stage = true)
+{
+    return sweep_smem_doubles(N, P, nR, Wp, stage) * sizeof(double);
+}
 // 227 KB per block, less a margin for the kernel's few static shared variables
 constexpr size_t kMaxSmem = 227 * 1024 - 256;
 constexpr int kMaxNR = 11;  // widest band the shared-tile solver is instantiated for
 
 // Row blocks per line: about 32 rows per block (shorter dependency chains, more warps per
-// tile), a power of two up to kMaxP, and every block at least nR+1 rows long.
-int choose_blocks(int N, int nR)
+// tile), a power of two up to kMaxP, every block at least nR+1 rows long, and few enough
+// that the shared tile fits (long lines: fewer blocks, halo and exchange rows).
+int choose_blocks(int N, int nR, int Wp, int rows = 0)
 {
-    static int rows = [] {
+    if (rows < 4) {
         const char *e = getenv("GATT_BLOCK_ROWS");
         const int v = e ? atoi(e) : 0;
-        return v >= 4 ? v : 32;
-    }();
+        rows = v >= 4 ? v : 32;
+    }
     int P = 1;
     while (P * 2 <= kMaxP && N / (P * 2) >= rows && N / (P * 2) >= nR + 1) P *= 2;
+    while (P > 1 && sweep_smem(N, P, nR, Wp, false) > kMaxSmem) P /= 2;
     return P;
 }
 
@@ -538,7 +543,8 @@ int sweep(gatt_ctx *c, int d, int kind, const double *in, long long in_bs, const
         int r = launch_psweep(c, m, d, a, nmembers, cls);
         if (r != GATT_ERR_STATE) return r;  // GATT_ERR_STATE: layout not expressible, use k_rsweep
     }
-    const size_t smem = m.rpb ? (size_t)3 * m.P * kLanes * sizeof(double) : sweep_smem(m.N, m.P, m.nR, m.Wp);
+    a.stage = !m.rpb && sweep_smem(m.N, m.P, m.nR, m.Wp, true) <= kMaxSmem;
+    const size_t smem = m.rpb ? (size_t)3 * m.P * kLanes * sizeof(double) : sweep_smem(m.N, m.P, m.nR, m.Wp, a.stage);
     void *k = m.rpb ? reg_kernel(false, d == 0, m.periodic != 0, m.nR)
                     : sweep_kernel(d == 0, m.periodic != 0, m.nR, m.P > 4);
     if (k && smem <= kMaxSmem && m.N >= 2) {
@@ -1544,8 +1550,7 @@ std::vector<TuneCand> tune_candidates(const DevDir &m)
         out.push_back({FAM_REG, kRPB, m.N / kRPB});
     }
     for (int rows : {8, 16, 32, 64}) {
-        int P = 1;
-        while (P * 2 <= kMaxP && m.N / (P * 2) >= rows && m.N / (P * 2) >= m.nR + 1) P *= 2;
+        const int P = choose_blocks(m.N, m.nR, m.Wp, rows);
         bool dup = false;
         for (const TuneCand &t : out) dup |= (t.family == FAM_TILE && t.P == P);
         if (!dup) out.push_back({FAM_TILE, 0, P});
@@ -1815,7 +1820,7 @@ int gatt_set_matrices(gatt_ctx *c, int dir, int kind, int periodic, int nRHS, in
             if (t >= nTypes) return fail(GATT_ERR_BADARG, "existing block types exceed nTypes");
     }
     const int rpb = choose_rpb(N, nRHS);
-    const int P = rpb ? N / rpb : choose_blocks(N, nRHS);
+    const int P = rpb ? N / rpb : choose_blocks(N, nRHS, (W + 3) / 4 * 4);
     TRY(sync_stream(c));
     DevDir &m = c->mat[d][kind];
     cudaFree(m.Rm);

@@ -68,6 +68,7 @@ struct SweepArgs {
     double blend_fct;
     int epi;                 // SweepEpi
     int P;                   // row blocks per line (1 .. kMaxP); CTA = 32*P threads
+    int stage;               // k_sweep: shared memory holds a coefficient copy (1) or not (0)
     // pipelined solver (k_psweep) only
     int dir;                 // 0 x, 1 y, 2 z
     int nf;                  // fields per launch
@@ -118,11 +119,12 @@ __device__ __forceinline__ void ld4_coef(const double *p, double *v)
 constexpr int kCh = 8;
 
 // Shared memory of k_sweep, in doubles: the tile [N][32], the right halos of the row
-// blocks [P][NR-1][32], the block-exchange values [3][P][32], then the coefficients of the
-// tile's matrix type (band rows [N][Wp] and records [N][kQ]) when all its lines share one.
-__host__ __device__ __forceinline__ size_t sweep_smem_doubles(int N, int P, int NR, int Wp)
+// blocks [P][NR-1][32], the block-exchange values [3][P][32], then (stage) the coefficients
+// of the tile's matrix type (band rows [N][Wp] and records [N][kQ]) when all its lines share
+// one.  Long lines whose tile leaves no room for the coefficients read them through L1.
+__host__ __device__ __forceinline__ size_t sweep_smem_doubles(int N, int P, int NR, int Wp, bool stage = true)
 {
-    return ((size_t)N + (size_t)P * (NR - 1) + 3 * (size_t)P) * kLanes + (size_t)N * (Wp + kQ);
+    return ((size_t)N + (size_t)P * (NR - 1) + 3 * (size_t)P) * kLanes + (stage ? (size_t)N * (Wp + kQ) : 0);
 }
 
 // BIG: instantiation for P > 4 (up to 32*kMaxP threads); otherwise at most 128 threads,
@@ -214,7 +216,7 @@ __global__ void __launch_bounds__(BIG ? 32 * kMaxP : 128) k_sweep(const SweepArg
     double *sQ = sR + (size_t)N * Wp;
     const int sp = block_start(p, N, P), ep = block_start(p + 1, N, P) - 1;
     const double *Rm, *Q;
-    if (tu >= 0) {
+    if (tu >= 0 && a.stage) {
         // each warp copies the records of its own rows
         const double *gR = a.Rm + ((size_t)tu * N + sp) * Wp;
         const double *gQ = a.Q + ((size_t)tu * N + sp) * kQ;

@@ -54,6 +54,8 @@ def get_case(name):
                                              sfd={"X": 0.05, "Delta": 10.0, "buffer": 6})
         elif name == "bl":
             _CASES[name] = cs.boundary_layer(nx=48, ny=32, nz=16)
+        elif name == "bl_cavity":
+            _CASES[name] = cs.boundary_layer_cavity(nx=96, ny=48, buffers=((8, 6), (0, 8)))
         elif name == "long_x":
             _CASES[name] = cs.lid_driven(nxy=(900, 12))
     return _CASES[name]
@@ -95,7 +97,7 @@ def test_line_solves(libs, monkeypatch, name, kind, solver):
 
 
 @pytest.mark.parametrize("name", ["box", "box_aniso", "box64", "lid", "lid64", "lid_tanh", "cavity2d", "cavity3d",
-                                  "cavity3d_32", "bl"])
+                                  "cavity3d_32", "bl", "bl_cavity"])
 def test_rhs(libs, name):
     c, g, o = pair(name)
     f = flow_for(c)
@@ -133,7 +135,7 @@ def test_filter_in_place(libs, name):
 
 
 @pytest.mark.parametrize("name", ["box", "box_aniso", "box64", "lid", "lid64", "lid_tanh", "cavity2d", "cavity3d",
-                                  "cavity3d_32", "bl"])
+                                  "cavity3d_32", "bl", "bl_cavity"])
 def test_step(libs, name):
     c, g, o = pair(name)
     f = flow_for(c, seed=2)
