@@ -344,8 +344,11 @@ __global__ void __launch_bounds__(32 * kMaxP) k_rsweep(const SweepArgs a)
 // y/z tiles: one tensor box {x: 32, line: N} of the 5-D map (x, y, z, field slot, member);
 // x tiles: one bulk copy per line into a [32][N+2] stage (the pad keeps 16-byte reads of
 // two rows conflict-free).
+// Register cap: the 768-thread bound holds a thread to 80 registers, which keeps three
+// 256-thread CTAs resident (84 registers round up to two); the y/z 6-band filter spills at
+// 80 and keeps the plain 512-thread bound.
 template <bool XD, bool PER, int NR, int RPB>
-__global__ void __launch_bounds__(32 * kMaxP) k_psweep(const SweepArgs a, const __grid_constant__ CUtensorMap tmap)
+__global__ void __launch_bounds__((NR == 6 && !XD) ? 32 * kMaxP : 768) k_psweep(const SweepArgs a, const __grid_constant__ CUtensorMap tmap)
 {
     constexpr int H = NR - 1;
     constexpr int WP = (2 * NR - 1 + 3) / 4 * 4;
