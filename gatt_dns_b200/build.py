@@ -8,7 +8,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc", "gatt_dns.cu")
 OUT = os.path.join(HERE, "libgatt_dns_b200.so")
-HEADERS = [os.path.join(HERE, "csrc", f) for f in ("sweep.cuh", "rsweep.cuh", "pointwise.cuh", "bc.cuh", "arnoldi.cuh", "tangent.cuh")] + \
+HEADERS = [os.path.join(HERE, "csrc", f) for f in ("sweep.cuh", "rsweep.cuh", "pointwise.cuh", "pwpipe.cuh", "bc.cuh", "arnoldi.cuh", "tangent.cuh")] + \
     [os.path.join(HERE, "..", "include", "gatt_dns.h")]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",

@@ -22,6 +22,7 @@
 #include "tangent.cuh"
 #include "bc.cuh"
 #include "pointwise.cuh"
+#include "pwpipe.cuh"
 #include "rsweep.cuh"
 #include "sweep.cuh"
 
@@ -163,6 +164,7 @@ struct gatt_ctx {
     int nsm = 148;
     int *h_err = nullptr;   // pipeline wait give-up flag (pinned, device-mapped)
     int *d_err = nullptr;
+    bool pw_pipe = true;    // 3-D assembly fed by bulk copies (GATT_PW=plain: thread loads)
     // per-kernel-class timing (gatt_profile_kernels): events around every launch
     bool profiling = false;
     int prof_cls = -1;
@@ -182,7 +184,7 @@ int sync_stream(gatt_ctx *c)
     CU(cudaStreamSynchronize(c->stream));
     if (c->h_err && *(volatile int *)c->h_err) {
         *(volatile int *)c->h_err = 0;
-        return fail(GATT_ERR_TIMEOUT, "a line-solve copy pipeline gave up (tile wait timed out or misaligned ring)");
+        return fail(GATT_ERR_TIMEOUT, "a copy pipeline gave up (tile wait timed out or misaligned ring)");
     }
     return GATT_OK;
 }
@@ -406,6 +408,8 @@ int set_sweep_attributes()
                 CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
                 CU(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
             }
+    CU(cudaFuncSetAttribute((const void *)k_assemble3d_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)pw_smem_bytes(kPwStages)));
     return GATT_OK;
 }
 
@@ -581,6 +585,70 @@ int sweep(gatt_ctx *c, int d, int kind, const double *in, long long in_bs, const
 // right-hand side + stage update
 // ---------------------------------------------------------------------------
 
+// Tensor map {points, slots, members, 1, 1} of `nslots` fields starting at base[0..nslots)
+// (equally spaced, checked) with member stride bstride; false when the layout does not fit the
+// copy engine's rules (16-byte aligned start, strides multiples of 16 bytes).
+bool pw_map(const gatt_ctx *c, CUtensorMap *map, const double *const *base, int nslots, long long bstride, int nmem)
+{
+    const long long n = c->npts;
+    const long long sstride = nslots > 1 ? (long long)(base[1] - base[0]) : n;
+    for (int f = 1; f < nslots; f++)
+        if (base[f] != base[0] + f * sstride) return false;
+    if ((reinterpret_cast<uintptr_t>(base[0]) & 15) || (n & 1) || (sstride & 1) || sstride < n) return false;
+    if (nmem > 1 && ((bstride & 1) || bstride < sstride * nslots)) return false;
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return false;
+    memset(map, 0, sizeof(*map));
+    cuuint64_t dims[5] = {(cuuint64_t)n, (cuuint64_t)nslots, (cuuint64_t)nmem, 1, 1};
+    const long long ms = nmem > 1 ? bstride : sstride * nslots;
+    cuuint64_t strides[4] = {(cuuint64_t)sstride * 8, (cuuint64_t)ms * 8, (cuuint64_t)ms * nmem * 8,
+                             (cuuint64_t)ms * nmem * 8};
+    cuuint32_t box[5] = {(cuuint32_t)kPwC, (cuuint32_t)nslots, 1, 1, 1};
+    cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<double *>(base[0]), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// 3-D assembly fed by tensor copies (pwpipe.cuh).  Returns GATT_ERR_STATE without launching
+// when a set's layout does not fit the tensor maps; the caller then runs k_assemble3d.
+int launch_assemble3d_pipe(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet &out,
+                           const FieldSet &delta, const FieldSet &d1, const FieldSet &d2, int mode, int nmem)
+{
+    if (!c->pw_pipe || (c->npts & 1)) return GATT_ERR_STATE;
+    PwArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = c->npts;
+    a.nchunks = (a.n + kPwC - 1) / kPwC;
+    a.njobs = a.nchunks * nmem;
+    a.nst = kPwStages;
+    a.mode = mode;
+    a.use_delta = delta.p && mode >= RK_STAGE2;
+    a.use_q0 = 0;
+    if (mode != RK_STORE_RHS)
+        for (int f = 0; f < 5; f++)
+            if (q0.v[f] != q.v[f] || q0.bstride != q.bstride) a.use_q0 = 1;
+    a.err = c->d_err;
+    PwMaps maps;
+    memset(&maps, 0, sizeof(maps));
+    const double *qb[5], *q0b[5], *d1b[D3_N], *d2b[S3_N], *dlb[5];
+    for (int f = 0; f < 5; f++) { qb[f] = q.v[f]; q0b[f] = q0.v[f]; dlb[f] = delta.p ? delta.p + f * delta.npts : nullptr; }
+    for (int f = 0; f < D3_N; f++) d1b[f] = d1.p + f * d1.npts;
+    for (int f = 0; f < S3_N; f++) d2b[f] = d2.p + f * d2.npts;
+    if (!pw_map(c, &maps.m[PW_Q], qb, 5, q.bstride, nmem) || !pw_map(c, &maps.m[PW_D1], d1b, D3_N, d1.bstride, nmem) ||
+        !pw_map(c, &maps.m[PW_D2], d2b, S3_N, d2.bstride, nmem))
+        return GATT_ERR_STATE;
+    if (a.use_q0 && !pw_map(c, &maps.m[PW_Q0], q0b, 5, q0.bstride, nmem)) return GATT_ERR_STATE;
+    if (a.use_delta && !pw_map(c, &maps.m[PW_DL], dlb, 5, delta.bstride, nmem)) return GATT_ERR_STATE;
+    const size_t smem = pw_smem_bytes(a.nst);
+    const int per_sm = resident_ctas((const void *)k_assemble3d_pipe, 2 * kPwC, smem);
+    if (per_sm < 1) return GATT_ERR_STATE;
+    const long long grid = std::min<long long>(a.njobs, (long long)per_sm * c->nsm);
+    TRY(before_launch(c, PC_ASSEMBLE));
+    k_assemble3d_pipe<<<(unsigned)grid, 2 * kPwC, smem, c->stream>>>(c->ph, out, delta, a, c->d_params, maps);
+    return after_launch(c);
+}
+
 // nseq2d/nseq3d on stage input q, fused with the RK4 update into out (mode).
 int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet &out, int mode, int nmem,
               double *d1, double *tq, double *d2, double *delta, bool assemble = true)
@@ -610,9 +678,11 @@ int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet
         TRY(sweep(c, 1, 0, tq, btq, iy, d2, bd2, sy, 4, nmem, 0, nullptr, PC_D2Y));
         TRY(sweep(c, 2, 0, tq, btq, iz, d2, bd2, sz, 4, nmem, 0, nullptr, PC_D2Z));
         if (!assemble) return GATT_OK;  // the gradients and second sweeps only (tangent / adjoint)
+        const FieldSet fd = fset(c, delta, 5), f1 = fset(c, d1, D3_N), f2 = fset(c, d2, S3_N);
+        const int pr = launch_assemble3d_pipe(c, q, q0, out, fd, f1, f2, mode, nmem);
+        if (pr != GATT_ERR_STATE) return pr;
         TRY(before_launch(c, PC_ASSEMBLE));
-        k_assemble3d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(
-            c->ph, q, q0, out, fset(c, delta, 5), fset(c, d1, D3_N), fset(c, d2, S3_N), n, mode, sp);
+        k_assemble3d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(c->ph, q, q0, out, fd, f1, f2, n, mode, sp);
         return after_launch(c);
     }
     const long long bd1 = D2_N * n, btq = T2_N * n, bd2 = S2_N * n;
@@ -1651,6 +1721,10 @@ int gatt_create(gatt_ctx **out, int nx, int ny, int nz, int nbatch)
     c->nx = nx; c->ny = ny; c->nz = nz; c->nb = nbatch;
     c->npts = (long long)nx * ny * nz;
     c->is3d = nz > 1;
+    {
+        const char *pw = getenv("GATT_PW");
+        c->pw_pipe = !(pw && !strcmp(pw, "plain"));
+    }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);

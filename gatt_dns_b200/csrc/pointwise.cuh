@@ -82,27 +82,37 @@ __device__ __forceinline__ Stress3 stress3d(double c, double dux, double duy, do
     return t;
 }
 
-// Stresses and heat fluxes, 3-D (nseq.F90:225-239, 286-288)
+// Stresses and heat fluxes at one point, 3-D (nseq.F90:225-239, 286-288): out[] in T3_* order;
+// ld(i) returns the gradient of slot i in D3_* order (the R gradients are not read).
+template <typename Ld>
+__device__ __forceinline__ void visc3d_point(const Phys &ph, double E, Ld ld, double out[T3_N])
+{
+    const double mu = sutherland_mu(ph, E);
+    const double c = 1.0 / ph.Re * mu;
+    const Stress3 t = stress3d(c, ld(D3_UX), ld(D3_UY), ld(D3_UZ), ld(D3_VX), ld(D3_VY), ld(D3_VZ), ld(D3_WX),
+                               ld(D3_WY), ld(D3_WZ));
+    out[T3_XX] = t.xx;
+    out[T3_YY] = t.yy;
+    out[T3_ZZ] = t.zz;
+    out[T3_XY] = t.xy;
+    out[T3_XZ] = t.xz;
+    out[T3_YZ] = t.yz;
+    const double h = -ph.gamma / ph.Re / ph.Pr * mu;
+    out[T3_QX] = h * ld(D3_EX);
+    out[T3_QY] = h * ld(D3_EY);
+    out[T3_QZ] = h * ld(D3_EZ);
+}
+
+// Stresses and heat fluxes, 3-D, thread per point.
 __global__ void __launch_bounds__(256) k_visc3d(Phys ph, StateSet q, FieldSet d1, FieldSet tq, long long n)
 {
     const int b = blockIdx.y;
     const double *E = q.v[4] + b * q.bstride;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-        const double mu = sutherland_mu(ph, E[p]);
-        const double c = 1.0 / ph.Re * mu;
-        const Stress3 t = stress3d(c, d1.f(b, D3_UX)[p], d1.f(b, D3_UY)[p], d1.f(b, D3_UZ)[p], d1.f(b, D3_VX)[p],
-                                   d1.f(b, D3_VY)[p], d1.f(b, D3_VZ)[p], d1.f(b, D3_WX)[p], d1.f(b, D3_WY)[p],
-                                   d1.f(b, D3_WZ)[p]);
-        tq.f(b, T3_XX)[p] = t.xx;
-        tq.f(b, T3_YY)[p] = t.yy;
-        tq.f(b, T3_ZZ)[p] = t.zz;
-        tq.f(b, T3_XY)[p] = t.xy;
-        tq.f(b, T3_XZ)[p] = t.xz;
-        tq.f(b, T3_YZ)[p] = t.yz;
-        const double h = -ph.gamma / ph.Re / ph.Pr * mu;
-        tq.f(b, T3_QX)[p] = h * d1.f(b, D3_EX)[p];
-        tq.f(b, T3_QY)[p] = h * d1.f(b, D3_EY)[p];
-        tq.f(b, T3_QZ)[p] = h * d1.f(b, D3_EZ)[p];
+        double o[T3_N];
+        visc3d_point(ph, E[p], [&](int i) { return d1.f(b, i)[p]; }, o);
+#pragma unroll
+        for (int i = 0; i < T3_N; i++) tq.f(b, i)[p] = o[i];
     }
 }
 
@@ -136,43 +146,76 @@ __device__ __forceinline__ void rk_update(int mode, double dt, double k, double 
     }
 }
 
+// Input slots of the 3-D assembly: the stage state U, V, W, R, E, the 15 first derivatives
+// (D3_* order), the 12 second-sweep results (S3_* order).
+enum { A3_Q = 0, A3_D1 = 5, A3_D2 = 20, A3_NIN = 32 };
+
+// dU, dV, dW, dR of nseq.F90:310-317 at one point, k[] in U, V, W, R order; ld(i) returns
+// input slot i.  One definition for both assembly kernels.
+template <typename Ld>
+__device__ __forceinline__ void assemble3d_mom(const Phys &ph, Ld ld, double k[4])
+{
+    const double g = ph.gamma;
+    const double u = ld(A3_Q + 0), v = ld(A3_Q + 1), w = ld(A3_Q + 2), r = ld(A3_Q + 3), e = ld(A3_Q + 4);
+    const double dux = ld(A3_D1 + D3_UX), duy = ld(A3_D1 + D3_UY), duz = ld(A3_D1 + D3_UZ);
+    const double dvx = ld(A3_D1 + D3_VX), dvy = ld(A3_D1 + D3_VY), dvz = ld(A3_D1 + D3_VZ);
+    const double dwx = ld(A3_D1 + D3_WX), dwy = ld(A3_D1 + D3_WY), dwz = ld(A3_D1 + D3_WZ);
+    const double drx = ld(A3_D1 + D3_RX), dry = ld(A3_D1 + D3_RY), drz = ld(A3_D1 + D3_RZ);
+    const double dex = ld(A3_D1 + D3_EX), dey = ld(A3_D1 + D3_EY), dez = ld(A3_D1 + D3_EZ);
+    const double DPx = (g - 1.0) * (r * dex + drx * e);
+    const double DPy = (g - 1.0) * (r * dey + dry * e);
+    const double DPz = (g - 1.0) * (r * dez + drz * e);
+    const double vtx = ld(A3_D2 + S3_TXXX) + ld(A3_D2 + S3_TXYY) + ld(A3_D2 + S3_TXZZ);
+    const double vty = ld(A3_D2 + S3_TYYY) + ld(A3_D2 + S3_TXYX) + ld(A3_D2 + S3_TYZZ);
+    const double vtz = ld(A3_D2 + S3_TZZZ) + ld(A3_D2 + S3_TXZX) + ld(A3_D2 + S3_TYZY);
+    k[3] = -r * (dux + dvy + dwz) - drx * u - dry * v - drz * w;
+    k[0] = -(dux * u + duy * v + duz * w) + (vtx - DPx) / r;
+    k[1] = -(dvx * u + dvy * v + dvz * w) + (vty - DPy) / r;
+    k[2] = -(dwx * u + dwy * v + dwz * w) + (vtz - DPz) / r;
+}
+
+// dE of nseq.F90:318 at one point.  The stresses are recomputed from the gradients
+// (stress3d) rather than read back.
+template <typename Ld>
+__device__ __forceinline__ double assemble3d_energy(const Phys &ph, Ld ld)
+{
+    const double g = ph.gamma;
+    const double u = ld(A3_Q + 0), v = ld(A3_Q + 1), w = ld(A3_Q + 2), r = ld(A3_Q + 3), e = ld(A3_Q + 4);
+    const double dux = ld(A3_D1 + D3_UX), duy = ld(A3_D1 + D3_UY), duz = ld(A3_D1 + D3_UZ);
+    const double dvx = ld(A3_D1 + D3_VX), dvy = ld(A3_D1 + D3_VY), dvz = ld(A3_D1 + D3_VZ);
+    const double dwx = ld(A3_D1 + D3_WX), dwy = ld(A3_D1 + D3_WY), dwz = ld(A3_D1 + D3_WZ);
+    const double dex = ld(A3_D1 + D3_EX), dey = ld(A3_D1 + D3_EY), dez = ld(A3_D1 + D3_EZ);
+    const double P = (g - 1.0) * r * e;
+    const Stress3 t = stress3d(1.0 / ph.Re * sutherland_mu(ph, e), dux, duy, duz, dvx, dvy, dvz, dwx, dwy, dwz);
+    return -(dex * u + dey * v + dez * w)
+         + (-P * (dux + dvy + dwz) + t.xx * dux + t.yy * dvy
+            + t.zz * dwz + t.xy * (dvx + duy)
+            + t.xz * (dwx + duz) + t.yz * (dwy + dvz)
+            - ld(A3_D2 + S3_HTX) - ld(A3_D2 + S3_HTY) - ld(A3_D2 + S3_HTZ)) / r;
+}
+
+// All five: k[] in U, V, W, R, E order.
+template <typename Ld>
+__device__ __forceinline__ void assemble3d_rhs(const Phys &ph, Ld ld, double k[5])
+{
+    assemble3d_mom(ph, ld, k);
+    k[4] = assemble3d_energy(ph, ld);
+}
+
 // Assembly of dR, dU, dV, dW, dE (nseq.F90:310-318) fused with the RK4 stage update.
 // q: stage input; q0: step start; out: stage output (may alias q: pointwise in place).
-// The stresses are recomputed from the gradients (stress3d) rather than read back.
 __global__ void __launch_bounds__(256, 3) k_assemble3d(Phys ph, StateSet q, StateSet q0, StateSet out, FieldSet delta,
                                                        FieldSet d1, FieldSet d2, long long n, int mode,
                                                        const StepParams *sp)
 {
     const int b = blockIdx.y;
     const double dt = sp ? sp->dt : 0.0;
-    const double g = ph.gamma;
-    const double *U = q.v[0] + b * q.bstride, *V = q.v[1] + b * q.bstride, *W = q.v[2] + b * q.bstride;
-    const double *R = q.v[3] + b * q.bstride, *E = q.v[4] + b * q.bstride;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-        const double u = U[p], v = V[p], w = W[p], r = R[p], e = E[p];
-        const double dux = d1.f(b, D3_UX)[p], duy = d1.f(b, D3_UY)[p], duz = d1.f(b, D3_UZ)[p];
-        const double dvx = d1.f(b, D3_VX)[p], dvy = d1.f(b, D3_VY)[p], dvz = d1.f(b, D3_VZ)[p];
-        const double dwx = d1.f(b, D3_WX)[p], dwy = d1.f(b, D3_WY)[p], dwz = d1.f(b, D3_WZ)[p];
-        const double drx = d1.f(b, D3_RX)[p], dry = d1.f(b, D3_RY)[p], drz = d1.f(b, D3_RZ)[p];
-        const double dex = d1.f(b, D3_EX)[p], dey = d1.f(b, D3_EY)[p], dez = d1.f(b, D3_EZ)[p];
-        const double P = (g - 1.0) * r * e;
-        const double DPx = (g - 1.0) * (r * dex + drx * e);
-        const double DPy = (g - 1.0) * (r * dey + dry * e);
-        const double DPz = (g - 1.0) * (r * dez + drz * e);
-        const double vtx = d2.f(b, S3_TXXX)[p] + d2.f(b, S3_TXYY)[p] + d2.f(b, S3_TXZZ)[p];
-        const double vty = d2.f(b, S3_TYYY)[p] + d2.f(b, S3_TXYX)[p] + d2.f(b, S3_TYZZ)[p];
-        const double vtz = d2.f(b, S3_TZZZ)[p] + d2.f(b, S3_TXZX)[p] + d2.f(b, S3_TYZY)[p];
-        const double kR = -r * (dux + dvy + dwz) - drx * u - dry * v - drz * w;
-        const double kU = -(dux * u + duy * v + duz * w) + (vtx - DPx) / r;
-        const double kV = -(dvx * u + dvy * v + dvz * w) + (vty - DPy) / r;
-        const double kW = -(dwx * u + dwy * v + dwz * w) + (vtz - DPz) / r;
-        const Stress3 t = stress3d(1.0 / ph.Re * sutherland_mu(ph, e), dux, duy, duz, dvx, dvy, dvz, dwx, dwy, dwz);
-        const double kE = -(dex * u + dey * v + dez * w)
-                        + (-P * (dux + dvy + dwz) + t.xx * dux + t.yy * dvy
-                           + t.zz * dwz + t.xy * (dvx + duy)
-                           + t.xz * (dwx + duz) + t.yz * (dwy + dvz)
-                           - d2.f(b, S3_HTX)[p] - d2.f(b, S3_HTY)[p] - d2.f(b, S3_HTZ)[p]) / r;
-        const double k[5] = {kU, kV, kW, kR, kE};
+        auto ld = [&](int i) {
+            return i < A3_D1 ? q.v[i][b * q.bstride + p] : i < A3_D2 ? d1.f(b, i - A3_D1)[p] : d2.f(b, i - A3_D2)[p];
+        };
+        double k[5];
+        assemble3d_rhs(ph, ld, k);
 #pragma unroll
         for (int f = 0; f < 5; f++) {
             double *dl = delta.p ? delta.f(b, f) + p : nullptr;

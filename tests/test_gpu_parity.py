@@ -198,6 +198,31 @@ def test_batched_members_match_single_runs(libs):
     gb.close()
 
 
+@pytest.mark.parametrize("name", ["box", "cavity3d", "bl"])
+def test_assembly_paths_agree(libs, monkeypatch, name):
+    """The tensor-copy-fed assembly and the thread-load assembly (GATT_PW=plain, read when a
+    context is created) run the same arithmetic: the states after three steps (batch of two,
+    every RK stage mode) are equal bit for bit."""
+    from gatt_dns_b200.solver import GattDNS
+    c = get_case(name)
+    fa, fb = flow_for(c, seed=3), flow_for(c, seed=4)
+    dt = 0.2 * c.cfl_dt(fa["U"], fa["V"], fa["W"], 1.0)
+    out = {}
+    for mode in ("pipe", "plain"):
+        if mode == "plain":
+            monkeypatch.setenv("GATT_PW", "plain")
+        g = GattDNS(c, nbatch=2)
+        g.upload(fa, 0)
+        g.upload(fb, 1)
+        mc = g.run(3, 0.0, dt)
+        out[mode] = (mc, g.download(0), g.download(1))
+        g.close()
+    assert np.array_equal(out["pipe"][0], out["plain"][0])
+    for i in (1, 2):
+        for k in KEYS:
+            assert np.array_equal(out["pipe"][i][k], out["plain"][i][k]), (name, i, k)
+
+
 def test_full_size_box_one_step(libs):
     """128^3 periodic box: one step against the oracle, plus exact mass conservation."""
     from gatt_dns_b200.solver import GattDNS
