@@ -484,11 +484,33 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
     }
     if (nst == 0 || per_sm < 1) return GATT_ERR_STATE;
     a.nst = nst;
-    // 16-byte aligned field starts and line starts (bulk copies), even strides (tensor map)
+    // 16-byte aligned field starts, even strides (tensor maps)
     if ((reinterpret_cast<uintptr_t>(a.in) & 15) || (c->npts & 1) || (a.in_bstride & 1)) return GATT_ERR_STATE;
-    CUtensorMap map;
+    CUtensorMap map, omap;
     memset(&map, 0, sizeof(map));
-    if (!xd) {
+    memset(&omap, 0, sizeof(omap));
+    if (xd) {
+        // {row in chunk, line, chunk of 16 rows, field slot, member}, 128-byte swizzle: a box
+        // {16, 32, N/16} is one tile of 32 lines
+        if ((N & 15) || (reinterpret_cast<uintptr_t>(a.out) & 15) || (a.out_bstride & 1)) return GATT_ERR_STATE;
+        EncodeTiledFn enc = encode_tiled();
+        if (!enc) return GATT_ERR_STATE;
+        auto xmap = [&](CUtensorMap *mp, const double *base, const int *slots, long long bstride) {
+            int nslots = 1;
+            for (int f = 0; f < a.nf; f++) nslots = std::max(nslots, slots[f] + 1);
+            const long long mstride = nmembers > 1 ? bstride : (long long)nslots * c->npts;
+            cuuint64_t dims[5] = {16, (cuuint64_t)a.nlines, (cuuint64_t)(N / 16), (cuuint64_t)nslots,
+                                  (cuuint64_t)nmembers};
+            cuuint64_t strides[4] = {(cuuint64_t)N * 8, 128, (cuuint64_t)c->npts * 8, (cuuint64_t)mstride * 8};
+            cuuint32_t box[5] = {16, (cuuint32_t)kLanes, (cuuint32_t)(N / 16), 1, 1};
+            cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+            return enc(mp, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<double *>(base), dims, strides, box, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+        };
+        if (!xmap(&map, a.in, a.in_slot, a.in_bstride) || !xmap(&omap, a.out, a.out_slot, a.out_bstride))
+            return GATT_ERR_STATE;
+    } else {
         if (N > 256 || (c->nx & 1)) return GATT_ERR_STATE;
         EncodeTiledFn enc = encode_tiled();
         if (!enc) return GATT_ERR_STATE;
@@ -507,7 +529,7 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
         if (r != CUDA_SUCCESS) return GATT_ERR_STATE;
     }
     const int grid = std::min(a.njobs, per_sm * c->nsm);
-    void *args[] = {&a, &map};
+    void *args[] = {&a, &map, &omap};
     TRY(before_launch(c, cls));
     CU(cudaLaunchKernel(k, dim3(grid), dim3(32 * m.P), args, smem, c->stream));
     return after_launch(c);

@@ -36,15 +36,12 @@ constexpr unsigned long long kWaitNs = 1000000000ull;
 // Shared memory of k_psweep in bytes: nst ring stages, the block exchange, the coefficient
 // records of every line type (band rows [nTypes][N][Wp], records [nTypes][N][kQ]), the
 // mbarriers.
-__host__ __device__ __forceinline__ size_t psweep_stage_doubles(bool xd, int N)
-{
-    return xd ? (size_t)kLanes * (N + 2) : (size_t)N * kLanes;
-}
+__host__ __device__ __forceinline__ size_t psweep_stage_doubles(bool, int N) { return (size_t)N * kLanes; }
 __host__ __device__ __forceinline__ size_t psweep_smem_bytes(bool xd, int N, int P, int ntypes, int Wp, int nst)
 {
     return (nst * psweep_stage_doubles(xd, N) + 3 * (size_t)P * kLanes + (size_t)ntypes * N * (Wp + kQ)) *
                sizeof(double) +
-           nst * 8;
+           nst * 8 + (xd ? 1024 : 0);  // x: room to align the ring to the 1 KB swizzle period
 }
 
 // Coefficient load: read-only data path (global records) or plain (shared-memory copy).
@@ -109,6 +106,15 @@ __device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap *map
         " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(bar)
         : "memory");
+}
+
+// 5-D tiled tensor store shared -> global (bulk-group completion).
+__device__ __forceinline__ void tma_store_5d(const CUtensorMap *map, int c0, int c1, int c2, int c3, int c4, uint32_t src)
+{
+    asm volatile("cp.async.bulk.tensor.5d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4, %5}], [%6];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(src)
+                 : "memory");
 }
 
 // Contiguous global -> shared copy (16-byte aligned ends, size a multiple of 16).
@@ -342,24 +348,30 @@ __global__ void __launch_bounds__(32 * kMaxP) k_rsweep(const SweepArgs a)
 // ---- persistent CTAs, TMA-fed two-stage ring --------------------------------------------
 // Job j = tile + ntiles * (field + nf * member); CTA b takes jobs b, b + G, b + 2G, ...
 // y/z tiles: one tensor box {x: 32, line: N} of the 5-D map (x, y, z, field slot, member);
-// x tiles: one bulk copy per line into a [32][N+2] stage (the pad keeps 16-byte reads of
-// two rows conflict-free).
+// x tiles: one tensor box {16 rows, 32 lines, N/16 row chunks} of the map (row in chunk, line,
+// chunk, field slot, member) with the 128-byte swizzle -- it lands as [chunk][line][16 rows],
+// the 16-byte pairs of rows of line L XOR-permuted by L % 8, so that a warp's 16-byte reads of
+// its lines' row pairs are conflict-free -- and the solved tile leaves the same way through the
+// output map (one tensor store; 32 line copies each way were bound by the number of copies).
 // Register cap: the 768-thread bound holds a thread to 80 registers, which keeps three
 // 256-thread CTAs resident (84 registers round up to two); the y/z 6-band filter spills at
 // 80 and keeps the plain 512-thread bound.
 template <bool XD, bool PER, int NR, int RPB>
-__global__ void __launch_bounds__((NR == 6 && !XD) ? 32 * kMaxP : 768) k_psweep(const SweepArgs a, const __grid_constant__ CUtensorMap tmap)
+__global__ void __launch_bounds__((NR == 6 && !XD) ? 32 * kMaxP : 768) k_psweep(const SweepArgs a, const __grid_constant__ CUtensorMap tmap,
+                                                                     const __grid_constant__ CUtensorMap omap)
 {
     constexpr int H = NR - 1;
     constexpr int WP = (2 * NR - 1 + 3) / 4 * 4;
     constexpr int NW = RPB + 2 * H;
-    extern __shared__ __align__(128) double psm[];
+    extern __shared__ __align__(128) double psm_raw[];
     const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
     const int P = a.P;
     const int N = a.N;
     const int sp = p * RPB;
     const size_t stage_d = psweep_stage_doubles(XD, N);
     const int nst = a.nst;
+    // x: the swizzled ring starts on a 1 KB boundary (the host budgets the slack)
+    double *psm = XD ? psm_raw + ((1024u - (smem_u32(psm_raw) & 1023u)) & 1023u) / sizeof(double) : psm_raw;
     double *xs = psm + nst * stage_d;
     double *sRm = xs + 3 * P * kLanes;                   // coefficient copy, all line types
     double *sQ = sRm + (size_t)a.ntypes * N * WP;
@@ -380,18 +392,11 @@ __global__ void __launch_bounds__((NR == 6 && !XD) ? 32 * kMaxP : 768) k_psweep(
         const int tile = j % a.ntiles, fb = j / a.ntiles, f = fb % a.nf, b = fb / a.nf;
         const uint32_t bar = bar0 + 8 * s, dst = st0 + (uint32_t)(s * stage_d * sizeof(double));
         if (XD) {
-            if (threadIdx.x < kLanes) {
-                const int L0 = tile * kLanes;
-                const int nv = min(kLanes, a.nlines - L0);
-                bulk_wait_read0();  // this lane's store out of the stage has read it
+            if (threadIdx.x == 0) {
+                bulk_wait_read0();  // the tile stored out of this stage has been read
                 fence_proxy_async();
-                if (lane == 0) mbar_expect_tx(bar, (uint32_t)(nv * N * sizeof(double) + a.tx_extra));
-                __syncwarp();
-                if (lane < nv)
-                    bulk_g2s(dst + lane * (N + 2) * (uint32_t)sizeof(double),
-                             a.in + (long long)b * a.in_bstride + (long long)a.in_slot[f] * a.npts +
-                                 (long long)(L0 + lane) * N,
-                             (uint32_t)(N * sizeof(double)), bar);
+                mbar_expect_tx(bar, (uint32_t)(N * kLanes * sizeof(double) + a.tx_extra));
+                tma_load_5d(dst, &tmap, 0, tile * kLanes, 0, a.in_slot[f], b, bar);
             }
         } else if (threadIdx.x == 0) {
             fence_proxy_async();
@@ -429,13 +434,19 @@ __global__ void __launch_bounds__((NR == 6 && !XD) ? 32 * kMaxP : 768) k_psweep(
 
         // window rows from the stage
         double w[NW];
-        const double *ln = XD ? stg + lane * (N + 2) : stg + lane;
-        const int ls = XD ? 1 : kLanes;
-        auto lds = [&](int r) { return ln[r * ls]; };
+        // x: row r of this lane's line sits in chunk r/16, line row `lane`, 16-byte unit
+        // (r%16)/2 XOR (lane%8); y/z: row r at [r][lane]
+        auto xoff = [&](int r) {
+            return (((r >> 4) * kLanes + lane) << 4) + (((((r & 15) >> 1) ^ (lane & 7))) << 1) + (r & 1);
+        };
+        auto lds = [&](int r) { return XD ? stg[xoff(r)] : stg[r * kLanes + lane]; };
+        // x: the 16-byte unit of rows sp+2q, sp+2q+1 (sp is a multiple of 16: one chunk)
+        const int xrow = ((sp >> 4) * kLanes + lane) << 4;
+        auto xpair = [&](int q) { return xrow + ((q ^ (lane & 7)) << 1); };
         if (XD) {
 #pragma unroll
             for (int q = 0; q < RPB / 2; q++) {
-                const double2 v = *reinterpret_cast<const double2 *>(ln + sp + 2 * q);
+                const double2 v = *reinterpret_cast<const double2 *>(stg + xpair(q));
                 w[H + 2 * q] = v.x;
                 w[H + 2 * q + 1] = v.y;
             }
@@ -465,30 +476,25 @@ __global__ void __launch_bounds__((NR == 6 && !XD) ? 32 * kMaxP : 768) k_psweep(
 
         solve_block<PER, NR, RPB, false>(w, Rr, Qt, Qr, xs, lane, p, P);
         if (XD) {
-            // results back into the stage (its own line, rows sp..), then one contiguous bulk
-            // store per line: 1 KB copies instead of 32-byte pieces scattered over 32 lines
-            double *lw = const_cast<double *>(ln);
+            // results back into the stage (own rows, same swizzled places), then one tensor
+            // store of the tile (lines past the last one are clipped by the copy engine)
+            double *sw = const_cast<double *>(stg);
 #pragma unroll
             for (int q = 0; q < RPB / 2; q++) {
                 double2 v = make_double2(w[2 * q], w[2 * q + 1]);
                 if (blend_on) {
-                    const double2 o = *reinterpret_cast<const double2 *>(lw + sp + 2 * q);
+                    const double2 o = *reinterpret_cast<const double2 *>(sw + xpair(q));
                     v.x = o.x + blend * (v.x - o.x);
                     v.y = o.y + blend * (v.y - o.y);
                 }
-                *reinterpret_cast<double2 *>(lw + sp + 2 * q) = v;
+                *reinterpret_cast<double2 *>(sw + xpair(q)) = v;
             }
             fence_proxy_async();
             __syncthreads();
-            if (threadIdx.x < kLanes) {
-                const int L0 = tile * kLanes;
-                if (lane < min(kLanes, a.nlines - L0)) {
-                    bulk_s2g(a.out + (long long)b * a.out_bstride + (long long)a.out_slot[f] * a.npts +
-                                 (long long)(L0 + lane) * N,
-                             st0 + (uint32_t)((s * stage_d + lane * (N + 2)) * sizeof(double)),
-                             (uint32_t)(N * sizeof(double)));
-                    bulk_commit();
-                }
+            if (threadIdx.x == 0) {
+                tma_store_5d(&omap, 0, tile * kLanes, 0, a.out_slot[f], b,
+                             st0 + (uint32_t)(s * stage_d * sizeof(double)));
+                bulk_commit();
             }
             if (j + nst * G < a.njobs) issue(j + nst * G, s);
         } else {
