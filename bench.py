@@ -37,10 +37,11 @@ BYTES_PER_POINT_STAGE = 27 * 16 + 5 * 32 + 15 * 16 / 4
 # (stages 2-4; in stage 1 it is the stage input), RK increment read 5 (stages 2-4) and
 # written 5 (stages 1-3).  Stages 1..4: 42, 52, 52, 47 fields; mean 48.25.
 ASSEMBLE_FIELDS = (5 + 15 + 12 + 5) + 3 * (3 * 5) / 4.0
-# DRAM traffic of the assembly from ncu (profiles/k_assemble3d_periodic_box_128.md): a
-# stage-3 launch moved 876.3 MB (read + write) for 52 algorithmic fields of 128^3 points;
-# scaled to the four-stage mean by algorithmic fields, for n = 128 only.
-ASSEMBLE_TRAFFIC_STAGE3_128 = 876.3e6
+# DRAM traffic of the assembly from ncu (profiles/k_assemble3d_pipe_periodic_box_128.md): a
+# stage-3 launch moved 849.7 MB (read 704.7 + write 145.0; part of the output is still in L2
+# when it ends) for 52 algorithmic fields of 128^3 points (872.4 MB); scaled to the
+# four-stage mean by algorithmic fields, for n = 128 only.
+ASSEMBLE_TRAFFIC_STAGE3_128 = 849.7e6
 
 
 def parse():
@@ -53,6 +54,10 @@ def parse():
     p.add_argument("--no-clocks", action="store_true")
     p.add_argument("--no-arnoldi", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
+    # profiling runs: keep the default line-solve configuration (under a profiler the autotuner's
+    # timings are distorted) and leave out the CPU, Arnoldi, adjoint and other-case samples
+    p.add_argument("--no-autotune", action="store_true")
+    p.add_argument("--kernels-only", action="store_true")
     return p.parse_args()
 
 
@@ -394,7 +399,7 @@ def main():
     dt = c.cfl_dt(f["U"], f["V"], f["W"], 0.5)
     stream = torch.cuda.Stream()
     g = GattDNS(c, stream=stream.cuda_stream)
-    tuned = g.autotune(reps=3)  # line-solve family and row blocks per matrix set
+    tuned = {} if args.no_autotune else g.autotune(reps=3)  # line-solve family and row blocks per set
     npts = c.npts
 
     # pinned host buffers for the end-to-end leg
@@ -497,7 +502,7 @@ def main():
             "max_change_last": [float(x) for x in mc[0]]}
     if clocks:
         line["clocks"] = clocks
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.kernels_only:
         line["cpu_baseline"] = cpu_baseline_sample(c)
         if not args.no_arnoldi:
             g.close()
