@@ -482,6 +482,15 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
         const int r = resident_ctas(k, 32 * m.P, b);
         if (r > per_sm) { per_sm = r; nst = st; smem = b; }
     }
+    // x tiles hold their stage through the solve and the tensor store, so only a second stage
+    // lets the next tile load meanwhile: take the deepest ring that keeps two CTAs per SM
+    // (128^3: x sweeps 7-14 % faster at two CTAs and two stages than at three and one)
+    if (xd)
+        for (int st = kMaxStages; st > nst; st--) {
+            const size_t b = psweep_smem_bytes(xd, N, m.P, m.nTypes, m.Wp, st);
+            const int r = b <= kMaxSmem ? resident_ctas(k, 32 * m.P, b) : 0;
+            if (r >= 2) { per_sm = r; nst = st; smem = b; break; }
+        }
     if (nst == 0 || per_sm < 1) return GATT_ERR_STATE;
     a.nst = nst;
     // 16-byte aligned field starts, even strides (tensor maps)

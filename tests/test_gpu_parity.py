@@ -58,6 +58,12 @@ def get_case(name):
             _CASES[name] = cs.boundary_layer_cavity(nx=96, ny=48, buffers=((8, 6), (0, 8)))
         elif name == "long_x":
             _CASES[name] = cs.lid_driven(nxy=(900, 12))
+        elif name == "box_ragged":
+            # 5040 points: the last 256-point chunk of the tensor-copy assembly is partial
+            _CASES[name] = cs.periodic_box(nxyz=(20, 18, 14))
+        elif name == "box_odd":
+            # 5187 points (odd): the assembly takes the thread-load kernel
+            _CASES[name] = cs.periodic_box(nxyz=(21, 19, 13))
     return _CASES[name]
 
 
@@ -135,7 +141,7 @@ def test_filter_in_place(libs, name):
 
 
 @pytest.mark.parametrize("name", ["box", "box_aniso", "box64", "lid", "lid64", "lid_tanh", "cavity2d", "cavity3d",
-                                  "cavity3d_32", "bl", "bl_cavity"])
+                                  "cavity3d_32", "bl", "bl_cavity", "box_ragged", "box_odd"])
 def test_step(libs, name):
     c, g, o = pair(name)
     f = flow_for(c, seed=2)
@@ -198,7 +204,7 @@ def test_batched_members_match_single_runs(libs):
     gb.close()
 
 
-@pytest.mark.parametrize("name", ["box", "cavity3d", "bl"])
+@pytest.mark.parametrize("name", ["box", "cavity3d", "bl", "box_ragged"])
 def test_assembly_paths_agree(libs, monkeypatch, name):
     """The tensor-copy-fed assembly and the thread-load assembly (GATT_PW=plain, read when a
     context is created) run the same arithmetic: the states after three steps (batch of two,
