@@ -252,6 +252,72 @@ __device__ __forceinline__ LineRef line_of(const SweepArgs &a, int tile, int lan
     return r;
 }
 
+// Job j = tile + ntiles * (field + nf * member) of a persistent CTA, with the tile's outer
+// index o and x-tile tx (y/z: tile = o * tiles_per_row + tx).  A CTA advances its job by the
+// grid stride G; the stride is split the same way once, so that every later step is a few
+// adds and compares instead of run-time integer divisions (about twenty instructions each).
+struct JobCursor {
+    int tile, f, b, o, tx;
+};
+struct JobStride {
+    int gt, gf, gb, go, gx, nouter;
+};
+__device__ __forceinline__ JobCursor job_at(const SweepArgs &a, int j)
+{
+    JobCursor c;
+    c.tile = j % a.ntiles;
+    const int fb = j / a.ntiles;
+    c.f = fb % a.nf;
+    c.b = fb / a.nf;
+    c.o = c.tile / a.tiles_per_row;
+    c.tx = c.tile % a.tiles_per_row;
+    return c;
+}
+__device__ __forceinline__ JobStride job_stride(const SweepArgs &a, int G)
+{
+    JobStride s;
+    s.gt = G % a.ntiles;
+    const int q = G / a.ntiles;
+    s.gf = q % a.nf;
+    s.gb = q / a.nf;
+    s.go = s.gt / a.tiles_per_row;
+    s.gx = s.gt % a.tiles_per_row;
+    s.nouter = a.ntiles / a.tiles_per_row;
+    return s;
+}
+__device__ __forceinline__ void job_advance(JobCursor &c, const JobStride &s, const SweepArgs &a)
+{
+    c.tile += s.gt;
+    c.o += s.go;
+    c.tx += s.gx;
+    if (c.tx >= a.tiles_per_row) { c.tx -= a.tiles_per_row; c.o++; }
+    int carry = 0;
+    if (c.tile >= a.ntiles) { c.tile -= a.ntiles; c.o -= s.nouter; carry = 1; }
+    c.f += s.gf + carry;
+    c.b += s.gb;
+    if (c.f >= a.nf) { c.f -= a.nf; c.b++; }
+}
+
+// Line of a tile lane from a cursor (line_of without divisions).
+template <bool XD>
+__device__ __forceinline__ LineRef line_at(const SweepArgs &a, const JobCursor &c, int lane)
+{
+    LineRef r;
+    if (XD) {
+        r.L = c.tile * kLanes + lane;
+        r.valid = r.L < a.nlines;
+        r.base = (long long)r.L * a.N;
+        r.s = 1;
+    } else {
+        const int i = c.tx * kLanes + lane;
+        r.valid = i < a.nx;
+        r.base = i + (long long)c.o * a.os;
+        r.s = a.es;
+        r.L = i + a.nx * c.o;
+    }
+    return r;
+}
+
 // Store the solved block (optionally blended with the input values `orig(j)`).
 template <bool XD, int RPB, typename Orig>
 __device__ __forceinline__ void store_block(double *w, double *Gl, long long s, int sp, bool blend_on, double blend,
@@ -388,25 +454,24 @@ __global__ void __launch_bounds__((NR == 6 && !XD) ? 32 * kMaxP : 768) k_psweep(
     }
     __syncthreads();
 
-    auto issue = [&](int j, int s) {
-        const int tile = j % a.ntiles, fb = j / a.ntiles, f = fb % a.nf, b = fb / a.nf;
+    // thread 0: the copy of job c into stage s
+    auto issue = [&](const JobCursor &c, int s) {
         const uint32_t bar = bar0 + 8 * s, dst = st0 + (uint32_t)(s * stage_d * sizeof(double));
         if (XD) {
-            if (threadIdx.x == 0) {
-                bulk_wait_read0();  // the tile stored out of this stage has been read
-                fence_proxy_async();
-                mbar_expect_tx(bar, (uint32_t)(N * kLanes * sizeof(double) + a.tx_extra));
-                tma_load_5d(dst, &tmap, 0, tile * kLanes, 0, a.in_slot[f], b, bar);
-            }
-        } else if (threadIdx.x == 0) {
+            bulk_wait_read0();  // the tile stored out of this stage has been read
             fence_proxy_async();
             mbar_expect_tx(bar, (uint32_t)(N * kLanes * sizeof(double) + a.tx_extra));
-            const int o = tile / a.tiles_per_row, x0 = (tile % a.tiles_per_row) * kLanes;
-            tma_load_5d(dst, &tmap, x0, a.dir == 1 ? 0 : o, a.dir == 1 ? o : 0, a.in_slot[f], b, bar);
+            tma_load_5d(dst, &tmap, 0, c.tile * kLanes, 0, a.in_slot[c.f], c.b, bar);
+        } else {
+            fence_proxy_async();
+            mbar_expect_tx(bar, (uint32_t)(N * kLanes * sizeof(double) + a.tx_extra));
+            tma_load_5d(dst, &tmap, c.tx * kLanes, a.dir == 1 ? 0 : c.o, a.dir == 1 ? c.o : 0, a.in_slot[c.f], c.b,
+                        bar);
         }
     };
-    for (int s = 0; s < nst; s++)
-        if (blockIdx.x + s * G < a.njobs) issue(blockIdx.x + s * G, s);
+    if (threadIdx.x == 0)
+        for (int s = 0; s < nst; s++)
+            if (blockIdx.x + s * G < a.njobs) issue(job_at(a, blockIdx.x + s * G), s);
     // the coefficient records are read by every tile: copy them once while the first tiles land
     {
         const int nR2 = a.ntypes * N * WP / 2, nQ2 = a.ntypes * N * kQ / 2;
@@ -419,12 +484,27 @@ __global__ void __launch_bounds__((NR == 6 && !XD) ? 32 * kMaxP : 768) k_psweep(
 
     const bool blend_on = a.epi == EPI_BLEND;
     const double blend = blend_on ? sweep_blend(a) : 0.0;
-    int k = 0;
-    for (int j = blockIdx.x; j < a.njobs; j += G, k++) {
-        const int s = k % nst;
-        const uint32_t par = (uint32_t)(k / nst) & 1u;
-        const int tile = j % a.ntiles, fb = j / a.ntiles, f = fb % a.nf, b = fb / a.nf;
-        const LineRef lr = line_of<XD>(a, tile, lane);
+    // cursors of this job and of the job nst strides ahead (the next copy into this stage):
+    // advanced by adds where registers allow (x tiles, wide bands; measured 3-9 % faster
+    // there), recomputed by division in the y/z narrow-band solvers, which sit at the
+    // register cap and ran 5 % slower with two live cursors
+    constexpr bool kIncr = XD || NR >= 6;
+    const JobStride gs = job_stride(a, G);
+    JobCursor cur = job_at(a, blockIdx.x), ahead = job_at(a, min(blockIdx.x + nst * G, a.njobs));
+    int s = 0;
+    uint32_t par = 0;
+    for (int j = blockIdx.x; j < a.njobs; j += G, s = (s + 1 == nst) ? 0 : s + 1, par ^= (s == 0) ? 1u : 0u) {
+        if constexpr (kIncr) {
+            if (j != (int)blockIdx.x) {
+                job_advance(cur, gs, a);
+                job_advance(ahead, gs, a);
+            }
+        } else {
+            cur = job_at(a, j);
+            if (threadIdx.x == 0 && j + nst * G < a.njobs) ahead = job_at(a, j + nst * G);
+        }
+        const int tile = cur.tile, f = cur.f, b = cur.b;
+        const LineRef lr = line_at<XD>(a, cur, lane);
         const int t = lr.valid ? a.ltype[lr.L] : 0;
         const double *Qt = sQ + (size_t)t * N * kQ;
         const double *Rr = sRm + ((size_t)t * N + sp) * WP;
@@ -464,7 +544,8 @@ __global__ void __launch_bounds__((NR == 6 && !XD) ? 32 * kMaxP : 768) k_psweep(
             // give up: report, let the other stage's copy land (bounded), leave
             if (threadIdx.x == 0) {
                 *(volatile int *)a.err = 1;
-                if (nst > 1 && j + G < a.njobs) mbar_wait(bar0 + 8 * ((k + 1) % nst), (uint32_t)((k + 1) / nst) & 1u);
+                const int s1 = (s + 1 == nst) ? 0 : s + 1;
+                if (nst > 1 && j + G < a.njobs) mbar_wait(bar0 + 8 * s1, par ^ (s1 == 0 ? 1u : 0u));
             }
             if (XD && threadIdx.x < kLanes) bulk_wait0();  // stores already issued
             __syncthreads();
@@ -472,7 +553,7 @@ __global__ void __launch_bounds__((NR == 6 && !XD) ? 32 * kMaxP : 768) k_psweep(
         }
         // y/z: every warp has its rows, refill this stage now (blend keeps it for the epilogue);
         // x: the stage also carries the results out, it is refilled after the stores
-        if (!XD && !blend_on && j + nst * G < a.njobs) issue(j + nst * G, s);
+        if (!XD && !blend_on && threadIdx.x == 0 && j + nst * G < a.njobs) issue(ahead, s);
 
         solve_block<PER, NR, RPB, false>(w, Rr, Qt, Qr, xs, lane, p, P);
         if (XD) {
@@ -496,7 +577,7 @@ __global__ void __launch_bounds__((NR == 6 && !XD) ? 32 * kMaxP : 768) k_psweep(
                              st0 + (uint32_t)(s * stage_d * sizeof(double)));
                 bulk_commit();
             }
-            if (j + nst * G < a.njobs) issue(j + nst * G, s);
+            if (threadIdx.x == 0 && j + nst * G < a.njobs) issue(ahead, s);
         } else {
             if (lr.valid) {
                 double *Gl = a.out + (long long)b * a.out_bstride + (long long)a.out_slot[f] * a.npts + lr.base;
@@ -504,7 +585,7 @@ __global__ void __launch_bounds__((NR == 6 && !XD) ? 32 * kMaxP : 768) k_psweep(
             }
             if (blend_on) {
                 __syncthreads();
-                if (j + nst * G < a.njobs) issue(j + nst * G, s);
+                if (threadIdx.x == 0 && j + nst * G < a.njobs) issue(ahead, s);
             }
         }
     }
