@@ -5,11 +5,15 @@
 // The reference applies its lists strictly in order (Dirichlet U,V,W,E,P; Neumann
 // U,V,W,E,P; corners; null second derivative U,V,W,E,P; disturbances), and later
 // items read values earlier ones wrote.  The host flattens those lists into one
-// program of box operations (BcOp) in that order; one CTA per batch member executes
-// the program with a block barrier between dependent phases.  Boxes are boundary
-// planes, so the whole program touches a small fraction of the field.
+// program of box operations (BcOp) in that order.  A cluster of CTAs (up to 16 SMs) per batch
+// member executes the program, the points of each op spread over all its threads, with the
+// cluster barrier (release/acquire at cluster scope: every write of one op is visible to the
+// next) between ops; where a cluster cannot be launched, one CTA per member with block
+// barriers.  Boxes are boundary planes, so the whole program touches a small fraction of
+// the field, but on one SM it cost half of a boundary-layer step.
 #pragma once
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include "pointwise.cuh"
 
@@ -61,8 +65,9 @@ __device__ __forceinline__ long long bidx(const BcProgram &pg, int i, int j, int
 }
 
 // Extrapolate the face of box b along dir from the next len nodes (applyNeumann,
-// nseq.F90:552-599).  Threads stride over the face points.
-__device__ void neumann_face(const BcProgram &pg, double *u, const int *b, int dir, int len, const double *c)
+// nseq.F90:552-599).  Thread tid of nthr strides over the face points.
+__device__ void neumann_face(const BcProgram &pg, double *u, const int *b, int dir, int len, const double *c,
+                             int tid, int nthr)
 {
     int n1, n2;  // the two extents that span the face
     int a0, a1, c0, c1;
@@ -71,7 +76,7 @@ __device__ void neumann_face(const BcProgram &pg, double *u, const int *b, int d
     else { a0 = b[0]; a1 = b[1]; c0 = b[2]; c1 = b[3]; }
     n1 = a1 - a0 + 1; n2 = c1 - c0 + 1;
     const long long total = (long long)n1 * n2;
-    for (long long q = threadIdx.x; q < total; q += blockDim.x) {
+    for (long long q = tid; q < total; q += nthr) {
         const int a = a0 + (int)(q % n1), cc = c0 + (int)(q / n1);
         int i, j, k, di = 0, dj = 0, dk = 0;
         const bool lo = (dir & 1);               // odd dirs extrapolate at the low end
@@ -86,27 +91,23 @@ __device__ void neumann_face(const BcProgram &pg, double *u, const int *b, int d
     }
 }
 
-// One CTA per batch member.  F: the five state arrays of this member (U,V,W,R,E);
-// P: a scratch field of this member; x coordinates for disturbances in pg.xs.
-__global__ void k_bc(BcProgram pg, StateSet q, double *Pbase, long long pstride)
+// The program on one member: F the five state arrays (U,V,W,R,E), P a scratch field, thread
+// tid of nthr; sync() is a barrier over all nthr threads that orders their memory accesses.
+template <typename Sync>
+__device__ __forceinline__ void bc_run(const BcProgram &pg, double *const *F, double *P, int tid, int nthr, Sync sync)
 {
-    const int b = blockIdx.x;
-    double *F[5];
-#pragma unroll
-    for (int f = 0; f < 5; f++) F[f] = q.v[f] + b * q.bstride;
-    double *P = Pbase + b * pstride;
     double *Rr = F[3], *Ee = F[4];
     for (int o = 0; o < pg.nops; o++) {
         const BcOp op = pg.ops[o];
         if (op.code == OP_NEU || op.code == OP_P_NEU) {
             double *u = (op.code == OP_NEU) ? F[op.var] : P;
-            neumann_face(pg, u, op.box, op.dir, op.len, op.coef ? pg.coef2 : pg.coef1);
-            __syncthreads();
+            neumann_face(pg, u, op.box, op.dir, op.len, op.coef ? pg.coef2 : pg.coef1, tid, nthr);
+            sync();
             continue;
         }
         const int ni = op.box[1] - op.box[0] + 1, nj = op.box[3] - op.box[2] + 1, nk = op.box[5] - op.box[4] + 1;
         const long long total = (long long)ni * nj * nk;
-        for (long long q2 = threadIdx.x; q2 < total; q2 += blockDim.x) {
+        for (long long q2 = tid; q2 < total; q2 += nthr) {
             const int i = op.box[0] + (int)(q2 % ni);
             const int j = op.box[2] + (int)((q2 / ni) % nj);
             const int k = op.box[4] + (int)(q2 / ((long long)ni * nj));
@@ -136,8 +137,32 @@ __global__ void k_bc(BcProgram pg, StateSet q, double *Pbase, long long pstride)
             }
         }
         // every item may read what the previous one wrote
-        __syncthreads();
+        sync();
     }
+}
+
+// One CTA per batch member (block barriers).
+__global__ void k_bc(BcProgram pg, StateSet q, double *Pbase, long long pstride)
+{
+    const int b = blockIdx.x;
+    double *F[5];
+#pragma unroll
+    for (int f = 0; f < 5; f++) F[f] = q.v[f] + b * q.bstride;
+    bc_run(pg, F, Pbase + b * pstride, threadIdx.x, blockDim.x, [] { __syncthreads(); });
+}
+
+// One cluster of CTAs per batch member (cluster barriers); launched with a cluster dimension.
+__global__ void k_bc_cluster(BcProgram pg, StateSet q, double *Pbase, long long pstride)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int b = blockIdx.x / (int)cl.num_blocks();
+    double *F[5];
+#pragma unroll
+    for (int f = 0; f < 5; f++) F[f] = q.v[f] + b * q.bstride;
+    const int nthr = (int)cl.num_threads();
+    const int tid = (int)cl.block_rank() * blockDim.x + threadIdx.x;
+    bc_run(pg, F, Pbase + b * pstride, tid, nthr, [&] { cl.sync(); });
 }
 
 // ---- tangent-linear and adjoint of the program (no counterpart in the reference) -------
@@ -192,7 +217,7 @@ __global__ void k_bc_rec(BcProgram pg, StateSet q, double *Pbase, long long pstr
         const BcOp op = pg.ops[o];
         if (op.code == OP_NEU || op.code == OP_P_NEU) {
             double *u = (op.code == OP_NEU) ? F[op.var] : P;
-            neumann_face(pg, u, op.box, op.dir, op.len, op.coef ? pg.coef2 : pg.coef1);
+            neumann_face(pg, u, op.box, op.dir, op.len, op.coef ? pg.coef2 : pg.coef1, threadIdx.x, blockDim.x);
             __syncthreads();
             continue;
         }
@@ -245,8 +270,8 @@ __global__ void k_bc_tl(BcProgram pg, StateSet q, double *Pbase, StateSet dq, do
         const BcOp op = pg.ops[o];
         if (op.code == OP_NEU || op.code == OP_P_NEU) {
             const double *cf = op.coef ? pg.coef2 : pg.coef1;
-            neumann_face(pg, op.code == OP_NEU ? F[op.var] : P, op.box, op.dir, op.len, cf);
-            neumann_face(pg, op.code == OP_NEU ? dF[op.var] : dP, op.box, op.dir, op.len, cf);
+            neumann_face(pg, op.code == OP_NEU ? F[op.var] : P, op.box, op.dir, op.len, cf, threadIdx.x, blockDim.x);
+            neumann_face(pg, op.code == OP_NEU ? dF[op.var] : dP, op.box, op.dir, op.len, cf, threadIdx.x, blockDim.x);
             __syncthreads();
             continue;
         }

@@ -165,6 +165,7 @@ struct gatt_ctx {
     int *h_err = nullptr;   // pipeline wait give-up flag (pinned, device-mapped)
     int *d_err = nullptr;
     bool pw_pipe = true;    // 3-D assembly fed by bulk copies (GATT_PW=plain: thread loads)
+    int bc_cluster = 0;     // CTAs per member for the boundary program (0: one CTA, k_bc)
     // per-kernel-class timing (gatt_profile_kernels): events around every launch
     bool profiling = false;
     int prof_cls = -1;
@@ -903,6 +904,38 @@ void invalidate_graphs(gatt_ctx *c)
     }
 }
 
+// Cluster size for the boundary program: 16 CTAs (non-portable size) when the GPU can
+// schedule such a cluster of 512-thread CTAs, else 8, else 0 (one CTA per member).
+// GATT_BC_CLUSTER=0 selects the one-CTA kernel.  Host queries only: called at creation.
+int choose_bc_cluster(gatt_ctx *c)
+{
+    c->bc_cluster = 0;
+    const char *e = getenv("GATT_BC_CLUSTER");
+    if (e && !strcmp(e, "0")) return GATT_OK;
+    if (cudaFuncSetAttribute((const void *)k_bc_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+        cudaSuccess)
+        cudaGetLastError();
+    for (int cs : {16, 8}) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(cs);
+        cfg.blockDim = dim3(512);
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = cs;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, (const void *)k_bc_cluster, &cfg) == cudaSuccess && n >= 1) {
+            c->bc_cluster = cs;
+            return GATT_OK;
+        }
+        cudaGetLastError();
+    }
+    return GATT_OK;
+}
+
 int apply_bc(gatt_ctx *c, const StateSet &q, int nmem)
 {
     if (c->bc_dirty) TRY(build_bc_program(c));
@@ -911,7 +944,22 @@ int apply_bc(gatt_ctx *c, const StateSet &q, int nmem)
     pg.ops = c->d_ops; pg.nops = c->nops; pg.coef1 = c->d_coef1; pg.coef2 = c->d_coef2; pg.xs = c->d_xs;
     pg.gamma = c->ph.gamma; pg.nx = c->nx; pg.ny = c->ny; pg.nz = c->nz;
     TRY(before_launch(c, PC_BC));
-    k_bc<<<nmem, 512, 0, c->stream>>>(pg, q, c->P, c->npts);
+    if (c->bc_cluster > 0) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(nmem * c->bc_cluster);
+        cfg.blockDim = dim3(512);
+        cfg.stream = c->stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = c->bc_cluster;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        CU(cudaLaunchKernelEx(&cfg, k_bc_cluster, pg, q, c->P, (long long)c->npts));
+    } else {
+        k_bc<<<nmem, 512, 0, c->stream>>>(pg, q, c->P, c->npts);
+    }
     return after_launch(c);
 }
 
@@ -1786,6 +1834,7 @@ int gatt_create(gatt_ctx **out, int nx, int ny, int nz, int nbatch)
         if (ea != cudaSuccess) rc = fail(GATT_ERR_NOMEM, cudaGetErrorString(ea));
     }
     if (rc == GATT_OK) chk(set_sweep_attributes());
+    if (rc == GATT_OK) chk(choose_bc_cluster(c));
     if (rc == GATT_OK) chk(ensure_hist(c, 64));
     if (rc == GATT_OK) {
         cudaError_t es = cudaStreamSynchronize(c->stream);

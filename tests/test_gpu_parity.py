@@ -229,6 +229,29 @@ def test_assembly_paths_agree(libs, monkeypatch, name):
             assert np.array_equal(out["pipe"][i][k], out["plain"][i][k]), (name, i, k)
 
 
+@pytest.mark.parametrize("name", ["lid", "cavity3d", "bl", "bl_cavity"])
+def test_boundary_program_cluster_matches_single_cta(libs, monkeypatch, name):
+    """The boundary program run by a cluster of CTAs per member (cluster barriers between
+    ops) and by one CTA per member (GATT_BC_CLUSTER=0, read when a context is created) give
+    the same states after three steps, bit for bit."""
+    from gatt_dns_b200.solver import GattDNS
+    c = get_case(name)
+    f = flow_for(c, seed=6)
+    dt = 0.2 * c.cfl_dt(f["U"], f["V"], f["W"], 1.0)
+    out = {}
+    for mode in ("cluster", "cta"):
+        if mode == "cta":
+            monkeypatch.setenv("GATT_BC_CLUSTER", "0")
+        g = GattDNS(c)
+        g.upload(f)
+        mc = g.run(3, 0.0, dt)
+        out[mode] = (mc, g.download())
+        g.close()
+    assert np.array_equal(out["cluster"][0], out["cta"][0])
+    for k in KEYS:
+        assert np.array_equal(out["cluster"][1][k], out["cta"][1][k]), (name, k)
+
+
 def test_full_size_box_one_step(libs):
     """128^3 periodic box: one step against the oracle, plus exact mass conservation."""
     from gatt_dns_b200.solver import GattDNS
