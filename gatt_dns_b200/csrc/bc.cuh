@@ -7,9 +7,10 @@
 // items read values earlier ones wrote.  The host flattens those lists into one
 // program of box operations (BcOp) in that order.  A cluster of CTAs (up to 16 SMs) per batch
 // member executes the program, the points of each op spread over all its threads, with the
-// cluster barrier (release/acquire at cluster scope: every write of one op is visible to the
-// next) between ops; where a cluster cannot be launched, one CTA per member with block
-// barriers.  Boxes are boundary planes, so the whole program touches a small fraction of
+// cluster barrier (release/acquire at cluster scope: every write is visible after it) between
+// dependent ops; where a cluster cannot be launched, one CTA per member with block barriers.
+// Consecutive ops whose boxes and fields do not conflict form one phase without a barrier
+// (the host sets BcOp::sync on the last op of each phase).  Boxes are boundary planes, so the whole program touches a small fraction of
 // the field, but on one SM it cost half of a boundary-layer step.
 #pragma once
 
@@ -45,9 +46,12 @@ struct BcOp {
     int coef;       // 0 = neumannCoeffs, 1 = neumann2Coeffs
     int aux;        // divisor for corner averages
     int xoff;       // offset of the box's x coordinates (OP_LID)
+    int sync;       // barrier after this op (the next op depends on this op's phase)
     double val;
     long long tape; // adjoint tape: offset of this op's recorded base values (-1: none)
 };
+
+static_assert(sizeof(BcOp) % sizeof(long long) == 0, "ops are staged as 8-byte words");
 
 struct BcProgram {
     const BcOp *ops;
@@ -91,26 +95,35 @@ __device__ void neumann_face(const BcProgram &pg, double *u, const int *b, int d
     }
 }
 
+// Largest program whose ops are staged in shared memory (48 KB, no opt-in needed); longer
+// programs read their ops from global memory.
+constexpr int kBcStagedOps = 48 * 1024 / (int)sizeof(BcOp);
+
 // The program on one member: F the five state arrays (U,V,W,R,E), P a scratch field, thread
 // tid of nthr; sync() is a barrier over all nthr threads that orders their memory accesses.
+// sops: the ops copied to this CTA's shared memory (nullptr: read them from pg.ops).
 template <typename Sync>
-__device__ __forceinline__ void bc_run(const BcProgram &pg, double *const *F, double *P, int tid, int nthr, Sync sync)
+__device__ __forceinline__ void bc_run(const BcProgram &pg, const BcOp *sops, double *const *F, double *P, int tid,
+                                       int nthr, Sync sync)
 {
     double *Rr = F[3], *Ee = F[4];
+    const BcOp *ops = sops ? sops : pg.ops;
     for (int o = 0; o < pg.nops; o++) {
-        const BcOp op = pg.ops[o];
+        const BcOp op = ops[o];
         if (op.code == OP_NEU || op.code == OP_P_NEU) {
             double *u = (op.code == OP_NEU) ? F[op.var] : P;
             neumann_face(pg, u, op.box, op.dir, op.len, op.coef ? pg.coef2 : pg.coef1, tid, nthr);
-            sync();
+            if (op.sync) sync();
             continue;
         }
-        const int ni = op.box[1] - op.box[0] + 1, nj = op.box[3] - op.box[2] + 1, nk = op.box[5] - op.box[4] + 1;
-        const long long total = (long long)ni * nj * nk;
-        for (long long q2 = tid; q2 < total; q2 += nthr) {
-            const int i = op.box[0] + (int)(q2 % ni);
-            const int j = op.box[2] + (int)((q2 / ni) % nj);
-            const int k = op.box[4] + (int)(q2 / ((long long)ni * nj));
+        // 32-bit index arithmetic: a box holds fewer than 2^31 points (the grid does)
+        const unsigned ni = op.box[1] - op.box[0] + 1, nj = op.box[3] - op.box[2] + 1, nk = op.box[5] - op.box[4] + 1;
+        const unsigned nij = ni * nj, total = nij * nk;
+        for (unsigned q2 = tid; q2 < total; q2 += nthr) {
+            const unsigned kq = q2 / nij, r = q2 - kq * nij, jq = r / ni;
+            const int i = op.box[0] + (int)(r - jq * ni);
+            const int j = op.box[2] + (int)jq;
+            const int k = op.box[4] + (int)kq;
             const long long p = bidx(pg, i, j, k);
             switch (op.code) {
             case OP_SET: F[op.var][p] = op.val; break;
@@ -136,19 +149,33 @@ __device__ __forceinline__ void bc_run(const BcProgram &pg, double *const *F, do
             default: break;
             }
         }
-        // every item may read what the previous one wrote
-        sync();
+        // the next op reads or writes what this phase wrote (or writes what it read)
+        if (op.sync) sync();
     }
 }
 
-// One CTA per batch member (block barriers).
+// Copy the ops to shared memory (when they fit); every thread of the CTA calls it.
+__device__ __forceinline__ const BcOp *bc_stage_ops(const BcProgram &pg, BcOp *sops)
+{
+    if (pg.nops > kBcStagedOps) return nullptr;
+    const int n = pg.nops * (int)(sizeof(BcOp) / sizeof(long long));
+    const long long *g = reinterpret_cast<const long long *>(pg.ops);
+    long long *d = reinterpret_cast<long long *>(sops);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) d[i] = g[i];
+    __syncthreads();
+    return sops;
+}
+
+// One CTA per batch member (block barriers); dynamic shared memory: the staged ops.
 __global__ void k_bc(BcProgram pg, StateSet q, double *Pbase, long long pstride)
 {
+    extern __shared__ BcOp bc_sops[];
     const int b = blockIdx.x;
     double *F[5];
 #pragma unroll
     for (int f = 0; f < 5; f++) F[f] = q.v[f] + b * q.bstride;
-    bc_run(pg, F, Pbase + b * pstride, threadIdx.x, blockDim.x, [] { __syncthreads(); });
+    const BcOp *sops = bc_stage_ops(pg, bc_sops);
+    bc_run(pg, sops, F, Pbase + b * pstride, threadIdx.x, blockDim.x, [] { __syncthreads(); });
 }
 
 // One cluster of CTAs per batch member (cluster barriers); launched with a cluster dimension.
@@ -160,9 +187,11 @@ __global__ void k_bc_cluster(BcProgram pg, StateSet q, double *Pbase, long long 
     double *F[5];
 #pragma unroll
     for (int f = 0; f < 5; f++) F[f] = q.v[f] + b * q.bstride;
+    extern __shared__ BcOp bc_sops[];
     const int nthr = (int)cl.num_threads();
     const int tid = (int)cl.block_rank() * blockDim.x + threadIdx.x;
-    bc_run(pg, F, Pbase + b * pstride, tid, nthr, [&] { cl.sync(); });
+    const BcOp *sops = bc_stage_ops(pg, bc_sops);
+    bc_run(pg, sops, F, Pbase + b * pstride, tid, nthr, [&] { cl.sync(); });
 }
 
 // ---- tangent-linear and adjoint of the program (no counterpart in the reference) -------

@@ -861,6 +861,52 @@ int build_bc_program(gatt_ctx *c)
         TRY(check_box(c, d.ind));
         BcOp o = mk(OP_LID, d.var, d.ind); o.xoff = d.xoff; o.val = d.par; ops.push_back(o);
     }
+    // phases: an op joins the running phase unless it reads or writes a field point that an op
+    // of the phase writes, or writes one that it reads (fields U, V, W, R, E and the P scratch;
+    // boxes compared as index ranges, the Neumann ones over their extended box)
+    {
+        auto access = [](const BcOp &o, unsigned &rd, unsigned &wr) {
+            const unsigned U = 1u << o.var, R = 1u << 3, E = 1u << 4, P = 1u << 5;
+            rd = wr = 0;
+            switch (o.code) {
+            case OP_SET: case OP_LID: wr = U; break;
+            case OP_DIR_P: rd = E; wr = R; break;
+            case OP_NEU: rd = wr = U; break;
+            case OP_P_LOAD: rd = R | E; wr = P; break;
+            case OP_P_NEU: rd = wr = P; break;
+            case OP_R_FROM_P: rd = P | E; wr = R; break;
+            case OP_CORNER_E0: wr = E; break;
+            case OP_P_FROM_E: rd = E; wr = P; break;
+            case OP_E_ADD_P: rd = E | P; wr = E; break;
+            case OP_E_DIV: rd = wr = E; break;
+            case OP_R0: wr = R; break;
+            case OP_R_ADD_P: rd = R | P; wr = R; break;
+            case OP_R_DIV_E: rd = R | E; wr = R; break;
+            default: rd = wr = 0x3f; break;
+            }
+        };
+        auto overlap = [](const BcOp &a, const BcOp &b) {
+            for (int q = 0; q < 3; q++)
+                if (a.box[2 * q + 1] < b.box[2 * q] || b.box[2 * q + 1] < a.box[2 * q]) return false;
+            return true;
+        };
+        size_t start = 0;
+        for (size_t i = 0; i < ops.size(); i++) {
+            unsigned rb, wb;
+            access(ops[i], rb, wb);
+            bool dep = false;
+            for (size_t k = start; k < i && !dep; k++) {
+                unsigned ra, wa;
+                access(ops[k], ra, wa);
+                dep = ((wa & (rb | wb)) || (ra & wb)) && overlap(ops[k], ops[i]);
+            }
+            if (dep) {
+                ops[i - 1].sync = 1;
+                start = i;
+            }
+        }
+        if (!ops.empty()) ops.back().sync = 1;
+    }
     // adjoint tape offsets (base values of the nonlinear ops, per box point)
     long long tape = 0;
     for (BcOp &o : ops) {
@@ -943,11 +989,13 @@ int apply_bc(gatt_ctx *c, const StateSet &q, int nmem)
     BcProgram pg;
     pg.ops = c->d_ops; pg.nops = c->nops; pg.coef1 = c->d_coef1; pg.coef2 = c->d_coef2; pg.xs = c->d_xs;
     pg.gamma = c->ph.gamma; pg.nx = c->nx; pg.ny = c->ny; pg.nz = c->nz;
+    const size_t smem = c->nops <= kBcStagedOps ? (size_t)c->nops * sizeof(BcOp) : 0;  // staged ops
     TRY(before_launch(c, PC_BC));
     if (c->bc_cluster > 0) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(nmem * c->bc_cluster);
         cfg.blockDim = dim3(512);
+        cfg.dynamicSmemBytes = smem;
         cfg.stream = c->stream;
         cudaLaunchAttribute at[1];
         at[0].id = cudaLaunchAttributeClusterDimension;
@@ -958,7 +1006,7 @@ int apply_bc(gatt_ctx *c, const StateSet &q, int nmem)
         cfg.numAttrs = 1;
         CU(cudaLaunchKernelEx(&cfg, k_bc_cluster, pg, q, c->P, (long long)c->npts));
     } else {
-        k_bc<<<nmem, 512, 0, c->stream>>>(pg, q, c->P, c->npts);
+        k_bc<<<nmem, 512, smem, c->stream>>>(pg, q, c->P, c->npts);
     }
     return after_launch(c);
 }
