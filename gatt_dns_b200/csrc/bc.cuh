@@ -233,9 +233,11 @@ __device__ __forceinline__ void neumann_extent(const int *b, int dir, int &n1, i
 }
 
 // the forward program on the base, recording the tape (same arithmetic as k_bc)
-__global__ void k_bc_rec(BcProgram pg, StateSet q, double *Pbase, long long pstride, double *tape, long long tstride)
+template <typename Sync>
+// member b, thread tid of nthr, sync(): a barrier over the nthr threads
+__device__ __forceinline__ void k_bc_rec_run(int b, int tid, int nthr, Sync sync,
+    BcProgram pg, StateSet q, double *Pbase, long long pstride, double *tape, long long tstride)
 {
-    const int b = blockIdx.x;
     double *F[5];
 #pragma unroll
     for (int f = 0; f < 5; f++) F[f] = q.v[f] + b * q.bstride;
@@ -246,14 +248,14 @@ __global__ void k_bc_rec(BcProgram pg, StateSet q, double *Pbase, long long pstr
         const BcOp op = pg.ops[o];
         if (op.code == OP_NEU || op.code == OP_P_NEU) {
             double *u = (op.code == OP_NEU) ? F[op.var] : P;
-            neumann_face(pg, u, op.box, op.dir, op.len, op.coef ? pg.coef2 : pg.coef1, threadIdx.x, blockDim.x);
-            __syncthreads();
+            neumann_face(pg, u, op.box, op.dir, op.len, op.coef ? pg.coef2 : pg.coef1, tid, nthr);
+            sync();
             continue;
         }
         const int ni = op.box[1] - op.box[0] + 1, nj = op.box[3] - op.box[2] + 1, nk = op.box[5] - op.box[4] + 1;
         const long long total = (long long)ni * nj * nk;
         const int tw = bc_tape_width(op.code);
-        for (long long q2 = threadIdx.x; q2 < total; q2 += blockDim.x) {
+        for (long long q2 = tid; q2 < total; q2 += nthr) {
             const int i = op.box[0] + (int)(q2 % ni);
             const int j = op.box[2] + (int)((q2 / ni) % nj);
             const int k = op.box[4] + (int)(q2 / ((long long)ni * nj));
@@ -282,14 +284,31 @@ __global__ void k_bc_rec(BcProgram pg, StateSet q, double *Pbase, long long pstr
             default: break;
             }
         }
-        __syncthreads();
+        sync();
     }
 }
 
-// tangent: base q (updated as k_bc does) and tangent dq (P, dP scratch)
-__global__ void k_bc_tl(BcProgram pg, StateSet q, double *Pbase, StateSet dq, double *dPbase, long long pstride)
+__global__ void k_bc_rec(
+    BcProgram pg, StateSet q, double *Pbase, long long pstride, double *tape, long long tstride)
 {
-    const int b = blockIdx.x;
+    k_bc_rec_run(blockIdx.x, threadIdx.x, blockDim.x, [] { __syncthreads(); }, pg, q, Pbase, pstride, tape, tstride);
+}
+
+__global__ void k_bc_rec_cluster(
+    BcProgram pg, StateSet q, double *Pbase, long long pstride, double *tape, long long tstride)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    k_bc_rec_run(blockIdx.x / (int)cl.num_blocks(), (int)cl.block_rank() * blockDim.x + threadIdx.x, (int)cl.num_threads(),
+           [&] { cl.sync(); }, pg, q, Pbase, pstride, tape, tstride);
+}
+
+// tangent: base q (updated as k_bc does) and tangent dq (P, dP scratch)
+template <typename Sync>
+// member b, thread tid of nthr, sync(): a barrier over the nthr threads
+__device__ __forceinline__ void k_bc_tl_run(int b, int tid, int nthr, Sync sync,
+    BcProgram pg, StateSet q, double *Pbase, StateSet dq, double *dPbase, long long pstride)
+{
     double *F[5], *dF[5];
 #pragma unroll
     for (int f = 0; f < 5; f++) { F[f] = q.v[f] + b * q.bstride; dF[f] = dq.v[f] + b * dq.bstride; }
@@ -299,14 +318,14 @@ __global__ void k_bc_tl(BcProgram pg, StateSet q, double *Pbase, StateSet dq, do
         const BcOp op = pg.ops[o];
         if (op.code == OP_NEU || op.code == OP_P_NEU) {
             const double *cf = op.coef ? pg.coef2 : pg.coef1;
-            neumann_face(pg, op.code == OP_NEU ? F[op.var] : P, op.box, op.dir, op.len, cf, threadIdx.x, blockDim.x);
-            neumann_face(pg, op.code == OP_NEU ? dF[op.var] : dP, op.box, op.dir, op.len, cf, threadIdx.x, blockDim.x);
-            __syncthreads();
+            neumann_face(pg, op.code == OP_NEU ? F[op.var] : P, op.box, op.dir, op.len, cf, tid, nthr);
+            neumann_face(pg, op.code == OP_NEU ? dF[op.var] : dP, op.box, op.dir, op.len, cf, tid, nthr);
+            sync();
             continue;
         }
         const int ni = op.box[1] - op.box[0] + 1, nj = op.box[3] - op.box[2] + 1, nk = op.box[5] - op.box[4] + 1;
         const long long total = (long long)ni * nj * nk;
-        for (long long q2 = threadIdx.x; q2 < total; q2 += blockDim.x) {
+        for (long long q2 = tid; q2 < total; q2 += nthr) {
             const int i = op.box[0] + (int)(q2 % ni);
             const int j = op.box[2] + (int)((q2 / ni) % nj);
             const int k = op.box[4] + (int)(q2 / ((long long)ni * nj));
@@ -350,17 +369,33 @@ __global__ void k_bc_tl(BcProgram pg, StateSet q, double *Pbase, StateSet dq, do
             default: break;
             }
         }
-        __syncthreads();
+        sync();
     }
 }
 
+__global__ void k_bc_tl(
+    BcProgram pg, StateSet q, double *Pbase, StateSet dq, double *dPbase, long long pstride)
+{
+    k_bc_tl_run(blockIdx.x, threadIdx.x, blockDim.x, [] { __syncthreads(); }, pg, q, Pbase, dq, dPbase, pstride);
+}
+
+__global__ void k_bc_tl_cluster(
+    BcProgram pg, StateSet q, double *Pbase, StateSet dq, double *dPbase, long long pstride)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    k_bc_tl_run(blockIdx.x / (int)cl.num_blocks(), (int)cl.block_rank() * blockDim.x + threadIdx.x, (int)cl.num_threads(),
+           [&] { cl.sync(); }, pg, q, Pbase, dq, dPbase, pstride);
+}
+
 // adjoint of a Neumann face: g = lam[face]; lam[face] = 0; lam[face + m s] += c_{m-1} g
-__device__ void neumann_face_adj(const BcProgram &pg, double *lam, const int *b, int dir, int len, const double *c)
+__device__ void neumann_face_adj(const BcProgram &pg, double *lam, const int *b, int dir, int len, const double *c,
+                                 int tid, int nthr)
 {
     int n1, n2;
     neumann_extent(b, dir, n1, n2);
     const long long total = (long long)n1 * n2;
-    for (long long q = threadIdx.x; q < total; q += blockDim.x) {
+    for (long long q = tid; q < total; q += nthr) {
         int i, j, k, di, dj, dk;
         neumann_geom(b, dir, len, q, n1, i, j, k, di, dj, dk);
         const long long pf = bidx(pg, i, j, k);
@@ -371,10 +406,11 @@ __device__ void neumann_face_adj(const BcProgram &pg, double *lam, const int *b,
 }
 
 // adjoint: lam (the five variables) and lP (the scratch's lambda, zero on entry), ops in reverse
-__global__ void k_bc_adj(BcProgram pg, StateSet lam, double *lPbase, long long pstride, const double *tape,
-                         long long tstride)
+template <typename Sync>
+// member b, thread tid of nthr, sync(): a barrier over the nthr threads
+__device__ __forceinline__ void k_bc_adj_run(int b, int tid, int nthr, Sync sync,
+    BcProgram pg, StateSet lam, double *lPbase, long long pstride, const double *tape, long long tstride)
 {
-    const int b = blockIdx.x;
     double *L[5];
 #pragma unroll
     for (int f = 0; f < 5; f++) L[f] = lam.v[f] + b * lam.bstride;
@@ -385,14 +421,14 @@ __global__ void k_bc_adj(BcProgram pg, StateSet lam, double *lPbase, long long p
         const BcOp op = pg.ops[o];
         if (op.code == OP_NEU || op.code == OP_P_NEU) {
             neumann_face_adj(pg, op.code == OP_NEU ? L[op.var] : lP, op.box, op.dir, op.len,
-                             op.coef ? pg.coef2 : pg.coef1);
-            __syncthreads();
+                             op.coef ? pg.coef2 : pg.coef1, tid, nthr);
+            sync();
             continue;
         }
         const int ni = op.box[1] - op.box[0] + 1, nj = op.box[3] - op.box[2] + 1, nk = op.box[5] - op.box[4] + 1;
         const long long total = (long long)ni * nj * nk;
         const int tw = bc_tape_width(op.code);
-        for (long long q2 = threadIdx.x; q2 < total; q2 += blockDim.x) {
+        for (long long q2 = tid; q2 < total; q2 += nthr) {
             const int i = op.box[0] + (int)(q2 % ni);
             const int j = op.box[2] + (int)((q2 / ni) % nj);
             const int k = op.box[4] + (int)(q2 / ((long long)ni * nj));
@@ -430,8 +466,23 @@ __global__ void k_bc_adj(BcProgram pg, StateSet lam, double *lPbase, long long p
             default: break;
             }
         }
-        __syncthreads();
+        sync();
     }
+}
+
+__global__ void k_bc_adj(
+    BcProgram pg, StateSet lam, double *lPbase, long long pstride, const double *tape, long long tstride)
+{
+    k_bc_adj_run(blockIdx.x, threadIdx.x, blockDim.x, [] { __syncthreads(); }, pg, lam, lPbase, pstride, tape, tstride);
+}
+
+__global__ void k_bc_adj_cluster(
+    BcProgram pg, StateSet lam, double *lPbase, long long pstride, const double *tape, long long tstride)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    k_bc_adj_run(blockIdx.x / (int)cl.num_blocks(), (int)cl.block_rank() * blockDim.x + threadIdx.x, (int)cl.num_threads(),
+           [&] { cl.sync(); }, pg, lam, lPbase, pstride, tape, tstride);
 }
 
 }  // namespace gatt

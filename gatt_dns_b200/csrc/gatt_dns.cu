@@ -166,6 +166,8 @@ struct gatt_ctx {
     int *d_err = nullptr;
     bool pw_pipe = true;    // 3-D assembly fed by bulk copies (GATT_PW=plain: thread loads)
     int bc_cluster = 0;     // CTAs per member for the boundary program (0: one CTA, k_bc)
+    int bc_cluster_rec = 0, bc_cluster_tl = 0, bc_cluster_adj = 0;  // same, tape / tangent / adjoint
+    long long bc_points = 0;  // point updates of one application of the program (sum over ops)
     // per-kernel-class timing (gatt_profile_kernels): events around every launch
     bool profiling = false;
     int prof_cls = -1;
@@ -916,6 +918,12 @@ int build_bc_program(gatt_ctx *c)
             tape += (long long)tw * (o.box[1] - o.box[0] + 1) * (o.box[3] - o.box[2] + 1) * (o.box[5] - o.box[4] + 1);
     }
     c->tape_len = tape;
+    c->bc_points = 0;
+    for (const BcOp &o : ops) {
+        const long long ni = o.box[1] - o.box[0] + 1, nj = o.box[3] - o.box[2] + 1, nk = o.box[5] - o.box[4] + 1;
+        c->bc_points += (o.code == OP_NEU || o.code == OP_P_NEU) ? (o.dir <= 2 ? nj * nk : o.dir <= 4 ? ni * nk : ni * nj)
+                                                                 : ni * nj * nk;
+    }
     cudaFree(c->d_ops); c->d_ops = nullptr;
     cudaFree(c->d_coef1); c->d_coef1 = nullptr;
     cudaFree(c->d_coef2); c->d_coef2 = nullptr;
@@ -950,21 +958,16 @@ void invalidate_graphs(gatt_ctx *c)
     }
 }
 
-// Cluster size for the boundary program: 16 CTAs (non-portable size) when the GPU can
+// Cluster size for a boundary-program kernel: 16 CTAs (non-portable size) when the GPU can
 // schedule such a cluster of 512-thread CTAs, else 8, else 0 (one CTA per member).
-// GATT_BC_CLUSTER=0 selects the one-CTA kernel.  Host queries only: called at creation.
-int choose_bc_cluster(gatt_ctx *c)
+int bc_cluster_size(const void *k)
 {
-    c->bc_cluster = 0;
-    const char *e = getenv("GATT_BC_CLUSTER");
-    if (e && !strcmp(e, "0")) return GATT_OK;
-    if (cudaFuncSetAttribute((const void *)k_bc_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
-        cudaSuccess)
-        cudaGetLastError();
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) cudaGetLastError();
     for (int cs : {16, 8}) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(cs);
         cfg.blockDim = dim3(512);
+        cfg.dynamicSmemBytes = 48 * 1024;  // the staged ops, at most
         cudaLaunchAttribute at[1];
         at[0].id = cudaLaunchAttributeClusterDimension;
         at[0].val.clusterDim.x = cs;
@@ -973,11 +976,55 @@ int choose_bc_cluster(gatt_ctx *c)
         cfg.attrs = at;
         cfg.numAttrs = 1;
         int n = 0;
-        if (cudaOccupancyMaxActiveClusters(&n, (const void *)k_bc_cluster, &cfg) == cudaSuccess && n >= 1) {
-            c->bc_cluster = cs;
-            return GATT_OK;
-        }
+        if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) == cudaSuccess && n >= 1) return cs;
         cudaGetLastError();
+    }
+    return 0;
+}
+
+// Cluster sizes of the boundary-program kernels (GATT_BC_CLUSTER=0: one CTA per member).
+// Host queries only: called at creation.
+int choose_bc_cluster(gatt_ctx *c)
+{
+    c->bc_cluster = c->bc_cluster_rec = c->bc_cluster_tl = c->bc_cluster_adj = 0;
+    const char *e = getenv("GATT_BC_CLUSTER");
+    if (e && !strcmp(e, "0")) return GATT_OK;
+    c->bc_cluster = bc_cluster_size((const void *)k_bc_cluster);
+    c->bc_cluster_rec = bc_cluster_size((const void *)k_bc_rec_cluster);
+    c->bc_cluster_tl = bc_cluster_size((const void *)k_bc_tl_cluster);
+    c->bc_cluster_adj = bc_cluster_size((const void *)k_bc_adj_cluster);
+    return GATT_OK;
+}
+
+// Launch a boundary-program kernel for nmem members: the cluster form with cs CTAs per
+// member, cs the largest power of two up to the schedulable size cs_max that keeps the
+// clusters of all members within the SMs and gives every CTA about 2048 point updates (small
+// or many-member programs gain nothing from more CTAs and pay a barrier per op); with cs < 2
+// the one-CTA form.
+template <typename... KArgs, typename... Args>
+int launch_bc(gatt_ctx *c, void (*kblock)(KArgs...), void (*kcluster)(KArgs...), int cs_max, int nmem, size_t smem,
+              Args &&...args)
+{
+    const long long by_work = (c->bc_points + 2047) / 2048;
+    const long long by_sms = std::max(1, c->nsm / std::max(1, nmem));
+    int cs = 1;
+    while (cs * 2 <= cs_max && cs * 2 <= by_work && cs * 2 <= by_sms) cs *= 2;
+    if (cs >= 2) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(nmem * cs);
+        cfg.blockDim = dim3(512);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = c->stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = cs;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        CU(cudaLaunchKernelEx(&cfg, kcluster, std::forward<Args>(args)...));
+    } else {
+        kblock<<<nmem, 512, smem, c->stream>>>(std::forward<Args>(args)...);
     }
     return GATT_OK;
 }
@@ -991,23 +1038,7 @@ int apply_bc(gatt_ctx *c, const StateSet &q, int nmem)
     pg.gamma = c->ph.gamma; pg.nx = c->nx; pg.ny = c->ny; pg.nz = c->nz;
     const size_t smem = c->nops <= kBcStagedOps ? (size_t)c->nops * sizeof(BcOp) : 0;  // staged ops
     TRY(before_launch(c, PC_BC));
-    if (c->bc_cluster > 0) {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(nmem * c->bc_cluster);
-        cfg.blockDim = dim3(512);
-        cfg.dynamicSmemBytes = smem;
-        cfg.stream = c->stream;
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeClusterDimension;
-        at[0].val.clusterDim.x = c->bc_cluster;
-        at[0].val.clusterDim.y = 1;
-        at[0].val.clusterDim.z = 1;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
-        CU(cudaLaunchKernelEx(&cfg, k_bc_cluster, pg, q, c->P, (long long)c->npts));
-    } else {
-        k_bc<<<nmem, 512, smem, c->stream>>>(pg, q, c->P, c->npts);
-    }
+    TRY(launch_bc(c, k_bc, k_bc_cluster, c->bc_cluster, nmem, smem, pg, q, c->P, (long long)c->npts));
     return after_launch(c);
 }
 
@@ -1435,7 +1466,8 @@ int bc_tl(gatt_ctx *c, const StateSet &x, const StateSet &y)
 {
     if (c->nops == 0) return GATT_OK;
     TRY(before_launch(c, PC_BC));
-    k_bc_tl<<<c->nb, 512, 0, c->stream>>>(bc_program(c), x, c->P, y, c->t_P, c->npts);
+    TRY(launch_bc(c, k_bc_tl, k_bc_tl_cluster, c->bc_cluster_tl, c->nb, 0, bc_program(c), x, c->P, y, c->t_P,
+                  (long long)c->npts));
     return after_launch(c);
 }
 
@@ -1445,7 +1477,8 @@ int bc_rec(gatt_ctx *c, const StateSet &x, int which)
     if (c->nops == 0) return GATT_OK;
     const long long ts = std::max(1LL, c->tape_len);
     TRY(before_launch(c, PC_BC));
-    k_bc_rec<<<c->nb, 512, 0, c->stream>>>(bc_program(c), x, c->P, c->npts, c->a_tape + which * ts * c->nb, ts);
+    TRY(launch_bc(c, k_bc_rec, k_bc_rec_cluster, c->bc_cluster_rec, c->nb, 0, bc_program(c), x, c->P,
+                  (long long)c->npts, c->a_tape + which * ts * c->nb, ts));
     return after_launch(c);
 }
 
@@ -1456,7 +1489,8 @@ int bc_adj(gatt_ctx *c, const StateSet &lam, int which)
     const long long ts = std::max(1LL, c->tape_len);
     CU(cudaMemsetAsync(c->a_lP, 0, sizeof(double) * (size_t)c->npts * c->nb, c->stream));
     TRY(before_launch(c, PC_BC));
-    k_bc_adj<<<c->nb, 512, 0, c->stream>>>(bc_program(c), lam, c->a_lP, c->npts, c->a_tape + which * ts * c->nb, ts);
+    TRY(launch_bc(c, k_bc_adj, k_bc_adj_cluster, c->bc_cluster_adj, c->nb, 0, bc_program(c), lam, c->a_lP,
+                  (long long)c->npts, (const double *)(c->a_tape + which * ts * c->nb), ts));
     return after_launch(c);
 }
 
