@@ -63,6 +63,8 @@ constexpr int kMatKinds = 6;
 struct DevDir {
     bool set = false;
     int periodic = 0, nR = 0, nTypes = 0, N = 0, W = 0, Wp = 0, P = 1;
+    int Np = 0;            // line length the pipelined solver runs: N, or N padded to 16 rows
+    int rows = 0;          // rows of the kernel records uploaded (N, or Np for the padded solver)
     int rpb = 0;           // rows per block of the register-resident solver (0: shared-tile solver)
     int family = 0;        // SweepFamily
     // the factors as given, repacked [type][row] ([type][row][diag] for R): kept to rebuild
@@ -359,14 +361,31 @@ int choose_family()
     return FAM_PIPE;
 }
 
-// Block height of the register-resident solvers for lines of N rows and band nR, or 0 when
-// the shared-tile solver handles them (N not a multiple of kRPB, more than kMaxP blocks, or a
-// band wider than kMaxNRreg).
-int choose_rpb(int N, int nR)
+// Padded line length for the pipelined solver: non-cyclic y/z lines whose length is not a
+// multiple of kRPB run as lines of the next multiple, the extra rows identity rows (A = C = 0,
+// reciprocal pivot 1, zero band) that the tile copy fills with zeros past the grid edge and
+// the store skips; the real rows' results are those of the unpadded line (the last real row
+// has no super-diagonal, the first padded one no sub-diagonal).  Returns N when that does not
+// apply (cyclic or x lines, lines past one tensor box of 256 rows, layouts the tensor map
+// cannot describe).
+int padded_rows(const gatt_ctx *c, int d, int N, int nR, int periodic)
+{
+    if (N % kRPB == 0 || periodic || d == 0 || nR < 2 || nR > kMaxNRreg) return N;
+    const int np = (N + kRPB - 1) / kRPB * kRPB;
+    if (np / kRPB > kMaxP || np > 256 || (c->nx & 1) || (c->npts & 1)) return N;
+    return np;
+}
+
+// Block height of the register-resident solvers for lines of Np rows (Np: N or its padded
+// length) and band nR, or 0 when the shared-tile solver handles them (length not a multiple of
+// kRPB, more than kMaxP blocks, or a band wider than kMaxNRreg).  Padded lines need the
+// pipelined solver (the only one that zero-fills past the grid edge).
+int choose_rpb(int N, int Np, int nR)
 {
     if (choose_family() == FAM_TILE) return 0;
     if (nR < 2 || nR > kMaxNRreg) return 0;
-    return (N % kRPB == 0 && N / kRPB <= kMaxP) ? kRPB : 0;
+    if (Np != N && choose_family() != FAM_PIPE) return 0;
+    return (Np % kRPB == 0 && Np / kRPB <= kMaxP) ? kRPB : 0;
 }
 
 size_t sweep_smem(int N, int P, int nR, int Wp, bool stage = true)
@@ -419,27 +438,33 @@ int set_sweep_attributes()
 // Kernel row records (sweep.cuh) of a matrix set for a partition into P row blocks: the
 // reference's factors in uniform row semantics plus the block propagators of the partitioned
 // recurrences (long double products).  Allocates the device arrays on first use.
-int upload_records(gatt_ctx *c, DevDir &m, int P)
+int upload_records(gatt_ctx *c, DevDir &m, int P, int rows = 0)
 {
-    const int N = m.N, W = m.W, Wp = m.Wp, nTypes = m.nTypes;
+    const int N0 = m.N, W = m.W, Wp = m.Wp, nTypes = m.nTypes;
+    const int N = rows > 0 ? rows : N0;  // records for N rows: rows past N0 are identity rows
     const bool periodic = m.periodic != 0;
+    if (N != N0 && periodic) return fail(GATT_ERR_STATE, "cyclic lines cannot be padded");
     std::vector<double> hRm((size_t)nTypes * N * Wp, 0.0), hQ((size_t)nTypes * N * kQ, 0.0);
     for (int t = 0; t < nTypes; t++) {
-        const double *tA = &m.hA[(size_t)t * N], *tB = &m.hB[(size_t)t * N], *tC = &m.hC[(size_t)t * N];
+        const double *tA = &m.hA[(size_t)t * N0], *tB = &m.hB[(size_t)t * N0], *tC = &m.hC[(size_t)t * N0];
         double *q = &hQ[(size_t)t * N * kQ];
         for (int r = 0; r < N; r++) {
             double *qr = q + (size_t)r * kQ;
+            if (r >= N0) {  // padding: x = 0 whatever comes before or after
+                qr[kQfB] = 1.0;
+                continue;
+            }
             if (!periodic) {
                 qr[kQfA] = r > 0 ? tA[r - 1] : 0.0;       // derivs.F90:607
                 qr[kQfB] = tB[r];
-                qr[kQbC] = r < N - 1 ? tC[r] : 0.0;       // derivs.F90:610
+                qr[kQbC] = r < N0 - 1 ? tC[r] : 0.0;      // derivs.F90:610
             } else {
                 qr[kQfA] = r >= 2 ? tA[r - 1] : 0.0;      // derivs.F90:798
                 qr[kQfB] = r >= 1 ? tB[r - 1] : 0.0;      // derivs.F90:796-798
                 qr[kQbC] = (r >= 1 && r <= N - 2) ? tC[r] : 0.0;  // derivs.F90:801
                 qr[kQD] = m.hD[(size_t)t * N + r];        // derivs.F90:786-789
             }
-            for (int k = 0; k < W; k++) hRm[((size_t)t * N + r) * Wp + k] = m.hR[((size_t)t * N + r) * W + k];
+            for (int k = 0; k < W; k++) hRm[((size_t)t * N + r) * Wp + k] = m.hR[((size_t)t * N0 + r) * W + k];
         }
         if (periodic) { q[kQcA] = tA[0]; q[kQcC] = tC[0]; }  // derivs.F90:792-793
         for (int p = 0; p < P; p++) {
@@ -463,6 +488,7 @@ int upload_records(gatt_ctx *c, DevDir &m, int P)
     CU(cudaMemcpy(m.Rm, hRm.data(), hRm.size() * sizeof(double), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(m.Q, hQ.data(), hQ.size() * sizeof(double), cudaMemcpyHostToDevice));
     m.P = P;
+    m.rows = N;
     return GATT_OK;
 }
 
@@ -471,7 +497,7 @@ int upload_records(gatt_ctx *c, DevDir &m, int P)
 // alignment rules, so that the caller falls back to k_rsweep.
 int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmembers, int cls)
 {
-    const int N = m.N;
+    const int N = m.rows;  // padded y/z lines: the box covers the padding (zero fill)
     const bool xd = d == 0;
     void *k = reg_kernel(true, xd, m.periodic != 0, m.nR);
     if (!k) return GATT_ERR_STATE;
@@ -563,7 +589,7 @@ int sweep(gatt_ctx *c, int d, int kind, const double *in, long long in_bs, const
     a.in = in; a.out = out; a.in_bstride = in_bs; a.out_bstride = out_bs; a.npts = c->npts;
     for (int f = 0; f < nf; f++) { a.in_slot[f] = in_slots[f]; a.out_slot[f] = out_slots[f]; }
     a.nx = c->nx; a.ny = c->ny; a.nz = c->nz;
-    a.N = m.N; a.nlines = nlines(c, d);
+    a.N = m.rows; a.Nreal = m.N; a.nlines = nlines(c, d);
     a.es = d == 1 ? c->nx : (long long)c->nx * c->ny;
     a.os = d == 1 ? (long long)c->nx * c->ny : c->nx;
     a.tiles_per_row = (c->nx + kLanes - 1) / kLanes;
@@ -580,6 +606,8 @@ int sweep(gatt_ctx *c, int d, int kind, const double *in, long long in_bs, const
     if (m.family == FAM_PIPE && m.rpb) {
         int r = launch_psweep(c, m, d, a, nmembers, cls);
         if (r != GATT_ERR_STATE) return r;  // GATT_ERR_STATE: layout not expressible, use k_rsweep
+        // padded lines: only the pipelined solver zero-fills past the grid edge
+        if (m.rows != m.N) return fail(GATT_ERR_STATE, "padded lines need the pipelined solver (layout refused)");
     }
     a.stage = !m.rpb && sweep_smem(m.N, m.P, m.nR, m.Wp, true) <= kMaxSmem;
     const size_t smem = m.rpb ? (size_t)3 * m.P * kLanes * sizeof(double) : sweep_smem(m.N, m.P, m.nR, m.Wp, a.stage);
@@ -1779,6 +1807,8 @@ std::vector<TuneCand> tune_candidates(const DevDir &m)
     if (m.N % kRPB == 0 && m.N / kRPB <= kMaxP && m.nR >= 2 && m.nR <= kMaxNRreg) {
         out.push_back({FAM_PIPE, kRPB, m.N / kRPB});
         out.push_back({FAM_REG, kRPB, m.N / kRPB});
+    } else if (m.Np > m.N) {
+        out.push_back({FAM_PIPE, kRPB, m.Np / kRPB});  // padded lines: the pipelined solver only
     }
     for (int rows : {8, 16, 32, 64}) {
         const int P = choose_blocks(m.N, m.nR, m.Wp, rows);
@@ -1817,7 +1847,7 @@ int autotune(gatt_ctx *c, int reps, int *family, int *blocks, double *us)
             float best_ms = -1.0f;
             for (const TuneCand &t : tune_candidates(m)) {
                 m.family = t.family; m.rpb = t.rpb;
-                rc = upload_records(c, m, t.P);
+                rc = upload_records(c, m, t.P, t.rpb ? t.P * t.rpb : m.N);
                 if (rc != GATT_OK) break;
                 rc = sweep(c, d, k, c->d1, bs, in, c->d1, bs, outs, nf, c->nb, 0.0, nullptr);
                 if (rc != GATT_OK) break;
@@ -1834,7 +1864,7 @@ int autotune(gatt_ctx *c, int reps, int *family, int *blocks, double *us)
             }
             if (rc != GATT_OK) break;
             m.family = best.family; m.rpb = best.rpb;
-            rc = upload_records(c, m, best.P);
+            rc = upload_records(c, m, best.P, best.rpb ? best.P * best.rpb : m.N);
             if (family) family[slot] = best.family;
             if (blocks) blocks[slot] = best.P;
             if (us) us[slot] = 1e3 * best_ms;
@@ -2055,8 +2085,9 @@ int gatt_set_matrices(gatt_ctx *c, int dir, int kind, int periodic, int nRHS, in
         for (uint8_t t : cur)
             if (t >= nTypes) return fail(GATT_ERR_BADARG, "existing block types exceed nTypes");
     }
-    const int rpb = choose_rpb(N, nRHS);
-    const int P = rpb ? N / rpb : choose_blocks(N, nRHS, (W + 3) / 4 * 4);
+    const int Np = padded_rows(c, d, N, nRHS, periodic);
+    const int rpb = choose_rpb(N, Np, nRHS);
+    const int P = rpb ? Np / rpb : choose_blocks(N, nRHS, (W + 3) / 4 * 4);
     TRY(sync_stream(c));
     DevDir &m = c->mat[d][kind];
     cudaFree(m.Rm);
@@ -2064,7 +2095,8 @@ int gatt_set_matrices(gatt_ctx *c, int dir, int kind, int periodic, int nRHS, in
     m = DevDir();
     m.periodic = periodic; m.nR = nRHS; m.nTypes = nTypes; m.N = N; m.W = W; m.Wp = (W + 3) / 4 * 4;
     m.hA = std::move(hA); m.hB = std::move(hB); m.hC = std::move(hC); m.hD = std::move(hD); m.hR = std::move(hR);
-    TRY(upload_records(c, m, P));
+    m.Np = Np;
+    TRY(upload_records(c, m, P, rpb ? Np : N));
     m.rpb = rpb;
     m.family = rpb ? choose_family() : FAM_TILE;
     m.set = true;
@@ -2410,7 +2442,7 @@ int gatt_selftest_pipeline_timeout(gatt_ctx *c)
     memset(&a, 0, sizeof(a));
     const StateSet q = state_set(c, 0);
     a.in = q.v[0]; a.out = c->tmp; a.npts = c->npts;
-    a.nx = c->nx; a.ny = c->ny; a.nz = c->nz; a.N = m.N; a.nlines = nlines(c, 0);
+    a.nx = c->nx; a.ny = c->ny; a.nz = c->nz; a.N = m.rows; a.Nreal = m.N; a.nlines = nlines(c, 0);
     a.es = 1; a.os = 0; a.tiles_per_row = (c->nx + kLanes - 1) / kLanes;
     a.Rm = m.Rm; a.Q = m.Q; a.W = m.W; a.Wp = m.Wp; a.P = m.P; a.ltype = c->ltype[0];
     a.epi = EPI_STORE; a.dir = 0; a.nf = 1; a.ntiles = (a.nlines + kLanes - 1) / kLanes; a.njobs = a.ntiles;

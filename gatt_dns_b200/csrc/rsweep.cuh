@@ -318,10 +318,11 @@ __device__ __forceinline__ LineRef line_at(const SweepArgs &a, const JobCursor &
     return r;
 }
 
-// Store the solved block (optionally blended with the input values `orig(j)`).
-template <bool XD, int RPB, typename Orig>
+// Store the solved block (optionally blended with the input values `orig(j)`); with GUARD,
+// y/z rows from nrows on (padding of non-cyclic lines) are not stored.
+template <bool XD, int RPB, bool GUARD = false, typename Orig>
 __device__ __forceinline__ void store_block(double *w, double *Gl, long long s, int sp, bool blend_on, double blend,
-                                            Orig orig)
+                                            Orig orig, int nrows)
 {
     if (XD) {
 #pragma unroll
@@ -344,7 +345,7 @@ __device__ __forceinline__ void store_block(double *w, double *Gl, long long s, 
                 const double o = orig(j);
                 v = o + blend * (v - o);
             }
-            Gl[(long long)(sp + j) * s] = v;
+            if (!GUARD || sp + j < nrows) Gl[(long long)(sp + j) * s] = v;
         }
     }
 }
@@ -408,7 +409,7 @@ __global__ void __launch_bounds__(32 * kMaxP) k_rsweep(const SweepArgs a)
     if (!lr.valid) return;
     const bool blend_on = a.epi == EPI_BLEND;
     const double blend = blend_on ? sweep_blend(a) : 0.0;
-    store_block<XD, RPB>(w, Gl, s, sp, blend_on, blend, [&](int j) { return ldg(sp + j); });
+    store_block<XD, RPB>(w, Gl, s, sp, blend_on, blend, [&](int j) { return ldg(sp + j); }, N);
 }
 
 // ---- persistent CTAs, TMA-fed two-stage ring --------------------------------------------
@@ -581,7 +582,8 @@ __global__ void __launch_bounds__((NR == 6 && !XD) ? 32 * kMaxP : 768) k_psweep(
         } else {
             if (lr.valid) {
                 double *Gl = a.out + (long long)b * a.out_bstride + (long long)a.out_slot[f] * a.npts + lr.base;
-                store_block<XD, RPB>(w, Gl, lr.s, sp, blend_on, blend, [&](int jj) { return lds(sp + jj); });
+                store_block<XD, RPB, !PER>(w, Gl, lr.s, sp, blend_on, blend, [&](int jj) { return lds(sp + jj); },
+                                           a.Nreal);
             }
             if (blend_on) {
                 __syncthreads();

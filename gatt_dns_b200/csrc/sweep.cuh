@@ -76,6 +76,7 @@ struct SweepArgs {
     int njobs;               // ntiles * nf * members
     int ntypes;              // line types of the coefficient set
     int nst;                 // ring stages (1 .. kMaxStages)
+    int Nreal;               // rows of a line that are stored (N, or fewer for padded lines)
     int tx_extra;            // bytes added to every copy barrier's expected count: 0, except in
                              // gatt_selftest_pipeline_timeout (its waits must run out)
     int *err;                // set to 1 when a pipeline wait gives up (host-mapped)
