@@ -310,8 +310,24 @@ void *pick_reg_kernel(int nR)
 #undef GATT_REG_CASE
 }
 
-void *reg_kernel(bool pipe, bool xd, bool per, int nR)
+// The pipelined x solver for more than 24 row blocks (800-thread bound).
+template <bool PER>
+void *pick_wide_kernel(int nR)
 {
+    switch (nR) {
+    case 2: return (void *)k_psweep<true, PER, 2, kRPB, true>;
+    case 3: return (void *)k_psweep<true, PER, 3, kRPB, true>;
+    case 4: return (void *)k_psweep<true, PER, 4, kRPB, true>;
+    case 5: return (void *)k_psweep<true, PER, 5, kRPB, true>;
+    case 6: return (void *)k_psweep<true, PER, 6, kRPB, true>;
+    case 7: return (void *)k_psweep<true, PER, 7, kRPB, true>;
+    default: return nullptr;
+    }
+}
+
+void *reg_kernel(bool pipe, bool xd, bool per, int nR, bool wide = false)
+{
+    if (wide) return (pipe && xd) ? (per ? pick_wide_kernel<true>(nR) : pick_wide_kernel<false>(nR)) : nullptr;
     if (pipe) {
         if (xd) return per ? pick_reg_kernel<true, true, true>(nR) : pick_reg_kernel<true, false, true>(nR);
         return per ? pick_reg_kernel<false, true, true>(nR) : pick_reg_kernel<false, false, true>(nR);
@@ -361,6 +377,9 @@ int choose_family()
     return FAM_PIPE;
 }
 
+// Shared memory a CTA may use (the opt-in maximum less a margin).
+constexpr size_t kMaxSmem = 227 * 1024 - 256;
+
 // Padded line length for the pipelined solver: non-cyclic y/z lines whose length is not a
 // multiple of kRPB run as lines of the next multiple, the extra rows identity rows (A = C = 0,
 // reciprocal pivot 1, zero band) that the tile copy fills with zeros past the grid edge and
@@ -378,14 +397,17 @@ int padded_rows(const gatt_ctx *c, int d, int N, int nR, int periodic)
 
 // Block height of the register-resident solvers for lines of Np rows (Np: N or its padded
 // length) and band nR, or 0 when the shared-tile solver handles them (length not a multiple of
-// kRPB, more than kMaxP blocks, or a band wider than kMaxNRreg).  Padded lines need the
-// pipelined solver (the only one that zero-fills past the grid edge).
-int choose_rpb(int N, int Np, int nR)
+// kRPB, too many blocks, or a band wider than kMaxNRreg).  Padded lines and x lines of more
+// than kMaxP blocks (up to kMaxPx) need the pipelined solver, and its shared memory must fit.
+int choose_rpb(int d, int N, int Np, int nR, int nTypes, int Wp)
 {
     if (choose_family() == FAM_TILE) return 0;
-    if (nR < 2 || nR > kMaxNRreg) return 0;
-    if (Np != N && choose_family() != FAM_PIPE) return 0;
-    return (Np % kRPB == 0 && Np / kRPB <= kMaxP) ? kRPB : 0;
+    if (nR < 2 || nR > kMaxNRreg || Np % kRPB) return 0;
+    const int P = Np / kRPB;
+    if (P <= kMaxP && Np == N) return kRPB;
+    const bool pipe = choose_family() == FAM_PIPE;
+    if (!pipe || P > (d == 0 ? kMaxPx : kMaxP)) return 0;
+    return psweep_smem_bytes(d == 0, Np, P, nTypes, Wp, 1) <= kMaxSmem ? kRPB : 0;
 }
 
 size_t sweep_smem(int N, int P, int nR, int Wp, bool stage = true)
@@ -393,7 +415,6 @@ size_t sweep_smem(int N, int P, int nR, int Wp, bool stage = true)
     return sweep_smem_doubles(N, P, nR, Wp, stage) * sizeof(double);
 }
 // 227 KB per block, less a margin for the kernel's few static shared variables
-constexpr size_t kMaxSmem = 227 * 1024 - 256;
 constexpr int kMaxNR = 11;  // widest band the shared-tile solver is instantiated for
 
 // Row blocks per line: about 32 rows per block (shorter dependency chains, more warps per
@@ -425,11 +446,13 @@ int set_sweep_attributes()
                 }
     for (int xd = 0; xd < 2; xd++)
         for (int per = 0; per < 2; per++)
-            for (int nR = 2; nR <= kMaxNRreg; nR++) {
-                void *k = reg_kernel(true, xd != 0, per != 0, nR);
-                CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
-                CU(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-            }
+            for (int nR = 2; nR <= kMaxNRreg; nR++)
+                for (int wide = 0; wide < 2; wide++) {
+                    void *k = reg_kernel(true, xd != 0, per != 0, nR, wide != 0);
+                    if (!k) continue;
+                    CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+                    CU(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+                }
     CU(cudaFuncSetAttribute((const void *)k_assemble3d_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)pw_smem_bytes(kPwStages)));
     return GATT_OK;
@@ -499,7 +522,7 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
 {
     const int N = m.rows;  // padded y/z lines: the box covers the padding (zero fill)
     const bool xd = d == 0;
-    void *k = reg_kernel(true, xd, m.periodic != 0, m.nR);
+    void *k = reg_kernel(true, xd, m.periodic != 0, m.nR, m.P > 24);  // 25 blocks: the 800-thread form
     if (!k) return GATT_ERR_STATE;
     // ring depth: the deepest ring that keeps the most CTAs resident (one stage suffices
     // when a tile's solve outlasts the next tile's copy)
@@ -607,7 +630,8 @@ int sweep(gatt_ctx *c, int d, int kind, const double *in, long long in_bs, const
         int r = launch_psweep(c, m, d, a, nmembers, cls);
         if (r != GATT_ERR_STATE) return r;  // GATT_ERR_STATE: layout not expressible, use k_rsweep
         // padded lines: only the pipelined solver zero-fills past the grid edge
-        if (m.rows != m.N) return fail(GATT_ERR_STATE, "padded lines need the pipelined solver (layout refused)");
+        if (m.rows != m.N || m.P > kMaxP)
+            return fail(GATT_ERR_STATE, "padded or long lines need the pipelined solver (layout refused)");
     }
     a.stage = !m.rpb && sweep_smem(m.N, m.P, m.nR, m.Wp, true) <= kMaxSmem;
     const size_t smem = m.rpb ? (size_t)3 * m.P * kLanes * sizeof(double) : sweep_smem(m.N, m.P, m.nR, m.Wp, a.stage);
@@ -1807,8 +1831,8 @@ std::vector<TuneCand> tune_candidates(const DevDir &m)
     if (m.N % kRPB == 0 && m.N / kRPB <= kMaxP && m.nR >= 2 && m.nR <= kMaxNRreg) {
         out.push_back({FAM_PIPE, kRPB, m.N / kRPB});
         out.push_back({FAM_REG, kRPB, m.N / kRPB});
-    } else if (m.Np > m.N) {
-        out.push_back({FAM_PIPE, kRPB, m.Np / kRPB});  // padded lines: the pipelined solver only
+    } else if (m.Np > m.N || (m.N % kRPB == 0 && m.N / kRPB > kMaxP && m.family == FAM_PIPE && m.rpb)) {
+        out.push_back({FAM_PIPE, kRPB, m.Np / kRPB});  // padded or long lines: the pipelined solver only
     }
     for (int rows : {8, 16, 32, 64}) {
         const int P = choose_blocks(m.N, m.nR, m.Wp, rows);
@@ -2086,7 +2110,7 @@ int gatt_set_matrices(gatt_ctx *c, int dir, int kind, int periodic, int nRHS, in
             if (t >= nTypes) return fail(GATT_ERR_BADARG, "existing block types exceed nTypes");
     }
     const int Np = padded_rows(c, d, N, nRHS, periodic);
-    const int rpb = choose_rpb(N, Np, nRHS);
+    const int rpb = choose_rpb(d, N, Np, nRHS, nTypes, (W + 3) / 4 * 4);
     const int P = rpb ? Np / rpb : choose_blocks(N, nRHS, (W + 3) / 4 * 4);
     TRY(sync_stream(c));
     DevDir &m = c->mat[d][kind];

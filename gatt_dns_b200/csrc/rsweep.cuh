@@ -422,9 +422,10 @@ __global__ void __launch_bounds__(32 * kMaxP) k_rsweep(const SweepArgs a)
 // output map (one tensor store; 32 line copies each way were bound by the number of copies).
 // Register cap: the 768-thread bound holds a thread to 80 registers, which keeps three
 // 256-thread CTAs resident (84 registers round up to two); the y/z 6-band filter spills at
-// 80 and keeps the plain 512-thread bound.
-template <bool XD, bool PER, int NR, int RPB>
-__global__ void __launch_bounds__((NR == 6 && !XD) ? 32 * kMaxP : 768) k_psweep(const SweepArgs a, const __grid_constant__ CUtensorMap tmap,
+// 80 and keeps the plain 512-thread bound.  WIDE (x lines of 25 row blocks, up to 400 points):
+// an 800-thread bound, which holds a thread to 72 registers.
+template <bool XD, bool PER, int NR, int RPB, bool WIDE = false>
+__global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * kMaxP : 768)) k_psweep(const SweepArgs a, const __grid_constant__ CUtensorMap tmap,
                                                                      const __grid_constant__ CUtensorMap omap)
 {
     constexpr int H = NR - 1;

@@ -32,6 +32,7 @@ namespace gatt {
 
 constexpr int kLanes = 32;   // lines per tile
 constexpr int kMaxP = 16;    // largest number of row blocks per line
+constexpr int kMaxPx = 25;   // row blocks of the pipelined x solver (800 threads: 80 registers)
 
 enum SweepEpi { EPI_STORE = 0, EPI_BLEND = 1 };
 

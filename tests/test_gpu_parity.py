@@ -58,6 +58,11 @@ def get_case(name):
             _CASES[name] = cs.boundary_layer_cavity(nx=96, ny=48, buffers=((8, 6), (0, 8)))
         elif name == "long_x":
             _CASES[name] = cs.lid_driven(nxy=(900, 12))
+        elif name == "lid_x400":
+            # 400-point x lines: 25 row blocks, the wide pipelined solver
+            _CASES[name] = cs.lid_driven(nxy=(400, 16))
+        elif name == "box_x400":
+            _CASES[name] = cs.periodic_box(nxyz=(400, 16, 8))
         elif name == "box_ragged":
             # 5040 points: the last 256-point chunk of the tensor-copy assembly is partial
             _CASES[name] = cs.periodic_box(nxyz=(20, 18, 14))
@@ -84,7 +89,7 @@ def pair(name):
 
 
 @pytest.mark.parametrize("name", ["box", "box_aniso", "box64", "lid", "lid64", "lid_tanh", "cavity2d", "cavity3d",
-                                  "cavity3d_32", "long_x"])
+                                  "cavity3d_32", "long_x", "lid_x400", "box_x400"])
 @pytest.mark.parametrize("kind", ["deriv", "filter"])
 @pytest.mark.parametrize("solver", ["pipe", "reg", "tile"])
 def test_line_solves(libs, monkeypatch, name, kind, solver):
@@ -141,7 +146,7 @@ def test_filter_in_place(libs, name):
 
 
 @pytest.mark.parametrize("name", ["box", "box_aniso", "box64", "lid", "lid64", "lid_tanh", "cavity2d", "cavity3d",
-                                  "cavity3d_32", "bl", "bl_cavity", "box_ragged", "box_odd"])
+                                  "cavity3d_32", "bl", "bl_cavity", "box_ragged", "box_odd", "lid_x400", "box_x400"])
 def test_step(libs, name):
     c, g, o = pair(name)
     f = flow_for(c, seed=2)
