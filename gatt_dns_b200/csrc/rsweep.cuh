@@ -1,6 +1,7 @@
 // Register-resident compact line solves for sm_100a: the fast forms of
 // solveSystem{X,Y,Z}[per] (reference source/Fortran/derivs.F90:556-948) for lines whose
-// length N is a multiple of the block height RPB (16 rows).
+// length N is a multiple of the block height RPB (16 rows); k_psweep also takes non-cyclic
+// y/z lines padded to such a length with identity rows (the host builds their records).
 //
 // Same algorithm and row records as k_sweep (sweep.cuh): band product, forward and backward
 // Thomas recurrences, cut into P = N / RPB row blocks that run from zero start values and
@@ -15,8 +16,8 @@
 //    the neighbouring block's rows, L2 hits);
 //  * k_psweep: persistent CTAs with a one- or two-stage shared-memory ring filled by the Tensor
 //    Memory Accelerator -- one cp.async.bulk.tensor box {32 x N} per y/z tile (it lands
-//    as [row][lane]) or 32 one-dimensional cp.async.bulk line copies per x tile -- so the
-//    next tile streams in while the current one is solved from registers and stored.
+//    as [row][lane]) or one 128-byte-swizzled box per x tile (stored back the same way) --
+//    so the next tile streams in while the current one is solved from registers and stored.
 //    The coefficient records of all line types are copied to shared memory once per CTA.
 //    Every mbarrier wait is bounded; a wait that gives up sets *err and the CTA returns.
 #pragma once

@@ -68,7 +68,7 @@ struct SweepArgs {
     const double *blend_dt;  // ... or, when set, blend = *blend_dt / blend_fct (device dt)
     double blend_fct;
     int epi;                 // SweepEpi
-    int P;                   // row blocks per line (1 .. kMaxP); CTA = 32*P threads
+    int P;                   // row blocks per line (1 .. kMaxP; kMaxPx for wide x lines); CTA = 32*P threads
     int stage;               // k_sweep: shared memory holds a coefficient copy (1) or not (0)
     // pipelined solver (k_psweep) only
     int dir;                 // 0 x, 1 y, 2 z
