@@ -385,13 +385,13 @@ constexpr size_t kMaxSmem = 227 * 1024 - 256;
 // reciprocal pivot 1, zero band) that the tile copy fills with zeros past the grid edge and
 // the store skips; the real rows' results are those of the unpadded line (the last real row
 // has no super-diagonal, the first padded one no sub-diagonal).  Returns N when that does not
-// apply (cyclic or x lines, lines past one tensor box of 256 rows, layouts the tensor map
+// apply (cyclic or x lines, more rows than the y/z solver's 24 blocks, layouts the tensor map
 // cannot describe).
 int padded_rows(const gatt_ctx *c, int d, int N, int nR, int periodic)
 {
     if (N % kRPB == 0 || periodic || d == 0 || nR < 2 || nR > kMaxNRreg) return N;
     const int np = (N + kRPB - 1) / kRPB * kRPB;
-    if (np / kRPB > kMaxP || np > 256 || (c->nx & 1) || (c->npts & 1)) return N;
+    if (np / kRPB > kMaxPyz || (c->nx & 1) || (c->npts & 1)) return N;
     return np;
 }
 
@@ -406,7 +406,10 @@ int choose_rpb(int d, int N, int Np, int nR, int nTypes, int Wp)
     const int P = Np / kRPB;
     if (P <= kMaxP && Np == N) return kRPB;
     const bool pipe = choose_family() == FAM_PIPE;
-    if (!pipe || P > (d == 0 ? kMaxPx : kMaxP)) return 0;
+    // thread bounds of the pipelined instantiations: x wide form 800, y/z 768 (512 for the
+    // 6-band filter)
+    const int maxp = d == 0 ? kMaxPx : (nR == 6 ? kMaxP : kMaxPyz);
+    if (!pipe || P > maxp) return 0;
     return psweep_smem_bytes(d == 0, Np, P, nTypes, Wp, 1) <= kMaxSmem ? kRPB : 0;
 }
 
@@ -572,7 +575,9 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
         if (!xmap(&map, a.in, a.in_slot, a.in_bstride) || !xmap(&omap, a.out, a.out_slot, a.out_bstride))
             return GATT_ERR_STATE;
     } else {
-        if (N > 256 || (c->nx & 1)) return GATT_ERR_STATE;
+        // one box of N rows, or two of N/2 for lines past the copy engine's 256-row box
+        if (N > 512 || (N > 256 && (N & 1)) || (c->nx & 1)) return GATT_ERR_STATE;
+        a.box2 = N > 256 ? N / 2 : 0;
         EncodeTiledFn enc = encode_tiled();
         if (!enc) return GATT_ERR_STATE;
         int nslots = 1;
@@ -582,7 +587,9 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
                               (cuuint64_t)nmembers};
         cuuint64_t strides[4] = {(cuuint64_t)c->nx * 8, (cuuint64_t)c->nx * c->ny * 8, (cuuint64_t)c->npts * 8,
                                  (cuuint64_t)mstride * 8};
-        cuuint32_t box[5] = {(cuuint32_t)kLanes, (cuuint32_t)(d == 1 ? N : 1), (cuuint32_t)(d == 2 ? N : 1), 1, 1};
+        const int brows = a.box2 ? a.box2 : N;
+        cuuint32_t box[5] = {(cuuint32_t)kLanes, (cuuint32_t)(d == 1 ? brows : 1), (cuuint32_t)(d == 2 ? brows : 1), 1,
+                             1};
         cuuint32_t estr[5] = {1, 1, 1, 1, 1};
         CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<double *>(a.in), dims, strides, box, estr,
                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -2119,7 +2126,7 @@ int gatt_set_matrices(gatt_ctx *c, int dir, int kind, int periodic, int nRHS, in
     m = DevDir();
     m.periodic = periodic; m.nR = nRHS; m.nTypes = nTypes; m.N = N; m.W = W; m.Wp = (W + 3) / 4 * 4;
     m.hA = std::move(hA); m.hB = std::move(hB); m.hC = std::move(hC); m.hD = std::move(hD); m.hR = std::move(hR);
-    m.Np = Np;
+    m.Np = rpb ? Np : N;  // a padded length the solver does not take is not kept
     TRY(upload_records(c, m, P, rpb ? Np : N));
     m.rpb = rpb;
     m.family = rpb ? choose_family() : FAM_TILE;

@@ -470,6 +470,9 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
             mbar_expect_tx(bar, (uint32_t)(N * kLanes * sizeof(double) + a.tx_extra));
             tma_load_5d(dst, &tmap, c.tx * kLanes, a.dir == 1 ? 0 : c.o, a.dir == 1 ? c.o : 0, a.in_slot[c.f], c.b,
                         bar);
+            if (a.box2)  // second half of a line past one 256-row box
+                tma_load_5d(dst + (uint32_t)(a.box2 * kLanes * sizeof(double)), &tmap, c.tx * kLanes,
+                            a.dir == 1 ? a.box2 : c.o, a.dir == 1 ? c.o : a.box2, a.in_slot[c.f], c.b, bar);
         }
     };
     if (threadIdx.x == 0)

@@ -32,7 +32,8 @@ namespace gatt {
 
 constexpr int kLanes = 32;   // lines per tile
 constexpr int kMaxP = 16;    // largest number of row blocks per line
-constexpr int kMaxPx = 25;   // row blocks of the pipelined x solver (800 threads: 80 registers)
+constexpr int kMaxPx = 25;   // row blocks of the pipelined x solver (wide form, 800 threads)
+constexpr int kMaxPyz = 24;  // row blocks of the pipelined y/z solver (768 threads; 6-band: kMaxP)
 
 enum SweepEpi { EPI_STORE = 0, EPI_BLEND = 1 };
 
@@ -78,6 +79,7 @@ struct SweepArgs {
     int ntypes;              // line types of the coefficient set
     int nst;                 // ring stages (1 .. kMaxStages)
     int Nreal;               // rows of a line that are stored (N, or fewer for padded lines)
+    int box2;                // y/z lines past 256 rows: rows per tensor box (two boxes), else 0
     int tx_extra;            // bytes added to every copy barrier's expected count: 0, except in
                              // gatt_selftest_pipeline_timeout (its waits must run out)
     int *err;                // set to 1 when a pipeline wait gives up (host-mapped)

@@ -61,6 +61,11 @@ def get_case(name):
         elif name == "lid_x400":
             # 400-point x lines: 25 row blocks, the wide pipelined solver
             _CASES[name] = cs.lid_driven(nxy=(400, 16))
+        elif name == "lid_y300":
+            # 300-point y lines: padded to 304, two tensor boxes of 152 rows, 19 row blocks
+            _CASES[name] = cs.lid_driven(nxy=(16, 300))
+        elif name == "box_y288":
+            _CASES[name] = cs.periodic_box(nxyz=(16, 288, 8))
         elif name == "box_x400":
             _CASES[name] = cs.periodic_box(nxyz=(400, 16, 8))
         elif name == "box_ragged":
@@ -89,7 +94,7 @@ def pair(name):
 
 
 @pytest.mark.parametrize("name", ["box", "box_aniso", "box64", "lid", "lid64", "lid_tanh", "cavity2d", "cavity3d",
-                                  "cavity3d_32", "long_x", "lid_x400", "box_x400"])
+                                  "cavity3d_32", "long_x", "lid_x400", "box_x400", "lid_y300", "box_y288"])
 @pytest.mark.parametrize("kind", ["deriv", "filter"])
 @pytest.mark.parametrize("solver", ["pipe", "reg", "tile"])
 def test_line_solves(libs, monkeypatch, name, kind, solver):
@@ -146,7 +151,8 @@ def test_filter_in_place(libs, name):
 
 
 @pytest.mark.parametrize("name", ["box", "box_aniso", "box64", "lid", "lid64", "lid_tanh", "cavity2d", "cavity3d",
-                                  "cavity3d_32", "bl", "bl_cavity", "box_ragged", "box_odd", "lid_x400", "box_x400"])
+                                  "cavity3d_32", "bl", "bl_cavity", "box_ragged", "box_odd", "lid_x400", "box_x400",
+                                  "lid_y300", "box_y288"])
 def test_step(libs, name):
     c, g, o = pair(name)
     f = flow_for(c, seed=2)
