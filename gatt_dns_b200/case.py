@@ -131,9 +131,55 @@ def _buffer_zone(par):
     raise ValueError("unknown buffer type %r" % par["type"])
 
 
+def _match_fixed(xp, fix_points):
+    """generateMesh.m:186-207 with matchFixed = 2: move the nodes nearest to the fixed points
+    onto them and shift the others by the pchip interpolant of those moves."""
+    from scipy.interpolate import PchipInterpolator
+    n = len(xp)
+    fp = np.unique(np.concatenate([xp[[0, 1]], np.asarray(fix_points, dtype=np.float64), xp[[-2, -1]]]))
+    fp = fp[np.isfinite(fp) & (fp >= xp[0]) & (fp <= xp[-1])]
+    closest = np.argmin(np.abs(xp[:, None] - fp[None, :]), axis=0)
+    for _ in range(n + 1):
+        dup = np.nonzero(np.diff(closest) == 0)[0]
+        if len(dup) == 0:
+            break
+        closest[dup] -= 1
+    shift = PchipInterpolator(closest.astype(np.float64), xp[closest] - fp)(np.arange(n, dtype=np.float64))
+    out = xp - shift
+    out[closest] = fp
+    return out
+
+
+def _attractor_mesh(xi, xf, n, points=(), regions=()):
+    """generateMesh.m:123-147 ('attractors'): node density 1 + sum of Gaussian attractors
+    (point, strength, size) + sum of region ramps (strength times the squared pchip of
+    0 0 1 1 0 0 over [a-1, a, b, c, d, d+1]), integrated on 100 n base points and inverted
+    with a not-a-knot cubic spline, as interp1(..., 'spline') does."""
+    from scipy.interpolate import CubicSpline, PchipInterpolator
+    xb = np.linspace(xi, xf, 100 * n)
+    eta = np.ones(100 * n)
+    for (p, strength, size) in points:
+        eta += strength * np.exp(-((xb - p) / size) ** 2)
+    for reg in regions:
+        pos = [float(v) for v in reg[:4]]
+        if math.isinf(pos[1]):
+            pos[0:2] = [xi - 2, xi - 1]
+        if math.isinf(pos[2]):
+            pos[2:4] = [xf + 1, xf + 2]
+        pos = [pos[0] - 1] + pos + [pos[3] + 1]
+        eta += reg[4] * PchipInterpolator(pos, [0, 0, 1, 1, 0, 0])(xb) ** 2
+    eta = np.cumsum(eta)
+    eta -= eta[0]
+    eta = (n - 1) * eta / eta[-1] + 1
+    eta[-1] = n
+    return CubicSpline(eta, xb)(np.arange(1, n + 1, dtype=np.float64))
+
+
 def generate_mesh(xi, xf, n, mtype="uniform", periodic=False, fix_periodic_domain_size=False,
-                  par=2.0, local="b", power=2.0, buffer_i=None, buffer_f=None):
-    """Node coordinates of one direction (generateMesh.m:1-247, no fixed-point matching)."""
+                  par=2.0, local="b", power=2.0, buffer_i=None, buffer_f=None, fix_points=None,
+                  attractor_points=(), attractor_regions=()):
+    """Node coordinates of one direction (generateMesh.m:1-247); ``fix_points`` are matched
+    as mesh.matchFixed = 2 does (points outside [xi, xf] are dropped, meshAddFixedPoints.m:54)."""
     buffer_i = dict(buffer_i or {"n": 0})
     buffer_f = dict(buffer_f or {"n": 0})
     if n == 1:
@@ -159,8 +205,12 @@ def generate_mesh(xi, xf, n, mtype="uniform", periodic=False, fix_periodic_domai
         else:
             eta = np.tanh(np.linspace(-par, par, n)); eta = eta / eta[-1]; eta = (eta + 1) / 2
         xp = (xf - xi) * eta + xi
+    elif mtype == "attractors":
+        xp = _attractor_mesh(xi, xf, n, attractor_points, attractor_regions)
     else:
         raise ValueError("mesh type %r not restated" % mtype)
+    if fix_points is not None and len(fix_points) and n > 1:
+        xp = _match_fixed(xp, fix_points)
     X = np.zeros(ntot)
     X[ni:ni + n] = xp
     if ni > 0:
@@ -398,10 +448,11 @@ def init_boundaries(items, corners, neumann_coeffs, neumann2_coeffs):
 
 def build_matrices(X, Y, Z, flow_region, periodic, fix_periodic, domain_ends, deriv="SL4", deriv_buffer="EX4",
                    filter_alpha=0.49, filter_borders="decentered", filter_border_flags=None,
-                   buffers=None, metric="SL4", round_fortran=True):
-    """Per-direction :class:`DirectionMatrices` for a case (``makeMatrices.m:1-155``)."""
+                   buffers=None, metric="SL4", round_fortran=True, break_points=(None, None, None)):
+    """Per-direction :class:`DirectionMatrices` for a case (``makeMatrices.m:1-155``);
+    ``break_points`` restates ``mesh.x/y/z.breakPoint`` (``findDerivativeRegions.m:45-60``)."""
     nx, ny, nz = len(X), len(Y), len(Z)
-    reg = mx.find_derivative_regions(flow_region, periodic)
+    reg = mx.find_derivative_regions(flow_region, periodic, break_points)
     cl, cr, dl, dr = mx.finite_difference_coefficients(deriv)
     clb, crb, dlb, drb = mx.finite_difference_coefficients(deriv_buffer)
     fl, fr_, fdl, fdr = mx.spatial_filter_coefficients(filter_alpha, filter_borders)
@@ -607,71 +658,112 @@ def sfd_region(shape, buffers, X):
 
 
 def boundary_layer_cavity(nx=800, ny=300, Re=1000.0, Ma=0.5, Pr=0.71, gamma=1.4, T0=300.0, filter_alpha=0.49,
-                          deriv="SL4", cavity=(1.0, 2.0), buffers=((40, 30), (0, 40)), ny_cavity=None,
-                          sfd=(0.02, 15.0)):
+                          deriv="SL4", cavity=(1.0, 2.0), buffers=((40, 30), (0, 40)),
+                          sfd=(0.02, 15.0), x_range=(-1.0, 5.0)):
     """2-D compressible boundary layer over a rectangular cavity with buffer zones and SFD.
 
     Domain x in [-1, 5], y in [-1, 4] (physical part), cavity of depth 1 at 1 < x < 2, the
     buffer zones of parameters.m:124-142 (sigmoid; inflow 40, outflow 30 and top 40 nodes
-    in the full case) with EX4 derivatives inside them, and the boundary set of
-    boundaryLayerIsothermal.m for mesh.X(1) < 0: Dirichlet inflow u = 1, v = 0, e = E0 with
-    pressure Neumann (:4-66), outflow null second derivatives with p = P0 (:83-145), outer
-    flow null second derivatives (:146-207), no-slip isothermal walls (findWallsForBoundaries
-    + the wall list), and free slip (u Neumann) on the wall upstream of the leading edge x = 0
-    (:408-429).  SFD type 2 on the buffer zones (calcSFDregion.m), X and Delta from `sfd`.
-    nx, ny count all nodes, buffers included.
+    in the full case) with EX4 derivatives inside them, the filter borders of
+    parameters.m:182-186 (reduced order, no filter on the first and last five x nodes nor
+    on the last five y nodes) and SFD type 2 on the buffer ramps (calcSFDregion.m), X and
+    Delta from `sfd`.  nx, ny count all nodes, buffers included.
+
+    The boundary set is boundaryLayerIsothermal.m's for mesh.X(1) < 0, in its order:
+    * Dirichlet inflow u = 1, v = w = 0, e = E0 and pressure Neumann over the whole x = X(1)
+      plane (:4-78), outflow null second derivatives with p = P0 (:80-138), outer flow null
+      second derivatives (:141-201);
+    * the flow region: solid at and below the row nearest y = 0, the cavity carved out
+      (:317-344), walls, corners and wall interiors from findWallsForBoundaries;
+    * the free-slip wall (:362-369): every up-facing wall is moved to start at the first node
+      with x >= 0, the plate row upstream of it becomes a wall of its own (the last up wall)
+      and the x derivative and filter stencils are cut there (mesh.x.breakPoint, restated by
+      findDerivativeRegions.m:45-60);
+    * pressure Neumann on every wall (:371-405), u and w Neumann on the free-slip wall
+      (:407-431), then p = P0, u = v = w = 0, e = E0 on every solid node (:433-497).
     """
     (bxi, bxf), (byi, byf) = buffers
     sig = lambda n, st: {"n": n, "type": "sigmoid", "stretching": st, "transition": 0.2}
-    X = generate_mesh(-1.0, 5.0, nx - bxi - bxf, buffer_i=sig(bxi, 30) if bxi else None,
-                      buffer_f=sig(bxf, 15) if bxf else None)
-    ny_phys = ny - byi - byf
-    nyc = ny_cavity or max(4, ny_phys // 6)
-    yc = np.linspace(-1.0, 0.0, nyc)
-    yu = generate_mesh(0.0, 4.0, ny_phys - nyc + 1, mtype="tanh", par=1.5, local="i",
-                       buffer_f=sig(byf, 30) if byf else None)
-    Y = np.concatenate([yc[:-1], yu])
-    Z = np.array([0.0])
     x0, x1 = cavity
-    # solid at and below y = 0 (the plate surface row is wall), except the cavity's inside
-    fr = (Y[None, :, None] > 0) | ((X[:, None, None] > x0) & (X[:, None, None] < x1))
-    fr = np.array(fr, copy=True)
-    fr[:, 0, :] = False
-    fr, walls, corners, inside = find_walls_for_boundaries(fr)
+    # meshes of parameters.m:84-115 ('attractors', matchFixed = 2) scaled to this domain: in
+    # x a region of strength 3 around the cavity and a point attractor at the leading edge
+    # (the reference's domain starts there); in y the region [-2D, -D/10, D/10, 2 delta99]
+    # of strength 12 with delta99 = 5 sqrt(xEnd / Re) at the outflow; fixed points
+    # (meshAddFixedPoints.m:3-10) at the leading edge, the cavity edges and its bottom
+    X = generate_mesh(x_range[0], x_range[1], nx - bxi - bxf, mtype="attractors",
+                      attractor_points=[(0.0, 2.0, 0.1)],
+                      attractor_regions=[(x0 - 0.5, x0 - 0.25, x1 + 0.25, x1 + 0.5, 3.0)],
+                      buffer_i=sig(bxi, 30) if bxi else None, buffer_f=sig(bxf, 15) if bxf else None,
+                      fix_points=(0.0, x0, x1))
+    d99 = 5.0 * math.sqrt(x_range[1] / Re)
+    Y = generate_mesh(-1.0, 4.0, ny - byi - byf, mtype="attractors",
+                      attractor_regions=[(-2.0, -0.1, 0.1, 2.0 * d99, 12.0)],
+                      buffer_i=sig(byi, 30) if byi else None, buffer_f=sig(byf, 30) if byf else None,
+                      fix_points=(-1.0, 0.0))
+    Z = np.array([0.0])
+    nz = 1
     E0 = 1.0 / ((gamma ** 2 - gamma) * Ma ** 2)
     P0 = (gamma - 1) * E0
-    # the reference's order: inflow, outflow and outer flow over whole boundary planes, then
-    # the walls, whose Dirichlet values override those planes at solid nodes
     items = []
-    inflow = [1, 1, 1, ny, 1, 1]
-    for v, val in (("u", 1.0), ("v", 0.0), ("e", E0)):
+    # inflow (:4-78; the mesh starts at x <= 0)
+    if X[0] > 0:
+        raise ValueError("the inflow hold of boundaryLayerIsothermal.m:53-66 (X(1) > 0) is not restated")
+    inflow = [1, 1, 1, ny, 1, nz]
+    for v, val in (("u", 1.0), ("v", 0.0), ("w", 0.0), ("e", E0)):
         items.append((v, "dir", "xi", val, list(inflow)))
     items.append(("p", "neu", "xi", 0.0, list(inflow)))
-    outflow = [nx, nx, 1, ny, 1, 1]
-    for v in ("u", "v", "e"):
+    # outflow (:80-138) and outer flow (:141-201)
+    outflow = [nx, nx, 1, ny, 1, nz]
+    for v in ("u", "v", "w", "e"):
         items.append((v, "sec", "xf", 0.0, list(outflow)))
     items.append(("p", "dir", "xf", P0, list(outflow)))
-    top = [1, nx, ny, ny, 1, 1]
-    for v in ("u", "v", "e", "p"):
+    top = [1, nx, ny, ny, 1, nz]
+    for v in ("u", "v", "w", "e", "p"):
         items.append((v, "sec", "yf", 0.0, list(top)))
-    items += wall_boundary_list(walls, inside, P0, E0)
-    j0 = int(np.argmin(np.abs(Y))) + 1                    # 1-based row of y = 0
-    # the solid nodes of the inflow and outflow planes keep the wall values (no slip, E0)
-    for i in (1, nx):
-        box = [i, i, 1, j0, 1, 1]
-        for v, val in (("u", 0.0), ("v", 0.0), ("e", E0)):
-            items.append((v, "dir", "yi", val, list(box)))
-    # free slip on the plate row upstream of the leading edge x = 0 (:408-429)
-    ile = int(np.argmin(np.abs(X)))                       # 0-based node of the leading edge
-    items.append(("u", "neu", "yi", 0.0, [1, max(1, ile), j0, j0, 1, 1]))
+    # flow region (:317-344): the plate, then the cavity (open interval in x and y)
+    fr = np.ones((nx, ny, nz), dtype=bool)
+    wall_j = int(np.argmin(np.abs(Y))) + 1
+    fr[:, :wall_j, :] = False
+    in_x = (X > x0) & (X < x1)
+    in_y = (Y > -1.0) & (Y < 0.0)
+    fr[np.ix_(in_x, in_y, np.ones(nz, dtype=bool))] = True
+    fr, walls, corners, inside = find_walls_for_boundaries(fr)
+    # free-slip wall and the break point (:362-369)
+    break_x = None
+    if X[0] < 0:
+        first_pos = int(np.nonzero(X >= 0)[0][0]) + 1
+        last_neg = int(np.nonzero(X < 0)[0][-1]) + 1
+        j_plate = int(np.nonzero(Y >= 0)[0][0]) + 1
+        up = [list(w) for w in walls["up"]]
+        for w in up:
+            w[0] = max(w[0], first_pos)
+        up.append([1, last_neg, j_plate, j_plate, 1, nz])
+        walls["up"] = up
+        break_x = [[last_neg, j_plate, j_plate, 1, nz]]
+    # pressure Neumann on every wall (:371-405)
+    for key, d in (("front", "xi"), ("back", "xf"), ("up", "yi"), ("down", "yf"), ("right", "zi"), ("left", "zf")):
+        for w in walls[key]:
+            items.append(("p", "neu", d, 0.0, list(w)))
+    # u and w Neumann on the free-slip wall, the last up wall (:407-431)
+    if X[0] < 0:
+        for v in ("u", "w"):
+            items.append((v, "neu", "yi", 0.0, list(walls["up"][-1])))
+    # every solid node (:433-497)
+    for w in inside:
+        w = list(w)
+        items.append(("p", "dir", "yi", P0, w))
+        for v in ("u", "v", "w"):
+            items.append((v, "dir", "yi", 0.0, w))
+        items.append(("e", "dir", "yi", E0, w))
     n1, n2 = mx.neumann_coefficients(6, 2)
     bc = init_boundaries(items, corners, mx.fortran_round(n1), mx.fortran_round(n2))
     bufs = [{"i": sig(bxi, 30) if bxi else {"n": 0}, "f": sig(bxf, 15) if bxf else {"n": 0}},
             {"i": {"n": 0}, "f": sig(byf, 30) if byf else {"n": 0}},
             {"i": {"n": 0}, "f": {"n": 0}}]
+    flags = {"filterBordersStartX": False, "filterBordersEndX": False, "filterBordersEndY": False}
     mats = build_matrices(X, Y, Z, fr, (False, False, False), (False, False, False), (6.0, 5.0, 1.0),
-                          deriv=deriv, deriv_buffer="EX4", filter_alpha=filter_alpha, filter_borders="decentered",
-                          buffers=bufs)
+                          deriv=deriv, deriv_buffer="EX4", filter_alpha=filter_alpha, filter_borders="reducedOrder",
+                          filter_border_flags=flags, buffers=bufs, break_points=(break_x, None, None))
     case = Case(name="bl_cavity_%dx%d" % (nx, ny), nx=nx, ny=ny, nz=1, Re=Re, Ma=Ma, Pr=Pr, gamma=gamma, T0=T0,
                 X=X, Y=Y, Z=Z, mats=mats, bc=bc, flowRegion=fr, dxmin=_dxmin(X, Y, Z))
     if sfd:
@@ -714,21 +806,26 @@ def blasius_profile(eta_max=12.0, n=6001):
     return eta, sol[:, 0], sol[:, 1]
 
 
-def blasius_flow(case: Case, x0=1.0):
-    """Blasius base flow: u = f'(eta), v = (eta f' - f) / (2 sqrt(Re x)) with eta = y sqrt(Re / x)
-    and x measured from a virtual origin x0 upstream of the leading edge x = 0 (upstream of
-    it the leading-edge profile is repeated; below y = 0 the fluid is at rest); R = 1, E = E0."""
-    eta_t, f_t, fp_t = blasius_profile()
+def blasius_flow(case: Case):
+    """generateInitialFlow.m:53-103 ('blasius', no blasiusFit): R = 1, E = E0, V = W = 0;
+    U = 1 at x <= 0; at x > 0 the Blasius u(eta) with the momentum thickness
+    theta = 0.664 sqrt(x / Re) (the table's eta scaled by theta / 0.664155), U = 0 below
+    y = 0, U clipped at 1.  The Blasius table comes from RK4 shooting instead of ode45 and is
+    interpolated linearly instead of by splines (differences of order 1e-7 in the initial
+    field, which only seeds the run)."""
+    eta_t, _, fp_t = blasius_profile()
+    theta_bl = 0.664155332943009
     s = (case.nx, case.ny, case.nz)
-    x = np.maximum(case.X, 0.0)[:, None] + x0
-    eta = case.Y[None, :] * np.sqrt(case.Re / x)
-    eta = np.maximum(eta, 0.0)
-    f = np.where(eta <= eta_t[-1], np.interp(eta, eta_t, f_t), f_t[-1] + (eta - eta_t[-1]))
-    fp = np.interp(eta, eta_t, fp_t, right=1.0)
-    v = (eta * fp - f) / (2.0 * np.sqrt(case.Re * x))
+    U = np.ones((case.nx, case.ny))
+    for i, xi in enumerate(case.X):
+        if xi > 0:
+            theta = 0.664 * math.sqrt(xi / case.Re)
+            u = np.interp(case.Y * theta_bl / theta, eta_t, fp_t, left=0.0, right=1.0)
+            u[case.Y < 0] = 0.0
+            U[i] = u
+    U = np.minimum(U, 1.0)
     out = uniform_flow(case)
-    out["U"] = np.asfortranarray(np.repeat(fp[:, :, None], s[2], axis=2))
-    out["V"] = np.asfortranarray(np.repeat(v[:, :, None], s[2], axis=2))
+    out["U"] = np.asfortranarray(np.repeat(U[:, :, None], s[2], axis=2))
     return out
 
 

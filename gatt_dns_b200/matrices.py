@@ -609,18 +609,44 @@ def _regions_one_direction(fr_lines, n_along, periodic):
     return tmap, starts, ends
 
 
-def find_derivative_regions(flow_region, periodic=(False, False, False)):
+def _apply_break_points(tmap, starts, ends, break_points):
+    """Cut lines at break points (``findDerivativeRegions.m:45-60``, same for y and z).
+
+    Each break point row is ``[node, a_i, a_f, b_i, b_f]`` (1-based): the lines
+    ``tmap[a_i-1:a_f, b_i-1:b_f]`` get, per matrix type present there, a new type whose
+    boundary stencils are the old ones plus an end stencil at ``node`` and a start stencil
+    at ``node + 1`` -- the derivative and filter stencils do not reach across the break.
+    The new stencils are appended after the old ones, as the reference appends them.
+    """
+    for bp in np.atleast_2d(np.asarray(break_points, dtype=np.int64)):
+        node, ai, af, bi, bf = (int(v) for v in bp)
+        box = (slice(ai - 1, af), slice(bi - 1, bf))
+        for t in np.unique(tmap[box]):
+            t_new = int(tmap.max()) + 1
+            starts.append(list(starts[t - 1]) + [node + 1])
+            ends.append(list(ends[t - 1]) + [node])
+            sub = tmap[box]
+            sub[sub == t] = t_new
+            tmap[box] = sub
+    return tmap, starts, ends
+
+
+def find_derivative_regions(flow_region, periodic=(False, False, False), break_points=(None, None, None)):
     """Per-line matrix types from the flow-region mask (``source/findDerivativeRegions.m``).
 
     ``flow_region`` is a boolean (nx, ny, nz) array.  Returns a dict with
     ``typeMapX (ny,nz)``, ``typeMapY (nx,nz)``, ``typeMapZ (nx,ny)`` and the
-    start/end lists per type for each direction.
+    start/end lists per type for each direction.  ``break_points[d]`` restates
+    ``mesh.x/y/z.breakPoint`` (rows ``[node, line box]``, see :func:`_apply_break_points`).
     """
     fr = np.asarray(flow_region, dtype=bool)
     nx, ny, nz = fr.shape
     tx, sx, ex = _regions_one_direction(np.transpose(fr, (1, 2, 0)), nx, periodic[0])
     ty, sy, ey = _regions_one_direction(np.transpose(fr, (0, 2, 1)), ny, periodic[1])
     tz, sz, ez = _regions_one_direction(fr, nz, periodic[2])
+    for bp, (tm, st, en) in zip(break_points, ((tx, sx, ex), (ty, sy, ey), (tz, sz, ez))):
+        if bp is not None and len(bp):
+            _apply_break_points(tm, st, en, bp)
     return dict(typeMapX=tx, typeMapY=ty, typeMapZ=tz,
                 derivStartsX=sx, derivEndsX=ex, derivStartsY=sy, derivEndsY=ey,
                 derivStartsZ=sz, derivEndsZ=ez)
