@@ -1266,19 +1266,22 @@ int check_member(const gatt_ctx *c, int b)
 // allocation-free max-change: the accumulators live in a file-scope device array
 // ---------------------------------------------------------------------------
 
-// Every GPU that loads this library holds this array (2560 bytes) until the process
-// exits.  Host code must not pass the symbol itself to a kernel: it names a host-side
-// stand-in.  The device address comes from cudaGetSymbolAddress, once per device.
+// Every GPU that loads this library holds this array (160 x 8 = 1280 bytes) until the
+// process exits.  Host code must not pass the symbol itself to a kernel: it names a
+// host-side stand-in.  The device address comes from cudaGetSymbolAddress, once per device.
 static __device__ __align__(256) unsigned long long g_noalloc_maxchange[kMaxChangeSlots];
 
+namespace {
 constexpr int kMaxDevices = 64;
 unsigned long long *g_noalloc_ptr[kMaxDevices] = {};
+std::mutex g_noalloc_mu;  // guards the per-device address cache
 
 int noalloc_scratch(unsigned long long **out)
 {
     int dev = 0;
     CU(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return fail(GATT_ERR_BADARG, "device ordinal beyond the supported range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
     if (!g_noalloc_ptr[dev]) {
         void *p = nullptr;
         CU(cudaGetSymbolAddress(&p, g_noalloc_maxchange));
@@ -1287,6 +1290,7 @@ int noalloc_scratch(unsigned long long **out)
     *out = g_noalloc_ptr[dev];
     return GATT_OK;
 }
+}  // namespace
 
 // ---------------------------------------------------------------------------
 // Jacobian-free Arnoldi (calcInstability.m:304-400, first-order variant), nbatch problems
@@ -2500,6 +2504,13 @@ int gatt_max_change_noalloc(int nsets, int nvar, long long n, const double *cons
     if ((long long)nsets * nvar > kMaxChangeSlots)
         return fail(GATT_ERR_BADARG, "gatt_max_change_noalloc: nsets*nvar exceeds the " + std::to_string(kMaxChangeSlots) +
                                          " accumulators of its static scratch");
+    cudaStream_t st = (cudaStream_t)stream;
+    // the result comes back through a synchronised copy, which a capturing stream refuses
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CU(cudaStreamIsCapturing(st, &cap));
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(GATT_ERR_STATE, "gatt_max_change_noalloc: the stream is being captured; the call synchronises "
+                                    "it and returns host values, so it cannot run inside a capture");
     PtrSets ps;
     for (int k = 0; k < nsets * nvar; k++) {
         if (!a[k] || !b[k]) return fail(GATT_ERR_BADARG, "gatt_max_change_noalloc: null field pointer");
@@ -2508,12 +2519,11 @@ int gatt_max_change_noalloc(int nsets, int nvar, long long n, const double *cons
     }
     unsigned long long *acc = nullptr;
     TRY(noalloc_scratch(&acc));
-    cudaStream_t st = (cudaStream_t)stream;
     // the array keeps the previous call's maxima: start this call from zero
     CU(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * nsets * nvar, st));
-    int dev = 0, nsm = 148;
+    int dev = 0, nsm = 0;
     CU(cudaGetDevice(&dev));
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     long long g = (n + kBlock - 1) / kBlock;
     if (g > (long long)nsm * 8) g = (long long)nsm * 8;
     k_maxchange_sets<<<dim3((unsigned)g, nsets), kBlock, 0, st>>>(ps, nvar, acc, n);

@@ -237,17 +237,19 @@ const char *gatt_profile_name(int cls);
 
 /* Max-change residual that allocates nothing.  No counterpart in the reference (whose
  * max-change is the maxval reduction of main.F90:413-418): for callers that cannot call
- * cudaMalloc -- code running while a CUDA graph is being captured, inside a host callback,
- * or under an external allocator that owns all device memory -- and so cannot create a
- * context.  For set s < nsets and variable v < nvar, maxChange[s*nvar+v] =
- * max_i |a[s*nvar+v][i] - b[s*nvar+v][i]| over n points, where a and b are host arrays of
- * device pointers; a NaN difference yields NaN.  The work runs on `stream` (a
- * cudaStream_t, NULL = default stream) and the call returns after it finishes.
- * Limits: nvar <= 5 and nsets*nvar <= 160 (the accumulators are a 2560-byte static device
+ * cudaMalloc -- typically a host application whose own allocator owns all device memory
+ * and forbids further allocations -- and so cannot create a context, but hold the fields
+ * in device memory themselves.  For set s < nsets and variable v < nvar,
+ * maxChange[s*nvar+v] = max_i |a[s*nvar+v][i] - b[s*nvar+v][i]| over n points, where a and
+ * b are host arrays of device pointers; a NaN difference yields NaN.  The work runs on
+ * `stream` (a cudaStream_t, NULL = default stream) and the call synchronises it and
+ * returns the maxima in host memory; on a stream that is being captured it returns
+ * GATT_ERR_STATE without enqueuing anything.
+ * Limits: nvar <= 5 and nsets*nvar <= 160 (the accumulators are a 1280-byte static device
  * array that every GPU loading the library keeps until exit); larger requests return
  * GATT_ERR_BADARG.  The first call on a device looks up that array's address (the only
- * set-up, done once per device): make it before any stream capture.  All calls share the
- * array, so calls that overlap on the GPU race; each call clears its accumulators first. */
+ * set-up, done once per device under a lock).  All calls share the array, so calls that
+ * overlap on the GPU race; each call clears its accumulators first. */
 int gatt_max_change_noalloc(int nsets, int nvar, long long n, const double *const *a, const double *const *b,
                             double *maxChange, void *stream);
 

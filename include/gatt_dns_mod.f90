@@ -1,7 +1,7 @@
 ! gatt_dns_mod.f90 -- ISO_C_BINDING interface to the B200 hot-path library
 ! (include/gatt_dns.h).  A reference build adds this module to its makefile and calls
 ! these functions from main.F90 in place of RK4_2D/RK4_3D, applyFilters2D/3D, the SFD
-! block and applyBoundCond (see INTEGRATION.md).  Arrays are passed exactly as main.F90
+! block and applyBoundCond.  Arrays are passed exactly as main.F90
 ! already holds them (explicit-shape real*8 / integer arrays, column-major, 1-based
 ! indices inside index arrays).
 module gatt_dns

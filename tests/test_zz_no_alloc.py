@@ -1,10 +1,9 @@
 """The allocation-free max-change entry point (gatt_max_change_noalloc) against the
 max-change gatt_step reports, on two calls in a row.
 
-gatt_max_change_noalloc serves callers that cannot call cudaMalloc (graph capture in
-progress, host callbacks, an external allocator owning device memory): its accumulators
-live in a static device array shared by all calls, which it clears at the start of each
-call.  Two consecutive calls on different data therefore each return their own maxima.
+gatt_max_change_noalloc serves callers that cannot call cudaMalloc (a host application
+whose own allocator owns all device memory): its accumulators live in a static device
+array shared by all calls, which it clears at the start of each call.  Two consecutive calls on different data therefore each return their own maxima.
 This file is collected last so a stop-at-first-failure run has executed every other test.
 """
 import ctypes
@@ -70,3 +69,29 @@ def test_no_alloc_rejects_requests_beyond_its_scratch(cuda_lib):
     assert b"160" in cuda_lib.gatt_last_error()
     rc, mc = _noalloc(cuda_lib, sets[:32], sets[:32], 8)
     assert rc == 0 and np.all(mc == 0.0)
+
+
+def test_no_alloc_refuses_a_capturing_stream(cuda_lib):
+    """The call synchronises its stream and returns host values, so on a stream that is
+    being captured it must return GATT_ERR_STATE (6) before enqueuing anything."""
+    import torch
+    x = torch.ones(64, dtype=torch.float64, device="cuda")
+    y = torch.zeros(64, dtype=torch.float64, device="cuda")
+    rc, mc = _noalloc(cuda_lib, [[x]], [[y]], 64, nvar=1)  # first call: address set-up
+    assert rc == 0 and mc[0, 0] == 1.0
+    s = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        graph.capture_begin()
+        try:
+            a = (ctypes.c_void_p * 1)(x.data_ptr())
+            b = (ctypes.c_void_p * 1)(y.data_ptr())
+            out = np.zeros(1)
+            rc = cuda_lib.gatt_max_change_noalloc(1, 1, 64, a, b, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                  ctypes.c_void_p(s.cuda_stream))
+        finally:
+            graph.capture_end()
+    assert rc == 6
+    assert b"captured" in cuda_lib.gatt_last_error()
+    rc, mc = _noalloc(cuda_lib, [[x]], [[y]], 64, nvar=1)  # still usable afterwards
+    assert rc == 0 and mc[0, 0] == 1.0
