@@ -602,45 +602,6 @@ def cavity_channel(nx=96, ny=64, nz=1, Re=1000.0, Ma=0.5, Pr=0.71, gamma=1.4, T0
     return case
 
 
-def boundary_layer(nx=400, ny=150, nz=64, Lx=6.0, Ly=5.0, Lz=1.0, Re=1000.0, Ma=0.5, Pr=0.71, gamma=1.4,
-                   T0=300.0, filter_alpha=0.49, deriv="SL4", ny_stretch=1.5):
-    """3-D compressible boundary layer over an isothermal flat plate, spanwise periodic.
-
-    The boundary set of source/boundaries/boundaryLayerIsothermal.m for a domain starting
-    at the plate's leading edge (mesh.X(1) = 0): inflow u = 1, v = w = 0, e = E0 with
-    pressure Neumann (:4-66); outflow null second derivatives of u, v, w, e and p = P0
-    (:83-145); outer flow null second derivatives of u, v, w, e, p (:146-207); the plate
-    (j = 1) from findWallsForBoundaries with the wall list of lidDrivenFlow.m (no-slip,
-    e = E0, pressure Neumann).  y is tanh-clustered at the plate; z is periodic.
-    """
-    X = generate_mesh(0.0, Lx, nx)
-    Y = generate_mesh(0.0, Ly, ny, mtype="tanh", par=ny_stretch, local="i")
-    Z = generate_mesh(0.0, Lz, nz, periodic=True, fix_periodic_domain_size=True)
-    fr = np.ones((nx, ny, nz), dtype=bool)
-    fr[:, 0, :] = False
-    fr, walls, corners, inside = find_walls_for_boundaries(fr)
-    E0 = 1.0 / ((gamma ** 2 - gamma) * Ma ** 2)
-    P0 = (gamma - 1) * E0
-    items = wall_boundary_list(walls, inside, P0, E0)
-    inflow = [1, 1, 2, ny, 1, nz]
-    for v, val in (("u", 1.0), ("v", 0.0), ("w", 0.0), ("e", E0)):
-        items.append((v, "dir", "xi", val, list(inflow)))
-    items.append(("p", "neu", "xi", 0.0, list(inflow)))
-    outflow = [nx, nx, 2, ny, 1, nz]
-    for v in ("u", "v", "w", "e"):
-        items.append((v, "sec", "xf", 0.0, list(outflow)))
-    items.append(("p", "dir", "xf", P0, list(outflow)))
-    top = [1, nx, ny, ny, 1, nz]
-    for v in ("u", "v", "w", "e", "p"):
-        items.append((v, "sec", "yf", 0.0, list(top)))
-    n1, n2 = mx.neumann_coefficients(6, 2)
-    bc = init_boundaries(items, corners, mx.fortran_round(n1), mx.fortran_round(n2))
-    mats = build_matrices(X, Y, Z, fr, (False, False, True), (False, False, True), (Lx, Ly, Lz),
-                          deriv=deriv, filter_alpha=filter_alpha, filter_borders="decentered")
-    return Case(name="boundary_layer_%dx%dx%d" % (nx, ny, nz), nx=nx, ny=ny, nz=nz, Re=Re, Ma=Ma, Pr=Pr,
-                gamma=gamma, T0=T0, X=X, Y=Y, Z=Z, mats=mats, bc=bc, flowRegion=fr, dxmin=_dxmin(X, Y, Z))
-
-
 def sfd_region(shape, buffers, X):
     """calcSFDregion.m:4-53 with applyX/Y/Z = 2: X * (1 - prod of 0.5 - 0.5 cos ramps over the
     buffer zones); buffers[d] = (n initial, n final) buffer nodes of direction d."""
@@ -657,22 +618,16 @@ def sfd_region(shape, buffers, X):
     return np.asfortranarray(X * (1.0 - chi))
 
 
-def boundary_layer_cavity(nx=800, ny=300, Re=1000.0, Ma=0.5, Pr=0.71, gamma=1.4, T0=300.0, filter_alpha=0.49,
-                          deriv="SL4", cavity=(1.0, 2.0), buffers=((40, 30), (0, 40)),
-                          sfd=(0.02, 15.0), x_range=(-1.0, 5.0)):
-    """2-D compressible boundary layer over a rectangular cavity with buffer zones and SFD.
-
-    Domain x in [-1, 5], y in [-1, 4] (physical part), cavity of depth 1 at 1 < x < 2, the
-    buffer zones of parameters.m:124-142 (sigmoid; inflow 40, outflow 30 and top 40 nodes
-    in the full case) with EX4 derivatives inside them, the filter borders of
-    parameters.m:182-186 (reduced order, no filter on the first and last five x nodes nor
-    on the last five y nodes) and SFD type 2 on the buffer ramps (calcSFDregion.m), X and
-    Delta from `sfd`.  nx, ny count all nodes, buffers included.
+def boundary_layer_isothermal(nx, ny, nz=1, Re=1000.0, Ma=0.5, Pr=0.71, gamma=1.4, T0=300.0, filter_alpha=0.49,
+                              deriv="SL4", cavity=None, buffers=((0, 0), (0, 0)), sfd=None, x_range=(-1.0, 5.0),
+                              y_top=4.0, Lz=1.0, name=None):
+    """Compressible boundary layer over an isothermal plate at y = 0, with an optional
+    rectangular cavity of depth 1 at cavity = (x0, x1); 2-D (nz = 1) or spanwise periodic.
 
     The boundary set is boundaryLayerIsothermal.m's for mesh.X(1) < 0, in its order:
     * Dirichlet inflow u = 1, v = w = 0, e = E0 and pressure Neumann over the whole x = X(1)
       plane (:4-78), outflow null second derivatives with p = P0 (:80-138), outer flow null
-      second derivatives (:141-201);
+      second derivatives (:141-201); z is periodic, so :203-315 add nothing;
     * the flow region: solid at and below the row nearest y = 0, the cavity carved out
       (:317-344), walls, corners and wall interiors from findWallsForBoundaries;
     * the free-slip wall (:362-369): every up-facing wall is moved to start at the first node
@@ -681,27 +636,36 @@ def boundary_layer_cavity(nx=800, ny=300, Re=1000.0, Ma=0.5, Pr=0.71, gamma=1.4,
       findDerivativeRegions.m:45-60);
     * pressure Neumann on every wall (:371-405), u and w Neumann on the free-slip wall
       (:407-431), then p = P0, u = v = w = 0, e = E0 on every solid node (:433-497).
+
+    Meshes follow parameters.m:84-147 ('attractors', matchFixed = 2, sigmoid buffer zones)
+    scaled to this domain: in x a point attractor at the leading edge (the reference's
+    domain starts there) and, with a cavity, a region of strength 3 around it; in y the
+    region [-2D, -D/10, D/10, 2 delta99] of strength 12 with delta99 = 5 sqrt(xEnd / Re) at
+    the outflow (D = 1 with a cavity, 0 without); fixed points (meshAddFixedPoints.m:3-10)
+    at the leading edge and the cavity's edges and bottom.  The filter borders are those of
+    parameters.m:182-186 (reduced order, no filter on the first and last five x nodes nor on
+    the last five y nodes).  With ``sfd = (X, Delta)``, SFD type 2 on the buffer ramps
+    (calcSFDregion.m).  nx, ny count all nodes, buffers included.
     """
     (bxi, bxf), (byi, byf) = buffers
     sig = lambda n, st: {"n": n, "type": "sigmoid", "stretching": st, "transition": 0.2}
-    x0, x1 = cavity
-    # meshes of parameters.m:84-115 ('attractors', matchFixed = 2) scaled to this domain: in
-    # x a region of strength 3 around the cavity and a point attractor at the leading edge
-    # (the reference's domain starts there); in y the region [-2D, -D/10, D/10, 2 delta99]
-    # of strength 12 with delta99 = 5 sqrt(xEnd / Re) at the outflow; fixed points
-    # (meshAddFixedPoints.m:3-10) at the leading edge, the cavity edges and its bottom
+    depth = 1.0 if cavity else 0.0
+    xf_pts = (0.0,) + (tuple(cavity) if cavity else ())
+    x_regions = [(cavity[0] - 0.5, cavity[0] - 0.25, cavity[1] + 0.25, cavity[1] + 0.5, 3.0)] if cavity else []
     X = generate_mesh(x_range[0], x_range[1], nx - bxi - bxf, mtype="attractors",
-                      attractor_points=[(0.0, 2.0, 0.1)],
-                      attractor_regions=[(x0 - 0.5, x0 - 0.25, x1 + 0.25, x1 + 0.5, 3.0)],
+                      attractor_points=[(0.0, 2.0, 0.1)], attractor_regions=x_regions,
                       buffer_i=sig(bxi, 30) if bxi else None, buffer_f=sig(bxf, 15) if bxf else None,
-                      fix_points=(0.0, x0, x1))
+                      fix_points=xf_pts)
     d99 = 5.0 * math.sqrt(x_range[1] / Re)
-    Y = generate_mesh(-1.0, 4.0, ny - byi - byf, mtype="attractors",
-                      attractor_regions=[(-2.0, -0.1, 0.1, 2.0 * d99, 12.0)],
+    Y = generate_mesh(-depth, y_top, ny - byi - byf, mtype="attractors",
+                      attractor_regions=[(-2.0 * depth if depth else -2.0, -depth / 10 if depth else -1.0,
+                                          depth / 10, 2.0 * d99, 12.0)],
                       buffer_i=sig(byi, 30) if byi else None, buffer_f=sig(byf, 30) if byf else None,
-                      fix_points=(-1.0, 0.0))
-    Z = np.array([0.0])
-    nz = 1
+                      fix_points=(-depth, 0.0) if depth else (0.0,))
+    if nz > 1:
+        Z = generate_mesh(0.0, Lz, nz, periodic=True, fix_periodic_domain_size=True)
+    else:
+        Z = np.array([0.0])
     E0 = 1.0 / ((gamma ** 2 - gamma) * Ma ** 2)
     P0 = (gamma - 1) * E0
     items = []
@@ -720,13 +684,14 @@ def boundary_layer_cavity(nx=800, ny=300, Re=1000.0, Ma=0.5, Pr=0.71, gamma=1.4,
     top = [1, nx, ny, ny, 1, nz]
     for v in ("u", "v", "w", "e", "p"):
         items.append((v, "sec", "yf", 0.0, list(top)))
-    # flow region (:317-344): the plate, then the cavity (open interval in x and y)
+    # flow region (:317-344): the plate, then the cavity (open intervals in x and y)
     fr = np.ones((nx, ny, nz), dtype=bool)
     wall_j = int(np.argmin(np.abs(Y))) + 1
     fr[:, :wall_j, :] = False
-    in_x = (X > x0) & (X < x1)
-    in_y = (Y > -1.0) & (Y < 0.0)
-    fr[np.ix_(in_x, in_y, np.ones(nz, dtype=bool))] = True
+    if cavity:
+        in_x = (X > cavity[0]) & (X < cavity[1])
+        in_y = (Y > -depth) & (Y < 0.0)
+        fr[np.ix_(in_x, in_y, np.ones(nz, dtype=bool))] = True
     fr, walls, corners, inside = find_walls_for_boundaries(fr)
     # free-slip wall and the break point (:362-369)
     break_x = None
@@ -758,18 +723,38 @@ def boundary_layer_cavity(nx=800, ny=300, Re=1000.0, Ma=0.5, Pr=0.71, gamma=1.4,
     n1, n2 = mx.neumann_coefficients(6, 2)
     bc = init_boundaries(items, corners, mx.fortran_round(n1), mx.fortran_round(n2))
     bufs = [{"i": sig(bxi, 30) if bxi else {"n": 0}, "f": sig(bxf, 15) if bxf else {"n": 0}},
-            {"i": {"n": 0}, "f": sig(byf, 30) if byf else {"n": 0}},
+            {"i": sig(byi, 30) if byi else {"n": 0}, "f": sig(byf, 30) if byf else {"n": 0}},
             {"i": {"n": 0}, "f": {"n": 0}}]
     flags = {"filterBordersStartX": False, "filterBordersEndX": False, "filterBordersEndY": False}
-    mats = build_matrices(X, Y, Z, fr, (False, False, False), (False, False, False), (6.0, 5.0, 1.0),
-                          deriv=deriv, deriv_buffer="EX4", filter_alpha=filter_alpha, filter_borders="reducedOrder",
-                          filter_border_flags=flags, buffers=bufs, break_points=(break_x, None, None))
-    case = Case(name="bl_cavity_%dx%d" % (nx, ny), nx=nx, ny=ny, nz=1, Re=Re, Ma=Ma, Pr=Pr, gamma=gamma, T0=T0,
-                X=X, Y=Y, Z=Z, mats=mats, bc=bc, flowRegion=fr, dxmin=_dxmin(X, Y, Z))
+    mats = build_matrices(X, Y, Z, fr, (False, False, True), (False, False, True),
+                          (x_range[1], y_top, Lz), deriv=deriv, deriv_buffer="EX4", filter_alpha=filter_alpha,
+                          filter_borders="reducedOrder", filter_border_flags=flags, buffers=bufs,
+                          break_points=(break_x, None, None))
+    case = Case(name=name or "bl_%dx%dx%d" % (nx, ny, nz), nx=nx, ny=ny, nz=nz, Re=Re, Ma=Ma, Pr=Pr, gamma=gamma,
+                T0=T0, X=X, Y=Y, Z=Z, mats=mats, bc=bc, flowRegion=fr, dxmin=_dxmin(X, Y, Z))
     if sfd:
         case.sfd_type, case.sfd_X, case.sfd_delta = 2, sfd[0], sfd[1]
-        case.sfd_chi = sfd_region((nx, ny, 1), ((bxi, bxf), (byi, byf), (0, 0)), sfd[0])
+        case.sfd_chi = sfd_region((nx, ny, nz), ((bxi, bxf), (byi, byf), (0, 0)), sfd[0])
     return case
+
+
+def boundary_layer_cavity(nx=800, ny=300, nz=1, buffers=((40, 30), (0, 40)), sfd=(0.02, 15.0), **kw):
+    """Config 3: the 2-D boundary layer over a cavity of depth 1 and length 1 at 1 < x < 2,
+    x in [-1, 5] and y in [-1, 4] (physical part), Re 1000, Ma 0.5, with the buffer zones of
+    parameters.m:124-142 (inflow 40, outflow 30 and top 40 nodes in the full case), EX4
+    derivatives inside them and SFD (X 0.02, Delta 15) on their ramps; see
+    :func:`boundary_layer_isothermal`.  nz > 1 gives the spanwise-periodic 3-D version."""
+    kw.setdefault("cavity", (1.0, 2.0))
+    c = boundary_layer_isothermal(nx, ny, nz, buffers=buffers, sfd=sfd, **kw)
+    c.name = "bl_cavity_%dx%d" % (nx, ny) + ("x%d" % nz if nz > 1 else "")
+    return c
+
+
+def boundary_layer(nx=400, ny=150, nz=64, **kw):
+    """Config 5: the 3-D spanwise-periodic boundary layer over a flat plate (no cavity, no
+    buffer zones, no SFD), x in [-1, 5], y in [0, 4], z in [0, 1); see
+    :func:`boundary_layer_isothermal`."""
+    return boundary_layer_isothermal(nx, ny, nz, name="boundary_layer_%dx%dx%d" % (nx, ny, nz), **kw)
 
 
 def blasius_profile(eta_max=12.0, n=6001):

@@ -193,6 +193,54 @@ def test_lid_driven_100_steps(libs):
     g.close()
 
 
+def _long_case(name):
+    """Cases for the 100-step comparison (each stable over the run on its grid)."""
+    if name == "box":
+        c = cs.periodic_box(n=32)
+        return c, cs.solenoidal_turbulence(c, seed=7)
+    if name == "bl":
+        c = cs.boundary_layer(nx=128, ny=64, nz=8, buffers=((10, 8), (0, 10)))
+    elif name == "bl_cavity3d":
+        c = cs.boundary_layer_cavity(nx=160, ny=64, nz=8, buffers=((10, 8), (0, 10)))
+    else:
+        c = cs.boundary_layer_cavity(nx=96, ny=48, buffers=((8, 6), (0, 8)))
+    f = cs.blasius_flow(c)
+    if c.is3d:  # a small spanwise-varying disturbance so that every direction carries work
+        r = cs.random_flow(c, seed=3, amp=0.01)
+        for k in ("U", "V", "W"):
+            f[k] = np.asfortranarray(f[k] + r[k])
+    return c, f
+
+
+@pytest.mark.parametrize("name", ["box", "bl", "bl_cavity3d", "bl_cavity"])
+def test_100_steps(libs, name):
+    """100 RK4 steps at CFL 0.5 against the oracle at 1e-9: the 3-D periodic turbulence box,
+    the 3-D boundary layer with its free-slip upstream wall and break point, the 3-D and
+    2-D boundary layers over a cavity with SFD in the buffer zones."""
+    from gatt_dns_b200.solver import GattDNS
+    from oracle import Oracle
+    c, f = _long_case(name)
+    o = Oracle(c)
+    f = o.apply_bound_cond(f, 0.0)
+    dt = c.cfl_dt(f["U"], f["V"], f["W"], 0.5)
+    st = o.new_state(f)
+    for s in range(100):
+        mo = o.step(st, s * dt, dt)
+    g = GattDNS(c)
+    g.upload(f)
+    mg = g.run(100, 0.0, dt)[0]
+    a = g.download()
+    assert np.all(np.isfinite(mg))
+    assert np.allclose(mg, mo, rtol=1e-7, atol=1e-14), (name, mg, mo)
+    for k in fields(c):
+        assert rel(a[k], st[k]) < LONG_TOL, (name, k, rel(a[k], st[k]))
+    if c.sfd_type:
+        m = g.download_mean()
+        for k in fields(c):
+            assert rel(m[k], st["m" + k]) < LONG_TOL, (name, "mean", k)
+    g.close()
+
+
 def test_batched_members_match_single_runs(libs):
     from gatt_dns_b200.solver import GattDNS
     c = get_case("box")
@@ -285,6 +333,27 @@ def test_full_size_box_one_step(libs):
     b = g.download()
     assert abs(np.sum(b["R"]) - m0) / m0 < 1e-12
     g.close()
+
+
+def test_full_size_box_ten_steps(libs):
+    """128^3 periodic box (the bench workload): ten steps against the oracle."""
+    from gatt_dns_b200.solver import GattDNS
+    from oracle import Oracle
+    c = cs.periodic_box(n=128)
+    f = cs.solenoidal_turbulence(c, seed=1234)
+    dt = c.cfl_dt(f["U"], f["V"], f["W"], 0.5)
+    g = GattDNS(c)
+    g.upload(f)
+    mg = g.run(10, 0.0, dt)[0]
+    a = g.download()
+    g.close()
+    o = Oracle(c)
+    st = o.new_state(f)
+    for s in range(10):
+        mo = o.step(st, s * dt, dt)
+    assert np.allclose(mg, mo, rtol=1e-9)
+    for k in KEYS:
+        assert rel(a[k], st[k]) < 1e-10, (k, rel(a[k], st[k]))
 
 
 def test_errors_are_reported(libs):
