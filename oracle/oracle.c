@@ -106,7 +106,22 @@ void orc_solve(const orc_case *c, int dir, int kind, const double *F, double *dF
 /* Navier-Stokes right-hand side: nseq.F90:10-323                             */
 /* ------------------------------------------------------------------------- */
 
-static double *alloc_field(long n) { return (double *)malloc(sizeof(double) * (size_t)n); }
+/* Work arrays: the Fortran keeps its temporaries as automatic arrays, so a call pays no
+ * allocation or first-touch cost after the first one.  Each call site owns fixed slots of a
+ * persistent pool that grows to the largest grid seen (the oracle is not re-entrant). */
+enum { SLOT_NSEQ = 0, SLOT_RK = 40, SLOT_BC = 50, SLOT_FILTER = 51, SLOT_STEP = 52, NSLOTS = 56 };
+static double *g_pool[NSLOTS];
+static long g_pool_n[NSLOTS];
+
+static double *work_field(int slot, long n)
+{
+    if (g_pool_n[slot] < n) {
+        free(g_pool[slot]);
+        g_pool[slot] = (double *)malloc(sizeof(double) * (size_t)n);
+        g_pool_n[slot] = n;
+    }
+    return g_pool[slot];
+}
 
 static void nseq2d(const orc_case *c, const double *U, const double *V, const double *R,
                    const double *E, double *dU, double *dV, double *dR, double *dE)
@@ -115,7 +130,7 @@ static void nseq2d(const orc_case *c, const double *U, const double *V, const do
     const double g = c->gamma, Re = c->Re, Ma = c->Ma, Pr = c->Pr, T0 = c->T0;
     enum { DUx, DVx, DRx, DEx, DUy, DVy, DRy, DEy, TXX, TYY, TXY, DTXYX, DTXYY, DTXXX, DTYYY, QX, QY, HTX, HTY, MU, NT };
     double *w[NT];
-    for (int k = 0; k < NT; k++) w[k] = alloc_field(n);
+    for (int k = 0; k < NT; k++) w[k] = work_field(SLOT_NSEQ + k, n);
     /* calcDerivsXY of U, V, R, E (nseq.F90:43-69) */
     orc_solve(c, 0, 0, U, w[DUx]); orc_solve(c, 1, 0, U, w[DUy]);
     orc_solve(c, 0, 0, V, w[DVx]); orc_solve(c, 1, 0, V, w[DVy]);
@@ -157,7 +172,6 @@ static void nseq2d(const orc_case *c, const double *U, const double *V, const do
               + (-P * (dux + dvy) + w[TXX][p] * dux + w[TYY][p] * dvy + w[TXY][p] * (dvx + duy)
                  - w[HTX][p] - w[HTY][p]) / R[p];
     }
-    for (int k = 0; k < NT; k++) free(w[k]);
 }
 
 static void nseq3d(const orc_case *c, const double *U, const double *V, const double *W,
@@ -170,7 +184,7 @@ static void nseq3d(const orc_case *c, const double *U, const double *V, const do
            TXX, TYY, TZZ, TXY, TXZ, TYZ, QX, QY, QZ,
            DTXYX, DTXYY, DTXZX, DTXZZ, DTYZY, DTYZZ, DTXXX, DTYYY, DTZZZ, HTX, HTY, HTZ, NT };
     double *w[NT];
-    for (int k = 0; k < NT; k++) w[k] = alloc_field(n);
+    for (int k = 0; k < NT; k++) w[k] = work_field(SLOT_NSEQ + k, n);
     const double *in[5] = {U, V, W, R, E};
     /* calcDerivsXYZ of U, V, W, R, E (nseq.F90:178-216) */
     for (int f = 0; f < 5; f++)
@@ -225,7 +239,6 @@ static void nseq3d(const orc_case *c, const double *U, const double *V, const do
                  + w[TXY][p] * (dvx + duy) + w[TXZ][p] * (dwx + duz) + w[TYZ][p] * (dwy + dvz)
                  - w[HTX][p] - w[HTY][p] - w[HTZ][p]) / R[p];
     }
-    for (int k = 0; k < NT; k++) free(w[k]);
 }
 
 void orc_nseq(const orc_case *c, const double *U, const double *V, const double *W,
@@ -341,7 +354,7 @@ void orc_apply_bc(const orc_case *c, double *U, double *V, double *W, double *R,
     const long n = (long)c->nx * c->ny * c->nz;
     double *F[5] = {U, V, W, NULL, E};
     const double g = c->gamma;
-    double *P = alloc_field(n);
+    double *P = work_field(SLOT_BC, n);
     const int NL = c->neumannLength, N2 = c->neumann2Length;
     /* Dirichlet: nseq.F90:357-373 (U, V, W, E, then P) */
     const int dorder[4] = {0, 1, 2, 4};
@@ -425,7 +438,6 @@ void orc_apply_bc(const orc_case *c, double *U, double *V, double *W, double *R,
         if (c->distType[d] == 1)
             lid_driven(c, vars[c->distVar[d]], b, c->distX + c->distXoff[d], c->distPar[d]);
     }
-    free(P);
 }
 
 /* ------------------------------------------------------------------------- */
@@ -441,7 +453,7 @@ void orc_rk4(const orc_case *c, const double *U, const double *V, double *W, con
     const double *q0[5] = {U, V, is3d ? W : NULL, R, E};
     double *qn[5] = {Un, Vn, is3d ? Wn : NULL, Rn, En};
     double *k[5], *delta[5];
-    for (int f = 0; f < 5; f++) { k[f] = alloc_field(n); delta[f] = alloc_field(n); }
+    for (int f = 0; f < 5; f++) { k[f] = work_field(SLOT_RK + f, n); delta[f] = work_field(SLOT_RK + 5 + f, n); }
     /* In 2-D, the stage inputs carry the caller's W (RK4_2D passes W to applyBoundCond). */
     double *Wst = is3d ? Wn : W;
     /* Step 1 */
@@ -475,7 +487,6 @@ void orc_rk4(const orc_case *c, const double *U, const double *V, double *W, con
         }
     }
     orc_apply_bc(c, Un, Vn, Wst, Rn, En, t + dt);
-    for (int f = 0; f < 5; f++) { free(k[f]); free(delta[f]); }
 }
 
 /* ------------------------------------------------------------------------- */
@@ -487,7 +498,7 @@ void orc_filters(const orc_case *c, double *U, double *V, double *W, double *R, 
     const long n = (long)c->nx * c->ny * c->nz;
     const int is3d = c->nz > 1;
     double *f[5] = {U, V, W, R, E};
-    double *tmp = alloc_field(n);
+    double *tmp = work_field(SLOT_FILTER, n);
     const int ndir = is3d ? 3 : 2;
     for (int d = 0; d < ndir; d++) {
         if (!c->filterDir[d]) continue;
@@ -501,7 +512,6 @@ void orc_filters(const orc_case *c, double *U, double *V, double *W, double *R, 
             memcpy(f[q], tmp, sizeof(double) * (size_t)n);
         }
     }
-    free(tmp);
 }
 
 /* ------------------------------------------------------------------------- */
@@ -514,7 +524,8 @@ void orc_step(const orc_case *c, double *U, double *V, double *W, double *R, dou
 {
     const long n = (long)c->nx * c->ny * c->nz;
     const int is3d = c->nz > 1;
-    double *Un = alloc_field(n), *Vn = alloc_field(n), *Rn = alloc_field(n), *En = alloc_field(n);
+    double *Un = work_field(SLOT_STEP, n), *Vn = work_field(SLOT_STEP + 1, n), *Rn = work_field(SLOT_STEP + 2, n),
+           *En = work_field(SLOT_STEP + 3, n);
     orc_rk4(c, U, V, W, R, E, Un, Vn, Wn, Rn, En, t, dt);
     /* main.F90:357-378 -- the filter receives dt/FilterCharTime */
     orc_filters(c, Un, Vn, Wn, Rn, En, dt / c->filterCharTime);
@@ -542,10 +553,16 @@ void orc_step(const orc_case *c, double *U, double *V, double *W, double *R, dou
     for (int q = 0; q < 5; q++) {
         /* any NaN makes the result NaN, so a divergence is never masked */
         double m = 0;
-        for (long p = 0; p < n; p++) {
-            double d = fabs(a[q][p] - b[q][p]);
-            if (d > m || d != d) m = d;
-            if (m != m) break;
+        #pragma omp parallel
+        {
+            double mt = 0;
+            #pragma omp for schedule(static) nowait
+            for (long p = 0; p < n; p++) {
+                double d = fabs(a[q][p] - b[q][p]);
+                if (d > mt || d != d) mt = d;
+            }
+            #pragma omp critical
+            if (mt > m || mt != mt) m = (m != m) ? m : mt;
         }
         maxChange[q] = m;
     }
@@ -555,5 +572,4 @@ void orc_step(const orc_case *c, double *U, double *V, double *W, double *R, dou
     memcpy(R, Rn, sizeof(double) * (size_t)n);
     memcpy(E, En, sizeof(double) * (size_t)n);
     if (is3d) memcpy(W, Wn, sizeof(double) * (size_t)n);
-    free(Un); free(Vn); free(Rn); free(En);
 }
