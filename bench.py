@@ -37,11 +37,10 @@ BYTES_PER_POINT_STAGE = 27 * 16 + 5 * 32 + 15 * 16 / 4
 # (stages 2-4; in stage 1 it is the stage input), RK increment read 5 (stages 2-4) and
 # written 5 (stages 1-3).  Stages 1..4: 42, 52, 52, 47 fields; mean 48.25.
 ASSEMBLE_FIELDS = (5 + 15 + 12 + 5) + 3 * (3 * 5) / 4.0
-# DRAM traffic of the assembly from ncu (profiles/k_assemble3d_pipe_periodic_box_128.md): a
-# stage-3 launch moved 849.7 MB (read 704.7 + write 145.0; part of the output is still in L2
-# when it ends) for 52 algorithmic fields of 128^3 points (872.4 MB); scaled to the
-# four-stage mean by algorithmic fields, for n = 128 only.
-ASSEMBLE_TRAFFIC_STAGE3_128 = 849.7e6
+# DRAM bytes per launch of each kernel function from an ncu capture of this workload
+# (dram__bytes_read.sum + dram__bytes_write.sum), one "traffic <function> <bytes>" line per
+# function; written by hand from the capture, with the capture's command in the file.
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dram_traffic_periodic_box_128.txt")
 
 
 def parse():
@@ -182,20 +181,38 @@ def cpu_baseline_sample(c, seconds=10.0):
         if el > seconds or n >= 20:
             break
     v = c.npts * STAGES * n / el / 1e6
-    return {"value": v, "unit": "Mpoint-stages/s", "cores": o.lib.orc_num_threads(), "kind": "port",
+    cores = o.lib.orc_num_threads()
+    # one core: two steps (about 15 s on this grid)
+    o.lib.orc_set_threads(1)
+    t0 = time.perf_counter()
+    for k in range(2):
+        o.step(st, (n + k) * dt, dt)
+    el1 = time.perf_counter() - t0
+    o.lib.orc_set_threads(cores)
+    v1 = c.npts * STAGES * 2 / el1 / 1e6
+    return {"value": v, "unit": "Mpoint-stages/s", "cores": cores, "kind": "port",
             "sample": "%d full RK4 steps of the %d^3 box in %.1f s (C restatement of the reference Fortran, "
-                      "OpenMP over lines)" % (n, c.nx, el)}
+                      "OpenMP over lines; work arrays kept across calls like the Fortran's)" % (n, c.nx, el),
+            "one_core": {"value": v1, "unit": "Mpoint-stages/s", "cores": 1,
+                         "sample": "2 full RK4 steps of the %d^3 box in %.1f s" % (c.nx, el1)},
+            "host": host_cpu()}
 
 
-def arnoldi_sample(cs, GattDNS, case, base, members, m, nsteps, seed, label):
-    """Batched vs serial Jacobian-free Arnoldi on one GPU (bounded sample).
+def arnoldi_sample(cs, GattDNS, case, base, members, m, nsteps, seed, label, dist=None):
+    """Batched vs serial Jacobian-free Arnoldi (bounded sample).
 
-    Batched: one context of `members` members, one gatt_arnoldi call (every kernel launch
-    covers all members).  Serial: one single-member context reused for the same problems one
-    after another.  Both include the host<->device transfers of the calls; each side's
-    graphs are captured in an untimed warm-up call first.
+    Batched: one context holding this rank's share of the `members` problems, one
+    gatt_arnoldi call (every kernel launch covers all of them).  Serial: one single-member
+    context reused for the same problems one after another.  Both include the host<->device
+    transfers of the calls; each side's graphs are captured in an untimed warm-up call first.
+    Times are CUDA events on the contexts' stream; with several ranks (torch.distributed
+    initialised) the problems are sharded across ranks (shard.arnoldi_sharded, no data-path
+    collective: the ranks gather H at the end) and each time is the max over ranks.
     """
     import torch
+    from gatt_dns_b200.shard import arnoldi_sharded, max_over_ranks, member_range
+    world = dist.get_world_size() if dist is not None else 1
+    rank = dist.get_rank() if dist is not None else 0
     rng = np.random.default_rng(seed)
     s = (case.nx, case.ny, case.nz)
     v0 = []
@@ -204,36 +221,51 @@ def arnoldi_sample(cs, GattDNS, case, base, members, m, nsteps, seed, label):
         d["U"][...] = 1e-6 * rng.standard_normal(s)
         d["V"][...] = 1e-6 * rng.standard_normal(s)
         v0.append(d)
+    lo, hi = member_range(members, world, rank)
+    mine = hi - lo
     dt = case.cfl_dt(base["U"], base["V"], base["W"], 0.5)
-    gb = GattDNS(case, nbatch=members)
-    gb.arnoldi(base, v0, 1, 1, dt)                      # warm-up: graph capture, buffers
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    Hb = gb.arnoldi(base, v0, m, nsteps, dt)
-    torch.cuda.synchronize()
-    tb = time.perf_counter() - t0
-    step_b = time_steps(gb, dt, 10) / members          # ms per member-step, batched
+    stream = torch.cuda.Stream()
+
+    def timed(fn):
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return out, max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, device="cuda")
+
+    gb = GattDNS(case, nbatch=mine, stream=stream.cuda_stream)
+    gb.arnoldi(base, v0[lo:hi], 1, 1, dt)               # warm-up: graph capture, buffers
+    Hb, tb = timed(lambda: arnoldi_sharded(lambda v: gb.arnoldi(base, v, m, nsteps, dt), v0, dist, device="cuda"))
+    step_b = time_steps(gb, dt, 10) / mine              # ms per member-step, batched
     gb.close()
-    g1 = GattDNS(case, nbatch=1)
-    g1.arnoldi(base, v0[:1], 1, 1, dt)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    same = True
-    for b in range(members):
-        Hs = g1.arnoldi(base, [v0[b]], m, nsteps, dt)[0]
-        same = same and bool(np.array_equal(Hs, Hb[b]))
-    torch.cuda.synchronize()
-    ts = time.perf_counter() - t0
+    g1 = GattDNS(case, nbatch=1, stream=stream.cuda_stream)
+    g1.arnoldi(base, v0[lo:lo + 1], 1, 1, dt)
+
+    def serial():
+        return [g1.arnoldi(base, [v0[b]], m, nsteps, dt)[0] for b in range(lo, hi)]
+
+    Hs, ts = timed(serial)
+    same = all(bool(np.array_equal(Hs[i], Hb[lo + i])) for i in range(mine))
+    if dist is not None:
+        flag = torch.tensor([1.0 if same else 0.0], device="cuda")
+        dist.all_reduce(flag, op=dist.ReduceOp.MIN)
+        same = bool(flag.item() == 1.0)
     step_1 = time_steps(g1, dt, 10)                    # ms per step, one member
     g1.close()
-    return {"workload": label, "members": members, "krylov_steps": m, "rk4_steps_per_run": nsteps,
-            "runs_per_member": m + 1, "batched_s": tb, "serial_s": ts, "serial_over_batched": ts / tb,
-            "H_batched_equals_serial": same,
+    return {"workload": label, "members": members, "ranks": world, "members_per_rank": mine, "krylov_steps": m,
+            "rk4_steps_per_run": nsteps, "runs_per_member": m + 1, "batched_s": tb, "serial_s": ts,
+            "serial_over_batched": ts / tb, "H_batched_equals_serial": same,
             "rk4_step_ms_per_member_batched": step_b, "rk4_step_ms_single": step_1,
             "full_config_serial_over_batched_est": step_1 / step_b,
             "sample": "%d Krylov steps of %d RK4 steps each (plus the base run) per problem; the full "
                       "config runs 32 Krylov steps of 500, where the RK4 steps dominate: its ratio is "
-                      "estimated from the time per member-step (10 synchronised steps)" % (m, nsteps)}
+                      "estimated from the time per member-step (10 synchronised steps)%s" % (
+                          m, nsteps, "; problems sharded over %d ranks, times max over ranks" % world
+                          if world > 1 else "")}
 
 
 def adjoint_sample(cs, GattDNS, nsteps=20, every=5, shape=(400, 150, 64)):
@@ -298,6 +330,71 @@ def adjoint_sample(cs, GattDNS, nsteps=20, every=5, shape=(400, 150, 64)):
                       "(graph capture, buffer allocation)" % (nsteps, every)}
 
 
+def kernel_functions(case, tuned):
+    """Map each profiled launch class to the kernel function it launches (the line-solve
+    family the context uses for that matrix set: the autotuner's choice, else the pipelined
+    solver) and to its algorithmic bytes per point (16 B per field for a line solve: read and
+    write once)."""
+    fam_name = {"pipe": "k_psweep", "reg": "k_rsweep", "tile": "k_sweep"}
+
+    def solver(d, kind):
+        m = case.mats[d - 1]
+        fam = tuned.get((d, kind), ("pipe",))[0]
+        nR = m.nRHS if kind == 0 else m.nRHSf
+        return "%s<%s, %s, nR=%d>" % (fam_name[fam], "x" if d == 1 else "y/z",
+                                      "cyclic" if m.periodic else "banded", nR)
+
+    return {"sweep_d1_x": (solver(1, 0), 5 * 16), "sweep_d1_y": (solver(2, 0), 5 * 16),
+            "sweep_d1_z": (solver(3, 0), 5 * 16), "sweep_d1_yz": (solver(2, 0), 10 * 16),
+            "sweep_d2_x": (solver(1, 0), 4 * 16), "sweep_d2_y": (solver(2, 0), 4 * 16),
+            "sweep_d2_z": (solver(3, 0), 4 * 16), "sweep_d2_yz": (solver(2, 0), 8 * 16),
+            "filter_x": (solver(1, 1), 5 * 16), "filter_y": (solver(2, 1), 5 * 16),
+            "filter_z": (solver(3, 1), 5 * 16),
+            "visc": ("k_visc3d", (13 + 9) * 8), "assemble_rk": ("k_assemble3d_pipe", ASSEMBLE_FIELDS * 8),
+            "maxchange": ("k_maxchange", 10 * 8)}
+
+
+def dominant_kernel(prof, funcs, npts):
+    """The kernel function with the largest device time per step (summed over all of its
+    launch classes), with its algorithmic bytes and time per step."""
+    per = {}
+    for cls, (ms, nl) in prof.items():
+        if nl <= 0 or cls not in funcs:
+            continue
+        fn, bpp = funcs[cls]
+        t, b, n = per.get(fn, (0.0, 0.0, 0.0))
+        per[fn] = (t + ms * nl, b + bpp * npts * nl, n + nl)
+    fn = max(per, key=lambda k: per[k][0])
+    return fn, per[fn], {k: round(v[0] / sum(x[0] for x in per.values()), 4) for k, v in per.items()}
+
+
+def captured_traffic(fn):
+    """DRAM bytes per launch of kernel function `fn` from the capture file, or None."""
+    if not os.path.exists(TRAFFIC_FILE):
+        return None
+    with open(TRAFFIC_FILE) as f:
+        for line in f:
+            if line.startswith("traffic "):
+                name, val = line[len("traffic "):].rsplit(" ", 1)
+                if name.strip() == fn:
+                    return float(val)
+    return None
+
+
+def host_cpu():
+    """CPU model and logical core count of this host."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "nproc": os.cpu_count()}
+
+
 def lid_sample(cs, GattDNS, nsteps=1000, cpu_steps=200):
     """Config 1: the 128^2 lid-driven cavity from rest, nsteps RK4 steps at CFL 0.5 on the GPU
     (wall clock of one gatt_run), and the CPU oracle on a bounded sample of the same steps."""
@@ -329,43 +426,46 @@ def lid_sample(cs, GattDNS, nsteps=1000, cpu_steps=200):
                       "timed, scaled to %d" % (nsteps, cpu_steps, nsteps)}
 
 
-def cavity_sample(cs, GattDNS, nsteps=15, repeats=10, cpu_steps=10):
+def cavity_sample(cs, GattDNS, nsteps=20000, chunk=1000, cpu_steps=10):
     """Config 3 on its full grid: the 800x300 boundary layer over a cavity with buffer zones
-    and SFD, from the Blasius profile; `repeats` runs of nsteps RK4 steps at CFL 0.5 from the
-    start state (the restated boundary set goes unstable after ~20 steps, so the run to the
-    1e-10 residual is not reproduced; the cost of a step does not depend on the state), and
-    the CPU oracle on a bounded sample of the same steps."""
+    and SFD, from the Blasius start at CFL 0.5, nsteps RK4 steps in chunks of `chunk` (one
+    gatt_run each), with the residual (max-change of the last step of each chunk, the
+    log.txt residual of main.F90:414-420); and the CPU oracle on a bounded sample of steps."""
     import oracle
     c = cs.boundary_layer_cavity()
     f = cs.blasius_flow(c)
+    o = oracle.Oracle(c)
+    f = o.apply_bound_cond(f, 0.0)
     dt = c.cfl_dt(f["U"], f["V"], f["W"], 0.5)
     g = GattDNS(c)
     g.upload(f)
-    g.apply_bound_cond(0.0)
-    g.run(5, 0.0, dt)
-    el = 0.0
-    for _ in range(repeats):
-        g.upload(f)
-        g.apply_bound_cond(0.0)
+    g.run(2, 0.0, dt)  # graph capture
+    g.upload(f)
+    hist = []
+    el, done = 0.0, 0
+    while done < nsteps:
+        k = min(chunk, nsteps - done)
         t0 = time.perf_counter()
-        mc = g.run(nsteps, 0.0, dt)
+        mc = g.run(k, done * dt, dt)
         el += time.perf_counter() - t0
+        done += k
+        hist.append([done, float(np.max(mc[0]))])
+        if not np.all(np.isfinite(mc)):
+            break
     g.close()
-    o = oracle.Oracle(c)
-    st = o.new_state(o.apply_bound_cond(f, 0.0))
+    st = o.new_state(f)
     t0 = time.perf_counter()
     for k in range(cpu_steps):
         o.step(st, k * dt, dt)
-    cel = (time.perf_counter() - t0) / cpu_steps * nsteps * repeats
+    cel = (time.perf_counter() - t0) / cpu_steps * done
     npts = c.nx * c.ny
-    total = nsteps * repeats
     return {"workload": "boundary layer over a cavity 800x300, buffers 40/30/40, SFD (X 0.02, Delta 15)",
-            "steps_timed": total, "gpu_s": el, "gpu_ms_per_step": el / total * 1e3,
-            "gpu_mpoint_stages_s": npts * STAGES * total / el / 1e6, "cpu_s_est": cel,
+            "dt": dt, "steps": done, "gpu_s": el, "gpu_ms_per_step": el / done * 1e3,
+            "gpu_mpoint_stages_s": npts * STAGES * done / el / 1e6, "cpu_s_est": cel,
             "cpu_cores": o.lib.orc_num_threads(), "gpu_over_cpu": cel / el,
-            "max_change_last": [float(x) for x in mc[0]],
-            "sample": "%d runs of %d steps from the Blasius start (the restated boundary set is not stable "
-                      "beyond ~20 steps); CPU oracle: %d steps timed, scaled" % (repeats, nsteps, cpu_steps)}
+            "residual_history": hist, "max_change_last": [float(x) for x in mc[0]],
+            "sample": "%d steps from the Blasius start (t = %.3f); residual = max over variables of the last "
+                      "step's max-change per chunk; CPU oracle: %d steps timed, scaled" % (done, done * dt, cpu_steps)}
 
 
 def time_steps(g, dt, k):
@@ -464,19 +564,13 @@ def main():
 
     # ---- per-kernel timing for the roofline (CUDA events around each launch) ------------
     prof = g.profile_kernels(t, dt, nsteps=2)
-    # algorithmic bytes per launch: a line solve reads and writes each of its fields once
-    alg = {"sweep_d1_x": 5 * 16, "sweep_d1_y": 5 * 16, "sweep_d1_z": 5 * 16,
-           "sweep_d2_x": 4 * 16, "sweep_d2_y": 4 * 16, "sweep_d2_z": 4 * 16,
-           "filter_x": 5 * 16, "filter_y": 5 * 16, "filter_z": 5 * 16,
-           "visc": (13 + 9) * 8, "assemble_rk": ASSEMBLE_FIELDS * 8, "maxchange": 10 * 8}
-    per_step = {k: v[0] * v[1] for k, v in prof.items()}
-    dom = max(per_step, key=per_step.get)
+    funcs = kernel_functions(c, tuned)
+    dom, (dom_ms_step, dom_bytes_step, dom_launches), shares = dominant_kernel(prof, funcs, npts)
     peak, peak_kind = measured_peaks()
-    dom_ms = prof[dom][0]
-    dom_bytes = alg.get(dom, 0) * npts
-    achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_bytes else None
+    achieved = dom_bytes_step / (dom_ms_step / 1e3) / 1e9
     step_ms = ms_max / args.steps
     stage_model = BYTES_PER_POINT_STAGE * npts * STAGES / (step_ms / 1e3) / 1e9
+    traffic = captured_traffic(dom) if args.n == 128 else None
 
     line = {"metric": "FP64 Mpoint-stages/s (RK4 step, 128^3 periodic box)", "value": value,
             "unit": "Mpoint-stages/s", "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
@@ -493,12 +587,15 @@ def main():
                     "path": "gatt_upload from pinned host, K x gatt_step (host maxChange each step), gatt_download"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": (achieved / peak) if achieved else None,
-                         "traffic": (ASSEMBLE_TRAFFIC_STAGE3_128 * ASSEMBLE_FIELDS / 52.0
-                                     if dom == "assemble_rk" and args.n == 128 else None),
-                         "traffic_bytes_algorithmic": dom_bytes,
-                         "peak_source": peak_kind,
+                         "frac": achieved / peak,
+                         "traffic": traffic,
+                         "traffic_source": ("ncu capture of this workload (dram__bytes_read.sum + "
+                                            "dram__bytes_write.sum per launch), profiles/"
+                                            + os.path.basename(TRAFFIC_FILE)) if traffic else None,
+                         "bytes_algorithmic": dom_bytes_step / dom_launches, "launches_per_step": dom_launches,
+                         "ms_per_launch": dom_ms_step / dom_launches, "peak_source": peak_kind,
                          "step_sweep_model_gbs": stage_model, "step_sweep_model_frac": stage_model / peak},
+            "kernel_time_shares": shares,
             "kernels_ms_per_launch": {k: round(v[0], 5) for k, v in prof.items() if v[1] > 0},
             "autotuned": {"%s/%s" % ("xyz"[d - 1], ("deriv", "filter", "derivT_lhs", "derivT_band", "filterT_lhs",
                                                    "filterT_band")[k]): [fam, P, round(us, 1)]
@@ -506,16 +603,21 @@ def main():
             "max_change_last": [float(x) for x in mc[0]]}
     if clocks:
         line["clocks"] = clocks
+    if not args.kernels_only and not args.no_arnoldi:
+        # config 4: the batched Arnoldi problems on the box after 200 steps, sharded across ranks
+        g.upload(host)
+        g.run(200, 0.0, dt)
+        base200 = g.download()
+        g.close()
+        line["arnoldi"] = [arnoldi_sample(cs, GattDNS, c, base200, 32, 2, 10, 4321,
+                                          "32 problems on the %d^3 periodic box after 200 steps" % args.n,
+                                          dist if world > 1 else None)]
+        if world == 1:
+            lid = cs.lid_driven(n=128)
+            line["arnoldi"].append(arnoldi_sample(cs, GattDNS, lid, cs.uniform_flow(lid), 32, 2, 100, 4321,
+                                                  "32 problems on the 128^2 lid-driven cavity (rest state base)"))
     if rank == 0 and world == 1 and not args.kernels_only:
         line["cpu_baseline"] = cpu_baseline_sample(c)
-        if not args.no_arnoldi:
-            g.close()
-            lid = cs.lid_driven(n=128)
-            line["arnoldi"] = [
-                arnoldi_sample(cs, GattDNS, c, f, 32, 2, 10, 4321,
-                               "32 problems on the %d^3 periodic box base flow" % args.n),
-                arnoldi_sample(cs, GattDNS, lid, cs.uniform_flow(lid), 32, 2, 100, 4321,
-                               "32 problems on the 128^2 lid-driven cavity (rest state base)")]
         if not args.no_adjoint:
             g.close()
             line["adjoint"] = adjoint_sample(cs, GattDNS)

@@ -91,11 +91,12 @@ constexpr int kBlock = 256;
 // kernel classes reported by gatt_profile_kernels (names in gatt_profile_name)
 enum {
     PC_D1X = 0, PC_D1Y, PC_D1Z, PC_VISC, PC_D2X, PC_D2Y, PC_D2Z, PC_ASSEMBLE, PC_BC,
-    PC_FX, PC_FY, PC_FZ, PC_SFD, PC_MAXCHANGE, PC_OTHER, PC_N
+    PC_FX, PC_FY, PC_FZ, PC_SFD, PC_MAXCHANGE, PC_OTHER, PC_D1YZ, PC_D2YZ, PC_N
 };
 const char *const kProfNames[PC_N] = {
     "sweep_d1_x", "sweep_d1_y", "sweep_d1_z", "visc", "sweep_d2_x", "sweep_d2_y", "sweep_d2_z",
-    "assemble_rk", "bc", "filter_x", "filter_y", "filter_z", "sfd", "maxchange", "other"};
+    "assemble_rk", "bc", "filter_x", "filter_y", "filter_z", "sfd", "maxchange", "other",
+    "sweep_d1_yz", "sweep_d2_yz"};
 
 }  // namespace
 
@@ -146,8 +147,14 @@ struct gatt_ctx {
     double *a_s1 = nullptr, *a_s2 = nullptr, *a_scr = nullptr;                       // 15, 12, 5
     double *a_ckpt = nullptr, *a_seg = nullptr;
     int a_nckpt = 0, a_nseg = 0;
+    bool a_ckpt_sfd = false, a_seg_sfd = false;  // checkpoint / segment slots hold a mean too
     long long tape_len = 0;              // doubles of the boundary-program tape per member
     double *t_P = nullptr, *a_lP = nullptr, *a_tape = nullptr, *a_tmp = nullptr;
+    // 2-D cases: the base gradients, stresses and second sweeps of the tangent / adjoint in the
+    // 3-D layouts (z slots zero); 3-D cases use d1 / tq / d2
+    double *g_d1 = nullptr, *g_tq = nullptr, *g_d2 = nullptr;
+    // SFD cases: the base mean of the step, the tangent mean, the adjoint mean and a scratch mean
+    double *dxm = nullptr, *dym = nullptr, *a_lm = nullptr, *a_mscr = nullptr;
     long long a_tape_cap = 0;
     bool mean_init = false;                  // SFD mean uploaded or copied from the state
     int cur = 0;
@@ -167,6 +174,7 @@ struct gatt_ctx {
     int *h_err = nullptr;   // pipeline wait give-up flag (pinned, device-mapped)
     int *d_err = nullptr;
     bool pw_pipe = true;    // 3-D assembly fed by bulk copies (GATT_PW=plain: thread loads)
+    bool merge_yz = true;   // y and z derivative sweeps in one launch where their sets allow (GATT_MERGE_YZ=0: no)
     int bc_cluster = 0;     // CTAs per member for the boundary program (0: one CTA, k_bc)
     int bc_cluster_rec = 0, bc_cluster_tl = 0, bc_cluster_adj = 0;  // same, tape / tangent / adjoint
     long long bc_points = 0;  // point updates of one application of the program (sum over ops)
@@ -521,10 +529,11 @@ int upload_records(gatt_ctx *c, DevDir &m, int P, int rows = 0)
 // Pipelined register solver: build the tensor map (y/z), size the persistent grid, launch.
 // Returns GATT_ERR_STATE (without launching) when the layout does not meet the copy engine's
 // alignment rules, so that the caller falls back to k_rsweep.
-int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmembers, int cls)
+int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmembers, int cls, const DevDir *m1 = nullptr)
 {
     const int N = m.rows;  // padded y/z lines: the box covers the padding (zero fill)
     const bool xd = d == 0;
+    const int nt1 = m1 ? m1->nTypes : 0;  // part 1 (z lines of a y+z launch)
     void *k = reg_kernel(true, xd, m.periodic != 0, m.nR, m.P > 24);  // 25 blocks: the 800-thread form
     if (!k) return GATT_ERR_STATE;
     // ring depth: the deepest ring that keeps the most CTAs resident (one stage suffices
@@ -532,7 +541,7 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
     int nst = 0, per_sm = 0;
     size_t smem = 0;
     for (int st = kMaxStages; st >= 1; st--) {
-        const size_t b = psweep_smem_bytes(xd, N, m.P, m.nTypes, m.Wp, st);
+        const size_t b = psweep_smem_bytes(xd, N, m.P, m.nTypes, m.Wp, st, nt1);
         if (b > kMaxSmem) continue;
         const int r = resident_ctas(k, 32 * m.P, b);
         if (r > per_sm) { per_sm = r; nst = st; smem = b; }
@@ -581,20 +590,27 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
         EncodeTiledFn enc = encode_tiled();
         if (!enc) return GATT_ERR_STATE;
         int nslots = 1;
-        for (int f = 0; f < a.nf; f++) nslots = std::max(nslots, a.in_slot[f] + 1);
+        for (int f = 0; f < a.nf; f++) {
+            nslots = std::max(nslots, a.in_slot[f] + 1);
+            if (m1) nslots = std::max(nslots, a.in_slot1[f] + 1);
+        }
         const long long mstride = nmembers > 1 ? a.in_bstride : (long long)nslots * c->npts;
         cuuint64_t dims[5] = {(cuuint64_t)c->nx, (cuuint64_t)c->ny, (cuuint64_t)c->nz, (cuuint64_t)nslots,
                               (cuuint64_t)nmembers};
         cuuint64_t strides[4] = {(cuuint64_t)c->nx * 8, (cuuint64_t)c->nx * c->ny * 8, (cuuint64_t)c->npts * 8,
                                  (cuuint64_t)mstride * 8};
         const int brows = a.box2 ? a.box2 : N;
-        cuuint32_t box[5] = {(cuuint32_t)kLanes, (cuuint32_t)(d == 1 ? brows : 1), (cuuint32_t)(d == 2 ? brows : 1), 1,
-                             1};
-        cuuint32_t estr[5] = {1, 1, 1, 1, 1};
-        CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<double *>(a.in), dims, strides, box, estr,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (r != CUDA_SUCCESS) return GATT_ERR_STATE;
+        // map of direction dd: a box of 32 x-points by `brows` rows of its lines
+        auto yzmap = [&](CUtensorMap *mp, int dd) {
+            cuuint32_t box[5] = {(cuuint32_t)kLanes, (cuuint32_t)(dd == 1 ? brows : 1), (cuuint32_t)(dd == 2 ? brows : 1),
+                                 1, 1};
+            cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+            return enc(mp, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<double *>(a.in), dims, strides, box, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+        };
+        if (!yzmap(&map, d)) return GATT_ERR_STATE;
+        if (m1 && !yzmap(&omap, 2)) return GATT_ERR_STATE;  // part 1: the z lines
     }
     const int grid = std::min(a.njobs, per_sm * c->nsm);
     void *args[] = {&a, &map, &omap};
@@ -631,6 +647,7 @@ int sweep(gatt_ctx *c, int d, int kind, const double *in, long long in_bs, const
     a.nf = nf;
     a.ntiles = d == 0 ? (a.nlines + kLanes - 1) / kLanes : a.tiles_per_row * (d == 1 ? c->nz : c->ny);
     a.njobs = a.ntiles * nf * nmembers;
+    a.fd_ntiles = make_fastdiv(a.ntiles); a.fd_nf = make_fastdiv(nf); a.fd_tpr = make_fastdiv(a.tiles_per_row);
     a.err = c->d_err;
     a.ntypes = m.nTypes;
     if (m.family == FAM_PIPE && m.rpb) {
@@ -672,6 +689,52 @@ int sweep(gatt_ctx *c, int d, int kind, const double *in, long long in_bs, const
         }
     }
     return GATT_OK;
+}
+
+// The y and z derivative sweeps of nf fields (input slots sy / sz, output slots oy / oz),
+// in one launch of the pipelined solver where both directions' sets allow it: x-tile column
+// by column, each field's y tiles and then its z tiles, which find the column's field in L2
+// (128^3: a column of one field is 4 MB).  Otherwise two launches.
+int sweep_yz(gatt_ctx *c, const double *in, long long in_bs, const int *sy, const int *sz, double *out,
+             long long out_bs, const int *oy, const int *oz, int nf, int nmembers, int cls_y, int cls_z, int cls_yz)
+{
+    const DevDir &my = c->mat[1][0], &mz = c->mat[2][0];
+    const bool merge = c->merge_yz && c->is3d && my.set && mz.set && c->lt_set[1] && c->lt_set[2] &&
+                       c->lt_max[1] < my.nTypes && c->lt_max[2] < mz.nTypes && my.family == FAM_PIPE &&
+                       mz.family == FAM_PIPE && my.rpb && mz.rpb && my.rows == my.N && mz.rows == mz.N &&
+                       my.rows == mz.rows && my.P == mz.P && my.nR == mz.nR && my.nR < 6 && my.Wp == mz.Wp &&
+                       my.periodic == mz.periodic && my.rows <= 256 && nf <= 16;
+    if (merge) {
+        SweepArgs a;
+        memset(&a, 0, sizeof(a));
+        a.in = in; a.out = out; a.in_bstride = in_bs; a.out_bstride = out_bs; a.npts = c->npts;
+        for (int f = 0; f < nf; f++) {
+            a.in_slot[f] = sy[f]; a.out_slot[f] = oy[f];
+            a.in_slot1[f] = sz[f]; a.out_slot1[f] = oz[f];
+        }
+        a.nx = c->nx; a.ny = c->ny; a.nz = c->nz;
+        a.N = my.rows; a.Nreal = my.N; a.nlines = nlines(c, 1);
+        a.es = c->nx; a.os = (long long)c->nx * c->ny;   // y lines: x stride nx, outer index z
+        a.es1 = (long long)c->nx * c->ny; a.os1 = c->nx;  // z lines: stride nx*ny, outer index y
+        a.tiles_per_row = (c->nx + kLanes - 1) / kLanes;
+        a.Rm = my.Rm; a.Q = my.Q; a.W = my.W; a.Wp = my.Wp; a.P = my.P;
+        a.ltype = c->ltype[1]; a.ntypes = my.nTypes;
+        a.Rm1 = mz.Rm; a.Q1 = mz.Q; a.ltype1 = c->ltype[2]; a.ntypes1 = mz.nTypes;
+        a.epi = EPI_STORE;
+        a.dir = 1;
+        a.nf = nf;
+        a.parts = 2;
+        a.nout0 = c->nz; a.nout1 = c->ny;
+        a.ntiles = a.tiles_per_row * (c->nz + c->ny);
+        a.njobs = a.ntiles * nf * nmembers;
+        a.fd_ntiles = make_fastdiv(a.ntiles); a.fd_nf = make_fastdiv(nf); a.fd_tpr = make_fastdiv(a.tiles_per_row);
+        a.fd_nout = make_fastdiv(c->nz + c->ny);
+        a.err = c->d_err;
+        const int r = launch_psweep(c, my, 1, a, nmembers, cls_yz, &mz);
+        if (r != GATT_ERR_STATE) return r;  // GATT_ERR_STATE: layout refused, two launches
+    }
+    TRY(sweep(c, 1, 0, in, in_bs, sy, out, out_bs, oy, nf, nmembers, 0, nullptr, cls_y));
+    return sweep(c, 2, 0, in, in_bs, sz, out, out_bs, oz, nf, nmembers, 0, nullptr, cls_z);
 }
 
 // ---------------------------------------------------------------------------
@@ -742,6 +805,21 @@ int launch_assemble3d_pipe(gatt_ctx *c, const StateSet &q, const StateSet &q0, c
     return after_launch(c);
 }
 
+// The 3-D assembly + RK4 stage update from gradients d1 and second sweeps d2 (tensor-copy
+// fed where the layouts allow, else thread loads).
+int assemble3d(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet &out, int mode, int nmem, double *d1,
+               double *d2, double *delta)
+{
+    const long long n = c->npts;
+    const FieldSet fd = fset(c, delta, 5), f1 = fset(c, d1, D3_N), f2 = fset(c, d2, S3_N);
+    const int pr = launch_assemble3d_pipe(c, q, q0, out, fd, f1, f2, mode, nmem);
+    if (pr != GATT_ERR_STATE) return pr;
+    TRY(before_launch(c, PC_ASSEMBLE));
+    k_assemble3d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(c->ph, q, q0, out, fd, f1, f2, n, mode,
+                                                                      c->d_params);
+    return after_launch(c);
+}
+
 // nseq2d/nseq3d on stage input q, fused with the RK4 update into out (mode).
 int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet &out, int mode, int nmem,
               double *d1, double *tq, double *d2, double *delta, bool assemble = true)
@@ -758,8 +836,7 @@ int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet
         const int oy[5] = {D3_UY, D3_VY, D3_WY, D3_RY, D3_EY};
         const int oz[5] = {D3_UZ, D3_VZ, D3_WZ, D3_RZ, D3_EZ};
         TRY(sweep(c, 0, 0, qin, qbs, fin, d1, bd1, ox, 5, nmem, 0, nullptr, PC_D1X));
-        TRY(sweep(c, 1, 0, qin, qbs, fin, d1, bd1, oy, 5, nmem, 0, nullptr, PC_D1Y));
-        TRY(sweep(c, 2, 0, qin, qbs, fin, d1, bd1, oz, 5, nmem, 0, nullptr, PC_D1Z));
+        TRY(sweep_yz(c, qin, qbs, fin, fin, d1, bd1, oy, oz, 5, nmem, PC_D1Y, PC_D1Z, PC_D1YZ));
         TRY(before_launch(c, PC_VISC));
         k_visc3d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(c->ph, q, fset(c, d1, D3_N), fset(c, tq, T3_N), n);
         TRY(after_launch(c));
@@ -768,15 +845,9 @@ int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet
         const int iy[4] = {T3_XY, T3_YY, T3_YZ, T3_QY}, sy[4] = {S3_TXYY, S3_TYYY, S3_TYZY, S3_HTY};
         const int iz[4] = {T3_XZ, T3_YZ, T3_ZZ, T3_QZ}, sz[4] = {S3_TXZZ, S3_TYZZ, S3_TZZZ, S3_HTZ};
         TRY(sweep(c, 0, 0, tq, btq, ix, d2, bd2, sx, 4, nmem, 0, nullptr, PC_D2X));
-        TRY(sweep(c, 1, 0, tq, btq, iy, d2, bd2, sy, 4, nmem, 0, nullptr, PC_D2Y));
-        TRY(sweep(c, 2, 0, tq, btq, iz, d2, bd2, sz, 4, nmem, 0, nullptr, PC_D2Z));
+        TRY(sweep_yz(c, tq, btq, iy, iz, d2, bd2, sy, sz, 4, nmem, PC_D2Y, PC_D2Z, PC_D2YZ));
         if (!assemble) return GATT_OK;  // the gradients and second sweeps only (tangent / adjoint)
-        const FieldSet fd = fset(c, delta, 5), f1 = fset(c, d1, D3_N), f2 = fset(c, d2, S3_N);
-        const int pr = launch_assemble3d_pipe(c, q, q0, out, fd, f1, f2, mode, nmem);
-        if (pr != GATT_ERR_STATE) return pr;
-        TRY(before_launch(c, PC_ASSEMBLE));
-        k_assemble3d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(c->ph, q, q0, out, fd, f1, f2, n, mode, sp);
-        return after_launch(c);
+        return assemble3d(c, q, q0, out, mode, nmem, d1, d2, delta);
     }
     const long long bd1 = D2_N * n, btq = T2_N * n, bd2 = S2_N * n;
     const int fin[4] = {0, 1, 3, 4};
@@ -1436,8 +1507,13 @@ int arnoldi(gatt_ctx *c, int m, int nsteps, double t0, double dt, double eps, co
 
 
 // ---------------------------------------------------------------------------
-// Tangent-linear and adjoint of the 3-D step (no counterpart in the reference)
+// Tangent-linear and adjoint of the step (no counterpart in the reference)
 // ---------------------------------------------------------------------------
+// Both run the 3-D data flow in the 3-D layouts.  A 2-D case runs it with no z direction:
+// the z gradients and z second sweeps stay zero and W is zero, so the 3-D expressions reduce
+// to nseq2d's (nseq.F90:10-139) and the W components of every vector are zero.  With SFD
+// (main.F90:381-402) the step maps the state and the mean, so the tangent and adjoint carry
+// both: a vector of a member is then its 5 state fields followed by its 5 mean fields.
 
 StateSet set5(const gatt_ctx *c, double *p)
 {
@@ -1453,28 +1529,44 @@ int copy_set5(gatt_ctx *c, double *dst, const double *src)
     return GATT_OK;
 }
 
-// copy between a context state slot (separate per-variable pointers) and a 5-field set
+// zero slot W of every member of a 5-field set (2-D cases)
+int zero_w(gatt_ctx *c, double *set)
+{
+    if (c->is3d) return GATT_OK;
+    CU(cudaMemset2DAsync(set + 2 * c->npts, sizeof(double) * 5 * (size_t)c->npts, 0, sizeof(double) * (size_t)c->npts,
+                         c->nb, c->stream));
+    return GATT_OK;
+}
+
+// copy between a context state slot (separate per-variable pointers) and a 5-field set; in
+// 2-D the set's W is zero and the state's W (the caller's) is never overwritten
 int state_to_set(gatt_ctx *c, const StateSet &q, double *dst, bool to_set)
 {
     for (int b = 0; b < c->nb; b++)
         for (int f = 0; f < 5; f++) {
+            if (!c->is3d && f == 2) continue;
             double *sp = q.v[f] + b * q.bstride, *dp = dst + ((size_t)b * 5 + f) * c->npts;
             if (to_set) CU(cudaMemcpyAsync(dp, sp, sizeof(double) * c->npts, cudaMemcpyDeviceToDevice, c->stream));
             else CU(cudaMemcpyAsync(sp, dp, sizeof(double) * c->npts, cudaMemcpyDeviceToDevice, c->stream));
         }
+    if (to_set) TRY(zero_w(c, dst));
     return GATT_OK;
 }
 
-// The tangent and the adjoint are built for 3-D cases whose step is RK4 + filter +
-// boundary conditions (no SFD).
-int check_diff(gatt_ctx *c, bool adjoint)
+bool diff_sfd(const gatt_ctx *c) { return c->sfd_type > 0; }
+
+// Vector fields per member of gatt_jvp / gatt_vjp: the state, and with SFD the mean.
+int diff_nv(const gatt_ctx *c) { return diff_sfd(c) ? 10 : 5; }
+
+int check_diff(gatt_ctx *c, bool adjoint, bool step = false)
 {
     TRY(check_ready(c, true));
-    if (!c->is3d) return fail(GATT_ERR_STATE, "tangent and adjoint are built for 3-D cases");
-    if (c->sfd_type > 0) return fail(GATT_ERR_STATE, "tangent and adjoint are built for cases without SFD");
     if (c->bc_dirty) TRY(build_bc_program(c));
+    if (step && diff_sfd(c) && (!c->mean || !c->mean_init))
+        return fail(GATT_ERR_STATE, "SFD: upload the mean (gatt_upload_mean) or run a step before the tangent/adjoint");
+    const int ndir = c->is3d ? 3 : 2;
     if (adjoint)
-        for (int d = 0; d < 3; d++) {
+        for (int d = 0; d < ndir; d++) {
             if (!c->mat[d][2].set || !c->mat[d][3].set)
                 return fail(GATT_ERR_STATE, "transposed derivative matrices (kinds 2, 3) missing");
             if (c->filt[d] && (!c->mat[d][4].set || !c->mat[d][5].set))
@@ -1483,28 +1575,48 @@ int check_diff(gatt_ctx *c, bool adjoint)
     return GATT_OK;
 }
 
+// allocate a set of nslots fields per member, zeroed (the 2-D z slots are never written)
+int alloc_zeroed(gatt_ctx *c, double **p, int nslots)
+{
+    if (*p) return GATT_OK;
+    TRY(alloc_fields(c, p, nslots, c->nb));
+    CU(cudaMemsetAsync(*p, 0, sizeof(double) * nslots * (size_t)c->npts * c->nb, c->stream));
+    return GATT_OK;
+}
+
 int diff_alloc(gatt_ctx *c, bool adjoint)
 {
-    for (double *&p : c->dx) if (!p) TRY(alloc_fields(c, &p, 5, c->nb));
+    for (double *&p : c->dx) TRY(alloc_zeroed(c, &p, 5));
+    if (!c->is3d) {
+        TRY(alloc_zeroed(c, &c->g_d1, D3_N));
+        TRY(alloc_zeroed(c, &c->g_tq, T3_N));
+        TRY(alloc_zeroed(c, &c->g_d2, S3_N));
+    }
+    if (diff_sfd(c)) TRY(alloc_zeroed(c, &c->dxm, 5));
     if (!adjoint) {
         if (!c->t_P) TRY(alloc_fields(c, &c->t_P, 1, c->nb));
-        for (double *&p : c->dy) if (!p) TRY(alloc_fields(c, &p, 5, c->nb));
-        if (!c->t_delta) TRY(alloc_fields(c, &c->t_delta, 5, c->nb));
-        if (!c->t_d1) TRY(alloc_fields(c, &c->t_d1, D3_N, c->nb));
-        if (!c->t_tq) TRY(alloc_fields(c, &c->t_tq, T3_N, c->nb));
-        if (!c->t_d2) TRY(alloc_fields(c, &c->t_d2, S3_N, c->nb));
+        for (double *&p : c->dy) TRY(alloc_zeroed(c, &p, 5));
+        TRY(alloc_zeroed(c, &c->t_delta, 5));
+        TRY(alloc_zeroed(c, &c->t_d1, D3_N));
+        TRY(alloc_zeroed(c, &c->t_tq, T3_N));
+        TRY(alloc_zeroed(c, &c->t_d2, S3_N));
+        if (diff_sfd(c)) TRY(alloc_zeroed(c, &c->dym, 5));
         return GATT_OK;
     }
     double **five[] = {&c->a_lam, &c->a_acc, &c->a_arg, &c->a_prev, &c->a_g, &c->a_lq, &c->a_scr};
-    for (double **p : five) if (!*p) TRY(alloc_fields(c, p, 5, c->nb));
-    if (!c->a_ld1) TRY(alloc_fields(c, &c->a_ld1, D3_N, c->nb));
-    if (!c->a_ltau) TRY(alloc_fields(c, &c->a_ltau, T3_N, c->nb));
-    if (!c->a_lvt) TRY(alloc_fields(c, &c->a_lvt, 4, c->nb));
-    if (!c->a_s1) TRY(alloc_fields(c, &c->a_s1, 15, c->nb));
-    if (!c->a_s2) TRY(alloc_fields(c, &c->a_s2, 12, c->nb));
+    for (double **p : five) TRY(alloc_zeroed(c, p, 5));
+    TRY(alloc_zeroed(c, &c->a_ld1, D3_N));
+    TRY(alloc_zeroed(c, &c->a_ltau, T3_N));
+    TRY(alloc_zeroed(c, &c->a_lvt, 4));
+    TRY(alloc_zeroed(c, &c->a_s1, 15));
+    TRY(alloc_zeroed(c, &c->a_s2, 12));
     if (!c->a_lP) TRY(alloc_fields(c, &c->a_lP, 1, c->nb));
-    if (!c->a_tmp) TRY(alloc_fields(c, &c->a_tmp, 5, c->nb));
-    // five boundary-program tapes per step (after each stage and after the filter)
+    TRY(alloc_zeroed(c, &c->a_tmp, 5));
+    if (diff_sfd(c)) {
+        TRY(alloc_zeroed(c, &c->a_lm, 5));
+        TRY(alloc_zeroed(c, &c->a_mscr, 5));
+    }
+    // five boundary-program tapes per step (after each stage and after the filter / SFD)
     const long long need = 5 * std::max(1LL, c->tape_len) * c->nb;
     if (c->a_tape_cap < need) {
         cudaFree(c->a_tape);
@@ -1565,6 +1677,38 @@ int set_params(gatt_ctx *c, int slot, double t, double dt)
     return GATT_OK;
 }
 
+// The base data the tangent / adjoint kernels read, in the 3-D layouts
+double *diff_d1(gatt_ctx *c) { return c->is3d ? c->d1 : c->g_d1; }
+double *diff_d2(gatt_ctx *c) { return c->is3d ? c->d2 : c->g_d2; }
+
+// rhs_stage for the tangent and adjoint on 5-field sets: in 3-D the forward itself; in 2-D the
+// 3-D data flow without the z direction (x and y sweeps into the 3-D slots, the z slots stay
+// zero), so the stage matches nseq2d + RK4_2D to rounding and leaves the base data in the
+// 3-D layouts.
+int rhs_stage_d(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet &out, int mode,
+                bool assemble = true)
+{
+    const int nm = c->nb;
+    if (c->is3d) return rhs_stage(c, q, q0, out, mode, nm, c->d1, c->tq, c->d2, c->delta, assemble);
+    const long long n = c->npts;
+    const long long bd1 = D3_N * n, btq = T3_N * n, bd2 = S3_N * n;
+    const int fin[5] = {0, 1, 2, 3, 4};
+    const int ox[5] = {D3_UX, D3_VX, D3_WX, D3_RX, D3_EX};
+    const int oy[5] = {D3_UY, D3_VY, D3_WY, D3_RY, D3_EY};
+    TRY(sweep(c, 0, 0, q.v[0], q.bstride, fin, c->g_d1, bd1, ox, 5, nm, 0, nullptr, PC_D1X));
+    TRY(sweep(c, 1, 0, q.v[0], q.bstride, fin, c->g_d1, bd1, oy, 5, nm, 0, nullptr, PC_D1Y));
+    TRY(before_launch(c, PC_VISC));
+    k_visc3d<<<dim3(grid_for(c, n), nm), kBlock, 0, c->stream>>>(c->ph, q, fset(c, c->g_d1, D3_N),
+                                                                fset(c, c->g_tq, T3_N), n);
+    TRY(after_launch(c));
+    const int ix[4] = {T3_XX, T3_XY, T3_XZ, T3_QX}, sx[4] = {S3_TXXX, S3_TXYX, S3_TXZX, S3_HTX};
+    const int iy[4] = {T3_XY, T3_YY, T3_YZ, T3_QY}, sy[4] = {S3_TXYY, S3_TYYY, S3_TYZY, S3_HTY};
+    TRY(sweep(c, 0, 0, c->g_tq, btq, ix, c->g_d2, bd2, sx, 4, nm, 0, nullptr, PC_D2X));
+    TRY(sweep(c, 1, 0, c->g_tq, btq, iy, c->g_d2, bd2, sy, 4, nm, 0, nullptr, PC_D2Y));
+    if (!assemble) return GATT_OK;
+    return assemble3d(c, q, q0, out, mode, nm, c->g_d1, c->g_d2, c->delta);
+}
+
 // Tangent of one RK stage (mode 1..4, or RK_STORE_RHS for the bare RHS): the base stage
 // xin -> xout (the forward kernels), then the tangent yin -> yout.
 int tl_stage(gatt_ctx *c, const StateSet &xin, const StateSet &x0, const StateSet &xout, const StateSet &yin,
@@ -1572,7 +1716,8 @@ int tl_stage(gatt_ctx *c, const StateSet &xin, const StateSet &x0, const StateSe
 {
     const int nm = c->nb;
     const long long n = c->npts;
-    TRY(rhs_stage(c, xin, x0, xout, mode, nm, c->d1, c->tq, c->d2, c->delta));
+    TRY(rhs_stage_d(c, xin, x0, xout, mode));
+    double *d1 = diff_d1(c), *d2 = diff_d2(c);
     const long long bd1 = D3_N * n, btq = T3_N * n, bd2 = S3_N * n;
     const int fin[5] = {0, 1, 2, 3, 4};
     const int ox[5] = {D3_UX, D3_VX, D3_WX, D3_RX, D3_EX};
@@ -1580,9 +1725,9 @@ int tl_stage(gatt_ctx *c, const StateSet &xin, const StateSet &x0, const StateSe
     const int oz[5] = {D3_UZ, D3_VZ, D3_WZ, D3_RZ, D3_EZ};
     TRY(sweep(c, 0, 0, yin.v[0], yin.bstride, fin, c->t_d1, bd1, ox, 5, nm, 0, nullptr, PC_D1X));
     TRY(sweep(c, 1, 0, yin.v[0], yin.bstride, fin, c->t_d1, bd1, oy, 5, nm, 0, nullptr, PC_D1Y));
-    TRY(sweep(c, 2, 0, yin.v[0], yin.bstride, fin, c->t_d1, bd1, oz, 5, nm, 0, nullptr, PC_D1Z));
+    if (c->is3d) TRY(sweep(c, 2, 0, yin.v[0], yin.bstride, fin, c->t_d1, bd1, oz, 5, nm, 0, nullptr, PC_D1Z));
     TRY(before_launch(c, PC_VISC));
-    k_tl_tau3d<<<dim3(grid_for(c, n), nm), kBlock, 0, c->stream>>>(c->ph, xin, fset(c, c->d1, D3_N), yin,
+    k_tl_tau3d<<<dim3(grid_for(c, n), nm), kBlock, 0, c->stream>>>(c->ph, xin, fset(c, d1, D3_N), yin,
                                                                   fset(c, c->t_d1, D3_N), fset(c, c->t_tq, T3_N), n);
     TRY(after_launch(c));
     const int ix[4] = {T3_XX, T3_XY, T3_XZ, T3_QX}, sx[4] = {S3_TXXX, S3_TXYX, S3_TXZX, S3_HTX};
@@ -1590,15 +1735,25 @@ int tl_stage(gatt_ctx *c, const StateSet &xin, const StateSet &x0, const StateSe
     const int iz[4] = {T3_XZ, T3_YZ, T3_ZZ, T3_QZ}, sz[4] = {S3_TXZZ, S3_TYZZ, S3_TZZZ, S3_HTZ};
     TRY(sweep(c, 0, 0, c->t_tq, btq, ix, c->t_d2, bd2, sx, 4, nm, 0, nullptr, PC_D2X));
     TRY(sweep(c, 1, 0, c->t_tq, btq, iy, c->t_d2, bd2, sy, 4, nm, 0, nullptr, PC_D2Y));
-    TRY(sweep(c, 2, 0, c->t_tq, btq, iz, c->t_d2, bd2, sz, 4, nm, 0, nullptr, PC_D2Z));
+    if (c->is3d) TRY(sweep(c, 2, 0, c->t_tq, btq, iz, c->t_d2, bd2, sz, 4, nm, 0, nullptr, PC_D2Z));
     TRY(before_launch(c, PC_ASSEMBLE));
     k_tl_assemble3d<<<dim3(grid_for(c, n), nm), kBlock, 0, c->stream>>>(
-        c->ph, xin, fset(c, c->d1, D3_N), fset(c, c->d2, S3_N), yin, fset(c, c->t_d1, D3_N), fset(c, c->t_d2, S3_N),
-        y0, yout, fset(c, c->t_delta, 5), n, mode, c->d_params);
+        c->ph, xin, fset(c, d1, D3_N), fset(c, d2, S3_N), yin, fset(c, c->t_d1, D3_N), fset(c, c->t_d2, S3_N), y0,
+        yout, fset(c, c->t_delta, 5), n, mode, c->d_params);
     return after_launch(c);
 }
 
-// One step of base and tangent: dx[0], dy[0] = step start -> step end (same arrays)
+// SFD relaxation of a 5-field set with the mean `mean` (a 5-field set), the forward kernel
+int sfd_set(gatt_ctx *c, const StateSet &q, double *mean)
+{
+    TRY(before_launch(c, PC_SFD));
+    k_sfd<<<dim3(grid_for(c, c->npts), c->nb), kBlock, 0, c->stream>>>(q, fset(c, mean, 5), c->chi, c->sfd_delta,
+                                                                     c->is3d ? 5 : 4, c->npts, c->d_params);
+    return after_launch(c);
+}
+
+// One step of base and tangent: dx[0], dy[0] (and with SFD the means dxm, dym) = step start
+// -> step end (same arrays)
 int tl_step(gatt_ctx *c)
 {
     const StateSet X0 = set5(c, c->dx[0]), XA = set5(c, c->dx[1]), XB = set5(c, c->dx[2]);
@@ -1616,6 +1771,11 @@ int tl_step(gatt_ctx *c)
     const double *bdt = c->fct > 0 ? &c->d_params->dt : nullptr;
     TRY(filter_set(c, XB, c->nb, 0.0, bdt));
     TRY(filter_set(c, YB, c->nb, 0.0, bdt));
+    // SFD (main.F90:381-402) is linear in the state and the mean: k_sfd is its own tangent
+    if (diff_sfd(c)) {
+        TRY(sfd_set(c, XB, c->dxm));
+        TRY(sfd_set(c, YB, c->dym));
+    }
     TRY(bc_tl(c, XB, YB));
     TRY(copy_set5(c, c->dx[0], c->dx[2]));
     return copy_set5(c, c->dy[0], c->dy[2]);
@@ -1637,25 +1797,27 @@ int adj_rhs(gatt_ctx *c, const StateSet &q, const StateSet &a, const StateSet &G
 {
     const int nm = c->nb;
     const long long n = c->npts;
-    TRY(rhs_stage(c, q, q, q, RK_STORE_RHS, nm, c->d1, c->tq, c->d2, nullptr, false));
+    const int ndir = c->is3d ? 3 : 2;  // 2-D: no z direction, its slots of a_s1 / a_s2 stay zero
+    TRY(rhs_stage_d(c, q, q, q, RK_STORE_RHS, false));
+    double *d1 = diff_d1(c), *d2 = diff_d2(c);
     TRY(before_launch(c, PC_OTHER));
     k_adj_asm3d<<<dim3(grid_for(c, n), nm), kBlock, 0, c->stream>>>(
-        c->ph, q, fset(c, c->d1, D3_N), fset(c, c->d2, S3_N), a, fset(c, c->a_lq, 5), fset(c, c->a_ld1, D3_N),
+        c->ph, q, fset(c, d1, D3_N), fset(c, d2, S3_N), a, fset(c, c->a_lq, 5), fset(c, c->a_ld1, D3_N),
         fset(c, c->a_ltau, T3_N), fset(c, c->a_lvt, 4), n);
     TRY(after_launch(c));
     // transposed second sweeps: (vtx, vty, vtz, ht) -> stress / heat-flux contributions
     const int v4[4] = {0, 1, 2, 3};
-    for (int d = 0; d < 3; d++) {
+    for (int d = 0; d < ndir; d++) {
         const int o4[4] = {4 * d, 4 * d + 1, 4 * d + 2, 4 * d + 3};
         TRY(sweep_T(c, d, 2, c->a_lvt, 4 * n, v4, c->a_s2, 12 * n, o4, 4));
     }
     TRY(before_launch(c, PC_OTHER));
-    k_adj_tau3d<<<dim3(grid_for(c, n), nm), kBlock, 0, c->stream>>>(c->ph, q, fset(c, c->d1, D3_N),
+    k_adj_tau3d<<<dim3(grid_for(c, n), nm), kBlock, 0, c->stream>>>(c->ph, q, fset(c, d1, D3_N),
                                                                    fset(c, c->a_ltau, T3_N), fset(c, c->a_s2, 12),
                                                                    fset(c, c->a_ld1, D3_N), fset(c, c->a_lq, 5), n);
     TRY(after_launch(c));
     // transposed first sweeps: gradient lambdas -> state lambdas
-    for (int d = 0; d < 3; d++) {
+    for (int d = 0; d < ndir; d++) {
         const int i5[5] = {D3_UX + d, D3_VX + d, D3_WX + d, D3_RX + d, D3_EX + d};
         const int o5[5] = {5 * d, 5 * d + 1, 5 * d + 2, 5 * d + 3, 5 * d + 4};
         TRY(sweep_T(c, d, 2, c->a_ld1, (long long)D3_N * n, i5, c->a_s1, 15 * n, o5, 5));
@@ -1674,27 +1836,38 @@ int axpby5(gatt_ctx *c, double *out, const double *x, const double *y, double al
     return after_launch(c);
 }
 
-// Adjoint of one step: a_lam holds lambda at the step end; dx[0] the step's start state.
-// Reverse of: 4 RK stages (timeIntegration.F90:338-498), then the x -> y -> z filter.
+// Adjoint of one step: a_lam (and with SFD a_lm) holds lambda at the step end; dx[0] (and
+// dxm) the step's start state.  Reverse of: 4 RK stages (timeIntegration.F90:338-498), the
+// x -> y -> z filter, SFD, the boundary conditions.
 int adj_step(gatt_ctx *c, double dt)
 {
     const StateSet X[5] = {set5(c, c->dx[0]), set5(c, c->dx[1]), set5(c, c->dx[2]), set5(c, c->dx[3]),
                            set5(c, c->dx[4])};
-    // recompute the stage states q1..q4 (after their boundary conditions) and the filtered
-    // state, recording the boundary program's tapes: 0..3 after the stages, 4 after the filter
+    // recompute the stage states q1..q4 (after their boundary conditions) and the end state,
+    // recording the boundary program's tapes: 0..3 after the stages, 4 after filter and SFD
     for (int s = 1; s <= 4; s++) {
-        TRY(rhs_stage(c, X[s - 1], X[0], X[s], s, c->nb, c->d1, c->tq, c->d2, c->delta));
+        TRY(rhs_stage_d(c, X[s - 1], X[0], X[s], s));
         TRY(bc_rec(c, X[s], s - 1));
     }
     if (c->nops > 0) {
         TRY(copy_set5(c, c->a_tmp, c->dx[4]));
         TRY(filter_set(c, set5(c, c->a_tmp), c->nb, 0.0, c->fct > 0 ? &c->d_params->dt : nullptr));
+        if (diff_sfd(c)) {
+            TRY(copy_set5(c, c->a_mscr, c->dxm));
+            TRY(sfd_set(c, set5(c, c->a_tmp), c->a_mscr));
+        }
         TRY(bc_rec(c, set5(c, c->a_tmp), 4));
     }
     TRY(bc_adj(c, set5(c, c->a_lam), 4));
+    if (diff_sfd(c)) {
+        TRY(before_launch(c, PC_OTHER));
+        k_sfd_adj<<<dim3(grid_for(c, c->npts), c->nb), kBlock, 0, c->stream>>>(
+            set5(c, c->a_lam), fset(c, c->a_lm, 5), c->chi, c->sfd_delta, c->is3d ? 5 : 4, c->npts, c->d_params);
+        TRY(after_launch(c));
+    }
     // filter^T, z -> y -> x; with the time blend lam = lam + b (F^T lam - lam)
     const int f5[5] = {0, 1, 2, 3, 4};
-    for (int d = 2; d >= 0; d--) {
+    for (int d = (c->is3d ? 2 : 1); d >= 0; d--) {
         if (!c->filt[d]) continue;
         if (c->fct > 0) {
             TRY(sweep_T(c, d, 4, c->a_lam, 5 * c->npts, f5, c->a_g, 5 * c->npts, f5, 5));
@@ -1706,6 +1879,7 @@ int adj_step(gatt_ctx *c, double dt)
             TRY(sweep_T(c, d, 4, c->a_lam, 5 * c->npts, f5, c->a_lam, 5 * c->npts, f5, 5));
         }
     }
+    TRY(zero_w(c, c->a_lam));  // 2-D: the filter leaves W alone
     // RK4: q4 = q0 + dt/6 k1 + dt/3 k2 + dt/3 k3 + dt/6 k4, q1 = q0 + dt/2 k1,
     // q2 = q0 + dt/2 k2, q3 = q0 + dt k3, k_s = F(q_{s-1})
     const StateSet A = set5(c, c->a_arg), G = set5(c, c->a_g);
@@ -1721,13 +1895,35 @@ int adj_step(gatt_ctx *c, double dt)
         TRY(axpby5(c, c->a_acc, c->a_acc, c->a_g, 1.0, 1.0));
         if (s > 0) TRY(copy_set5(c, c->a_prev, c->a_g));
     }
-    return copy_set5(c, c->a_lam, c->a_acc);
+    TRY(copy_set5(c, c->a_lam, c->a_acc));
+    return zero_w(c, c->a_lam);
+}
+
+// host vector [member][nv fields][point] <-> device sets: the state part into / from `q`
+// (a 5-field set), with SFD the mean part into / from `m`
+int upload_vec(gatt_ctx *c, double *q, double *m, const double *host)
+{
+    const int nv = diff_nv(c);
+    const size_t f5 = sizeof(double) * 5 * (size_t)c->npts, fv = sizeof(double) * nv * (size_t)c->npts;
+    CU(cudaMemcpy2DAsync(q, f5, host, fv, f5, c->nb, cudaMemcpyHostToDevice, c->stream));
+    if (nv == 10) CU(cudaMemcpy2DAsync(m, f5, host + 5 * c->npts, fv, f5, c->nb, cudaMemcpyHostToDevice, c->stream));
+    TRY(zero_w(c, q));
+    return nv == 10 ? zero_w(c, m) : GATT_OK;
+}
+
+int download_vec(gatt_ctx *c, double *host, const double *q, const double *m)
+{
+    const int nv = diff_nv(c);
+    const size_t f5 = sizeof(double) * 5 * (size_t)c->npts, fv = sizeof(double) * nv * (size_t)c->npts;
+    CU(cudaMemcpy2DAsync(host, fv, q, f5, f5, c->nb, cudaMemcpyDeviceToHost, c->stream));
+    if (nv == 10) CU(cudaMemcpy2DAsync(host + 5 * c->npts, fv, m, f5, f5, c->nb, cudaMemcpyDeviceToHost, c->stream));
+    return sync_stream(c);
 }
 
 int upload5(gatt_ctx *c, double *dst, const double *host)
 {
     CU(cudaMemcpyAsync(dst, host, sizeof(double) * 5 * (size_t)c->npts * c->nb, cudaMemcpyHostToDevice, c->stream));
-    return GATT_OK;
+    return zero_w(c, dst);
 }
 
 int download5(gatt_ctx *c, double *host, const double *src)
@@ -1754,16 +1950,18 @@ int rhs_vjp(gatt_ctx *c, const double *q, const double *a, double *lam)
     TRY(upload5(c, c->dx[0], q));
     TRY(upload5(c, c->a_arg, a));
     TRY(adj_rhs(c, set5(c, c->dx[0]), set5(c, c->a_arg), set5(c, c->a_g)));
+    TRY(zero_w(c, c->a_g));
     return download5(c, lam, c->a_g);
 }
 
 int jvp(gatt_ctx *c, int nsteps, double t0, double dt, const double *dq0, double *dqN)
 {
-    TRY(check_diff(c, false));
+    TRY(check_diff(c, false, true));
     if (nsteps < 1 || !(dt > 0) || !dq0 || !dqN) return fail(GATT_ERR_BADARG, "bad nsteps, dt or arrays");
     TRY(diff_alloc(c, false));
     TRY(state_to_set(c, state_set(c, 0), c->dx[0], true));
-    TRY(upload5(c, c->dy[0], dq0));
+    if (diff_sfd(c)) TRY(copy_set5(c, c->dxm, c->mean));
+    TRY(upload_vec(c, c->dy[0], c->dym, dq0));
     double t = t0;
     for (int s = 0; s < nsteps; s++) {
         TRY(set_params(c, 0, t, dt));
@@ -1772,57 +1970,71 @@ int jvp(gatt_ctx *c, int nsteps, double t0, double dt, const double *dq0, double
         t = t + dt;
     }
     TRY(state_to_set(c, state_set(c, 0), c->dx[0], false));
-    return download5(c, dqN, c->dy[0]);
+    if (diff_sfd(c)) TRY(copy_set5(c, c->mean, c->dxm));
+    return download_vec(c, dqN, c->dy[0], c->dym);
 }
 
-// Checkpointed reverse sweep: states every `every` steps are kept on the forward pass; each
-// segment is recomputed from its checkpoint (storing every step's start state), then its
-// steps are reversed.  Leaves the context state at the end of the forward run.
+// Checkpointed reverse sweep: states (and SFD means) every `every` steps are kept on the
+// forward pass; each segment is recomputed from its checkpoint (storing every step's start
+// state), then its steps are reversed.  Leaves the context state at the end of the forward run.
 int vjp(gatt_ctx *c, int nsteps, double t0, double dt, int every, const double *lamN, double *lam0)
 {
-    TRY(check_diff(c, true));
+    TRY(check_diff(c, true, true));
     if (nsteps < 1 || every < 1 || !(dt > 0) || !lamN || !lam0) return fail(GATT_ERR_BADARG, "bad nsteps, dt or arrays");
     TRY(diff_alloc(c, true));
+    const bool sfd = diff_sfd(c);
     const int nck = (nsteps + every - 1) / every, seg = std::min(every, nsteps);
-    const size_t st = 5 * (size_t)c->npts * c->nb;
-    if (c->a_nckpt < nck + 1) {
+    const size_t s5 = 5 * (size_t)c->npts * c->nb;  // one 5-field set of every member
+    const size_t st = (sfd ? 2 : 1) * s5;           // a checkpoint: state, then the SFD mean
+    if (c->a_nckpt < nck + 1 || (sfd && c->a_ckpt_sfd == false)) {
         cudaFree(c->a_ckpt);
         c->a_ckpt = nullptr;
         c->a_nckpt = 0;
         CU(cudaMalloc(&c->a_ckpt, sizeof(double) * st * (nck + 1)));
         c->a_nckpt = nck + 1;
+        c->a_ckpt_sfd = sfd;
     }
-    if (c->a_nseg < seg) {
+    if (c->a_nseg < seg || (sfd && c->a_seg_sfd == false)) {
         cudaFree(c->a_seg);
         c->a_seg = nullptr;
         c->a_nseg = 0;
         CU(cudaMalloc(&c->a_seg, sizeof(double) * st * seg));
         c->a_nseg = seg;
+        c->a_seg_sfd = sfd;
     }
+    auto save = [&](double *dst) -> int {
+        TRY(state_to_set(c, state_set(c, 0), dst, true));
+        return sfd ? copy_set5(c, dst + s5, c->mean) : GATT_OK;
+    };
+    auto restore = [&](const double *src) -> int {
+        TRY(state_to_set(c, state_set(c, 0), const_cast<double *>(src), false));
+        return sfd ? copy_set5(c, c->mean, src + s5) : GATT_OK;
+    };
     // forward: checkpoints at steps 0, every, 2*every, ...; slot nck keeps the final state
     for (int k = 0; k < nck; k++) {
-        TRY(state_to_set(c, state_set(c, 0), c->a_ckpt + st * k, true));
+        TRY(save(c->a_ckpt + st * k));
         const int len = std::min(every, nsteps - k * every);
         TRY(run_steps(c, len, t0 + (double)(k * every) * dt, dt, nullptr, false));
     }
-    TRY(state_to_set(c, state_set(c, 0), c->a_ckpt + st * nck, true));
-    TRY(upload5(c, c->a_lam, lamN));
+    TRY(save(c->a_ckpt + st * nck));
+    TRY(upload_vec(c, c->a_lam, c->a_lm, lamN));
     for (int k = nck - 1; k >= 0; k--) {
         const int len = std::min(every, nsteps - k * every);
-        TRY(state_to_set(c, state_set(c, 0), c->a_ckpt + st * k, false));
+        TRY(restore(c->a_ckpt + st * k));
         for (int i = 0; i < len; i++) {
-            TRY(state_to_set(c, state_set(c, 0), c->a_seg + st * i, true));
+            TRY(save(c->a_seg + st * i));
             if (i + 1 < len) TRY(run_steps(c, 1, t0 + (double)(k * every + i) * dt, dt, nullptr, false));
         }
         for (int i = len - 1; i >= 0; i--) {
             TRY(copy_set5(c, c->dx[0], c->a_seg + st * i));
+            if (sfd) TRY(copy_set5(c, c->dxm, c->a_seg + st * i + s5));
             TRY(set_params(c, 0, t0 + (double)(k * every + i) * dt, dt));
             TRY(adj_step(c, dt));
             TRY(sync_stream(c));
         }
     }
-    TRY(state_to_set(c, state_set(c, 0), c->a_ckpt + st * nck, false));
-    return download5(c, lam0, c->a_lam);
+    TRY(restore(c->a_ckpt + st * nck));
+    return download_vec(c, lam0, c->a_lam, c->a_lm);
 }
 
 
@@ -1950,6 +2162,8 @@ int gatt_create(gatt_ctx **out, int nx, int ny, int nz, int nbatch)
     {
         const char *pw = getenv("GATT_PW");
         c->pw_pipe = !(pw && !strcmp(pw, "plain"));
+        const char *my = getenv("GATT_MERGE_YZ");
+        c->merge_yz = !(my && !strcmp(my, "0"));
     }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -2013,7 +2227,8 @@ void gatt_destroy(gatt_ctx *c)
     for (double *p : c->dy) cudaFree(p);
     double *dbufs[] = {c->t_delta, c->t_d1, c->t_tq, c->t_d2, c->a_lam, c->a_acc, c->a_arg, c->a_prev, c->a_g,
                        c->a_lq, c->a_ld1, c->a_ltau, c->a_lvt, c->a_s1, c->a_s2, c->a_scr, c->a_ckpt, c->a_seg,
-                       c->t_P, c->a_lP, c->a_tape, c->a_tmp};
+                       c->t_P, c->a_lP, c->a_tape, c->a_tmp, c->g_d1, c->g_tq, c->g_d2, c->dxm, c->dym,
+                       c->a_lm, c->a_mscr};
     for (double *p : dbufs) cudaFree(p);
     for (double *p : bufs) cudaFree(p);
     cudaFree(c->d_ops); cudaFree(c->acc); cudaFree(c->d_params);
@@ -2481,6 +2696,7 @@ int gatt_selftest_pipeline_timeout(gatt_ctx *c)
     a.es = 1; a.os = 0; a.tiles_per_row = (c->nx + kLanes - 1) / kLanes;
     a.Rm = m.Rm; a.Q = m.Q; a.W = m.W; a.Wp = m.Wp; a.P = m.P; a.ltype = c->ltype[0];
     a.epi = EPI_STORE; a.dir = 0; a.nf = 1; a.ntiles = (a.nlines + kLanes - 1) / kLanes; a.njobs = a.ntiles;
+    a.fd_ntiles = make_fastdiv(a.ntiles); a.fd_nf = make_fastdiv(1); a.fd_tpr = make_fastdiv(a.tiles_per_row);
     a.err = c->d_err; a.ntypes = m.nTypes; a.tx_extra = 16;
     const int r = launch_psweep(c, m, 0, a, 1, PC_OTHER);
     if (r != GATT_OK) return r;

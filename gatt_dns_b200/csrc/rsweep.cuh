@@ -38,9 +38,10 @@ constexpr unsigned long long kWaitNs = 1000000000ull;
 // records of every line type (band rows [nTypes][N][Wp], records [nTypes][N][kQ]), the
 // mbarriers.
 __host__ __device__ __forceinline__ size_t psweep_stage_doubles(bool, int N) { return (size_t)N * kLanes; }
-__host__ __device__ __forceinline__ size_t psweep_smem_bytes(bool xd, int N, int P, int ntypes, int Wp, int nst)
+__host__ __device__ __forceinline__ size_t psweep_smem_bytes(bool xd, int N, int P, int ntypes, int Wp, int nst,
+                                                            int ntypes1 = 0)
 {
-    return (nst * psweep_stage_doubles(xd, N) + 3 * (size_t)P * kLanes + (size_t)ntypes * N * (Wp + kQ)) *
+    return (nst * psweep_stage_doubles(xd, N) + 3 * (size_t)P * kLanes + (size_t)(ntypes + ntypes1) * N * (Wp + kQ)) *
                sizeof(double) +
            nst * 8 + (xd ? 1024 : 0);  // x: room to align the ring to the 1 KB swizzle period
 }
@@ -258,7 +259,7 @@ __device__ __forceinline__ LineRef line_of(const SweepArgs &a, int tile, int lan
 // grid stride G; the stride is split the same way once, so that every later step is a few
 // adds and compares instead of run-time integer divisions (about twenty instructions each).
 struct JobCursor {
-    int tile, f, b, o, tx;
+    int tile, f, b, o, tx, part;
 };
 struct JobStride {
     int gt, gf, gb, go, gx, nouter;
@@ -266,24 +267,40 @@ struct JobStride {
 __device__ __forceinline__ JobCursor job_at(const SweepArgs &a, int j)
 {
     JobCursor c;
-    c.tile = j % a.ntiles;
-    const int fb = j / a.ntiles;
-    c.f = fb % a.nf;
-    c.b = fb / a.nf;
-    c.o = c.tile / a.tiles_per_row;
-    c.tx = c.tile % a.tiles_per_row;
+    if (a.parts == 2) {
+        // j = ((b * tiles_per_row + tx) * nf + f) * (nout0 + nout1) + r; r < nout0: y tile at
+        // z = r, else z tile at y = r - nout0 -- x-tile column by column, all fields of one
+        // column before the next
+        const int g = fdiv(j, a.fd_nout);
+        const int r = j - g * (a.nout0 + a.nout1);
+        const int h = fdiv(g, a.fd_nf);
+        c.f = g - h * a.nf;
+        c.b = fdiv(h, a.fd_tpr);
+        c.tx = h - c.b * a.tiles_per_row;
+        c.part = r >= a.nout0;
+        c.o = c.part ? r - a.nout0 : r;
+        c.tile = c.o * a.tiles_per_row + c.tx;
+        return c;
+    }
+    c.part = 0;
+    const int fb = fdiv(j, a.fd_ntiles);
+    c.tile = j - fb * a.ntiles;
+    c.b = fdiv(fb, a.fd_nf);
+    c.f = fb - c.b * a.nf;
+    c.o = fdiv(c.tile, a.fd_tpr);
+    c.tx = c.tile - c.o * a.tiles_per_row;
     return c;
 }
 __device__ __forceinline__ JobStride job_stride(const SweepArgs &a, int G)
 {
     JobStride s;
-    s.gt = G % a.ntiles;
-    const int q = G / a.ntiles;
-    s.gf = q % a.nf;
-    s.gb = q / a.nf;
-    s.go = s.gt / a.tiles_per_row;
-    s.gx = s.gt % a.tiles_per_row;
-    s.nouter = a.ntiles / a.tiles_per_row;
+    const int q = fdiv(G, a.fd_ntiles);
+    s.gt = G - q * a.ntiles;
+    s.gb = fdiv(q, a.fd_nf);
+    s.gf = q - s.gb * a.nf;
+    s.go = fdiv(s.gt, a.fd_tpr);
+    s.gx = s.gt - s.go * a.tiles_per_row;
+    s.nouter = fdiv(a.ntiles, a.fd_tpr);
     return s;
 }
 __device__ __forceinline__ void job_advance(JobCursor &c, const JobStride &s, const SweepArgs &a)
@@ -297,6 +314,7 @@ __device__ __forceinline__ void job_advance(JobCursor &c, const JobStride &s, co
     c.f += s.gf + carry;
     c.b += s.gb;
     if (c.f >= a.nf) { c.f -= a.nf; c.b++; }
+    c.part = 0;
 }
 
 // Line of a tile lane from a cursor (line_of without divisions).
@@ -312,8 +330,8 @@ __device__ __forceinline__ LineRef line_at(const SweepArgs &a, const JobCursor &
     } else {
         const int i = c.tx * kLanes + lane;
         r.valid = i < a.nx;
-        r.base = i + (long long)c.o * a.os;
-        r.s = a.es;
+        r.base = i + (long long)c.o * (c.part ? a.os1 : a.os);
+        r.s = c.part ? a.es1 : a.es;
         r.L = i + a.nx * c.o;
     }
     return r;
@@ -444,8 +462,10 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
     double *xs = psm + nst * stage_d;
     double *sRm = xs + 3 * P * kLanes;                   // coefficient copy, all line types
     double *sQ = sRm + (size_t)a.ntypes * N * WP;
+    double *sRm1 = sQ + (size_t)a.ntypes * N * kQ;       // part 1 (z lines of a y+z launch)
+    double *sQ1 = sRm1 + (size_t)(XD ? 0 : a.ntypes1) * N * WP;
     const uint32_t st0 = smem_u32(psm);
-    const uint32_t bar0 = smem_u32(sQ + (size_t)a.ntypes * N * kQ);
+    const uint32_t bar0 = smem_u32(sQ1 + (size_t)(XD ? 0 : a.ntypes1) * N * kQ);
     const int G = gridDim.x;
     if (st0 & 127u) {  // tensor copies need 128-byte aligned stages
         if (threadIdx.x == 0) *(volatile int *)a.err = 2;
@@ -468,11 +488,14 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
         } else {
             fence_proxy_async();
             mbar_expect_tx(bar, (uint32_t)(N * kLanes * sizeof(double) + a.tx_extra));
-            tma_load_5d(dst, &tmap, c.tx * kLanes, a.dir == 1 ? 0 : c.o, a.dir == 1 ? c.o : 0, a.in_slot[c.f], c.b,
-                        bar);
+            // part 1 of a y+z launch: z lines through the second map
+            const bool ydir = a.dir == 1 && !c.part;
+            const CUtensorMap *mp = c.part ? &omap : &tmap;
+            const int slot = c.part ? a.in_slot1[c.f] : a.in_slot[c.f];
+            tma_load_5d(dst, mp, c.tx * kLanes, ydir ? 0 : c.o, ydir ? c.o : 0, slot, c.b, bar);
             if (a.box2)  // second half of a line past one 256-row box
-                tma_load_5d(dst + (uint32_t)(a.box2 * kLanes * sizeof(double)), &tmap, c.tx * kLanes,
-                            a.dir == 1 ? a.box2 : c.o, a.dir == 1 ? c.o : a.box2, a.in_slot[c.f], c.b, bar);
+                tma_load_5d(dst + (uint32_t)(a.box2 * kLanes * sizeof(double)), mp, c.tx * kLanes,
+                            ydir ? a.box2 : c.o, ydir ? c.o : a.box2, slot, c.b, bar);
         }
     };
     if (threadIdx.x == 0)
@@ -485,6 +508,13 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
         const double2 *gQ = reinterpret_cast<const double2 *>(a.Q);
         for (int i = threadIdx.x; i < nR2; i += blockDim.x) reinterpret_cast<double2 *>(sRm)[i] = __ldg(gR + i);
         for (int i = threadIdx.x; i < nQ2; i += blockDim.x) reinterpret_cast<double2 *>(sQ)[i] = __ldg(gQ + i);
+        if (!XD && a.parts == 2) {
+            const int mR2 = a.ntypes1 * N * WP / 2, mQ2 = a.ntypes1 * N * kQ / 2;
+            const double2 *hR = reinterpret_cast<const double2 *>(a.Rm1);
+            const double2 *hQ = reinterpret_cast<const double2 *>(a.Q1);
+            for (int i = threadIdx.x; i < mR2; i += blockDim.x) reinterpret_cast<double2 *>(sRm1)[i] = __ldg(hR + i);
+            for (int i = threadIdx.x; i < mQ2; i += blockDim.x) reinterpret_cast<double2 *>(sQ1)[i] = __ldg(hQ + i);
+        }
     }
     __syncthreads();
 
@@ -510,10 +540,11 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
             if (threadIdx.x == 0 && j + nst * G < a.njobs) ahead = job_at(a, j + nst * G);
         }
         const int tile = cur.tile, f = cur.f, b = cur.b;
+        const bool p1 = !XD && cur.part;  // z lines of a y+z launch
         const LineRef lr = line_at<XD>(a, cur, lane);
-        const int t = lr.valid ? a.ltype[lr.L] : 0;
-        const double *Qt = sQ + (size_t)t * N * kQ;
-        const double *Rr = sRm + ((size_t)t * N + sp) * WP;
+        const int t = lr.valid ? (p1 ? a.ltype1 : a.ltype)[lr.L] : 0;
+        const double *Qt = (p1 ? sQ1 : sQ) + (size_t)t * N * kQ;
+        const double *Rr = (p1 ? sRm1 : sRm) + ((size_t)t * N + sp) * WP;
         const double *Qr = Qt + (size_t)sp * kQ;
         const double *stg = psm + s * stage_d;
         const bool late = !mbar_wait(bar0 + 8 * s, par);
@@ -586,7 +617,8 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
             if (threadIdx.x == 0 && j + nst * G < a.njobs) issue(ahead, s);
         } else {
             if (lr.valid) {
-                double *Gl = a.out + (long long)b * a.out_bstride + (long long)a.out_slot[f] * a.npts + lr.base;
+                double *Gl = a.out + (long long)b * a.out_bstride +
+                             (long long)(p1 ? a.out_slot1[f] : a.out_slot[f]) * a.npts + lr.base;
                 store_block<XD, RPB, !PER>(w, Gl, lr.s, sp, blend_on, blend, [&](int jj) { return lds(sp + jj); },
                                            a.Nreal);
             }

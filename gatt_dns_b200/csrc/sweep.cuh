@@ -37,6 +37,29 @@ constexpr int kMaxPyz = 24;  // row blocks of the pipelined y/z solver (768 thre
 
 enum SweepEpi { EPI_STORE = 0, EPI_BLEND = 1 };
 
+// Division by a divisor fixed for a launch (the job decoding of the persistent solvers):
+// floor(n / d) = (umulhi(n, m) + n) >> l for 0 <= n < 2^31, with l = ceil(log2 d) and
+// m = floor(2^32 (2^l - d) / d) + 1 (Granlund and Montgomery, PLDI 1994) -- a multiply-high,
+// an add and a shift instead of the twenty-odd instructions of a run-time integer division.
+struct FastDiv {
+    uint32_t d, m, l;
+};
+inline FastDiv make_fastdiv(uint32_t d)
+{
+    FastDiv f;
+    f.d = d;
+    uint32_t l = 0;
+    while ((1ull << l) < d) l++;
+    f.l = l;
+    f.m = (uint32_t)(((1ull << 32) * ((1ull << l) - d)) / d + 1);
+    return f;
+}
+__device__ __forceinline__ int fdiv(int n, const FastDiv &f)
+{
+    const uint32_t t = __umulhi((uint32_t)n, f.m);
+    return (int)((t + (uint32_t)n) >> f.l);
+}
+
 // Per-row coefficient record, in the kernel's uniform row semantics:
 //   forward  y(r) = (rhs(r) - fA(r) y(r-1)) * fB(r)
 //   backward x(r) = y(r) - bC(r) x(r+1)
@@ -79,6 +102,17 @@ struct SweepArgs {
     int ntypes;              // line types of the coefficient set
     int nst;                 // ring stages (1 .. kMaxStages)
     int Nreal;               // rows of a line that are stored (N, or fewer for padded lines)
+    FastDiv fd_ntiles, fd_nf, fd_tpr;  // dividers by ntiles, nf and tiles_per_row
+    // y and z lines in one launch (k_psweep, y/z form): parts = 2, part 1 the z lines.  The
+    // jobs of one x-tile column run y then z, so the z tiles find their input in L2.
+    int parts;               // 1, or 2
+    int nout0, nout1;        // tiles per x-tile column of part 0 (y: nz) and part 1 (z: ny)
+    FastDiv fd_nout;         // divider by nout0 + nout1
+    int in_slot1[16], out_slot1[16];
+    long long es1, os1;      // part 1's line and outer strides
+    const double *Rm1, *Q1;  // part 1's coefficients
+    const uint8_t *ltype1;
+    int ntypes1;
     int box2;                // y/z lines past 256 rows: rows per tensor box (two boxes), else 0
     int tx_extra;            // bytes added to every copy barrier's expected count: 0, except in
                              // gatt_selftest_pipeline_timeout (its waits must run out)

@@ -305,6 +305,36 @@ __global__ void k_adj_blend5(StateSet lam, StateSet z, const StepParams *sp, dou
     }
 }
 
+// Adjoint of the SFD relaxation (k_sfd, main.F90:381-402).  Per point and variable, with
+// x = dt chi and a = dt / Delta, the forward is m' = m + a (v - m), v' = v - x (v - m')
+// (Delta > 0; otherwise m' = m).  From the sensitivities (lv, lm) of (v', m') it returns
+// those of (v, m): with t = lm + x lv, lv <- (1 - x) lv + a t and lm <- (1 - a) t
+// (Delta > 0); lv <- (1 - x) lv and lm <- t (Delta <= 0).  The tangent is k_sfd itself (the
+// relaxation is linear in the state and the mean).
+__global__ void k_sfd_adj(StateSet lq, FieldSet lmean, const double *chi, double delta_sfd, int nvar, long long n,
+                          const StepParams *sp)
+{
+    const int b = blockIdx.y;
+    const double dt = sp->dt;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const double x = dt * chi[p];
+        for (int f = 0; f < 5; f++) {
+            if (nvar == 4 && f == 2) continue;
+            double *lmp = lmean.f(b, f) + p;
+            double *lvp = lq.v[f] + b * lq.bstride + p;
+            const double lv = *lvp, t = *lmp + x * *lvp;
+            if (delta_sfd > 0) {
+                const double a = dt / delta_sfd;
+                *lvp = (1.0 - x) * lv + a * t;
+                *lmp = (1.0 - a) * t;
+            } else {
+                *lvp = (1.0 - x) * lv;
+                *lmp = t;
+            }
+        }
+    }
+}
+
 #undef GATT_LOAD_D1
 
 }  // namespace gatt

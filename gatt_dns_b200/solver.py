@@ -267,19 +267,43 @@ class GattDNS:
         _lib.check(self.lib.gatt_rhs_vjp(self.h, _dp(qv), _dp(av), _dp(out)), "gatt_rhs_vjp")
         return self._unpack(out)
 
+    # step vectors of gatt_jvp / gatt_vjp: the five state fields, and with SFD the five mean
+    # fields (keys "mU" ... "mE") after them
+    _MEAN_KEYS = ("mU", "mV", "mW", "mR", "mE")
+
+    def _pack_vec(self, flows):
+        if not self.case.sfd_type:
+            return self._pack(flows)
+        if isinstance(flows, dict):
+            flows = [flows]
+        z = np.zeros(self.case.npts)
+        return np.concatenate([_f64(f[k]).ravel(order="F") if k in f else z
+                               for f in flows for k in ("U", "V", "W", "R", "E") + self._MEAN_KEYS])
+
+    def _unpack_vec(self, vec):
+        if not self.case.sfd_type:
+            return self._unpack(vec)
+        s = (self.case.nx, self.case.ny, self.case.nz)
+        n = self.case.npts
+        keys = ("U", "V", "W", "R", "E") + self._MEAN_KEYS
+        out = [{k: vec[(b * 10 + i) * n:(b * 10 + i + 1) * n].reshape(s, order="F") for i, k in enumerate(keys)}
+               for b in range(self.nbatch)]
+        return out if self.nbatch > 1 else out[0]
+
     def jvp(self, dq0, nsteps, t0, dt):
-        """Tangent over nsteps steps from the current state (which advances, as run())."""
-        dv = self._pack(dq0)
+        """Tangent over nsteps steps from the current state (which advances, as run()); with
+        SFD the vectors carry the mean's tangent under the keys mU ... mE."""
+        dv = self._pack_vec(dq0)
         out = np.zeros_like(dv)
         _lib.check(self.lib.gatt_jvp(self.h, nsteps, t0, dt, _dp(dv), _dp(out)), "gatt_jvp")
-        return self._unpack(out)
+        return self._unpack_vec(out)
 
     def vjp(self, lamN, nsteps, t0, dt, checkpoint_every=20):
-        """Adjoint over nsteps steps from the current state, checkpointed."""
-        lv = self._pack(lamN)
+        """Adjoint over nsteps steps from the current state, checkpointed (mean keys as jvp)."""
+        lv = self._pack_vec(lamN)
         out = np.zeros_like(lv)
         _lib.check(self.lib.gatt_vjp(self.h, nsteps, t0, dt, checkpoint_every, _dp(lv), _dp(out)), "gatt_vjp")
-        return self._unpack(out)
+        return self._unpack_vec(out)
 
     def autotune(self, reps=3):
         """Pick the fastest line-solve configuration per matrix set (gatt_autotune).
@@ -304,7 +328,7 @@ class GattDNS:
 
     def profile_kernels(self, t0, dt, nsteps=2):
         """Per kernel class: (mean ms per launch, launches per step), from CUDA events."""
-        n = 15
+        n = 17  # GATT_NPROF
         ms, la = np.zeros(n), np.zeros(n)
         _lib.check(self.lib.gatt_profile_kernels(self.h, t0, dt, nsteps, _dp(ms), _dp(la)), "gatt_profile_kernels")
         return {self.lib.gatt_profile_name(i).decode(): (float(ms[i]), float(la[i])) for i in range(n)}

@@ -181,12 +181,16 @@ int gatt_arnoldi(gatt_ctx *ctx, int m, int nsteps, double t0, double dt, double 
  * mode reconstruction of calcInstability.m:419 is left to the caller. */
 int gatt_arnoldi_vector(gatt_ctx *ctx, int b, int j, double *out);
 
-/* Tangent-linear and adjoint of the 3-D RHS and time step (no counterpart in the reference;
+/* Tangent-linear and adjoint of the RHS and time step (no counterpart in the reference;
  * the reference linearises only by finite differences, calcInstability.m:353-390).  They
- * cover 3-D cases whose step is RK4 + filter: no boundary-condition lists, no disturbances,
- * no SFD (GATT_ERR_STATE otherwise); the adjoint also needs matrix kinds 2..5.  Arrays are
- * host, nbatch*5*npts (member-major, then U, V, W, R, E).
- *   gatt_rhs_jvp: dk = F'(q) dq of nseq3d (nseq.F90:142-323)
+ * cover the whole step of 2-D and 3-D cases: RK4, boundary-condition program (lists,
+ * corners, disturbances), filter and SFD; the adjoint also needs matrix kinds 2..5.  Arrays
+ * are host, member-major: per member the five fields U, V, W, R, E of npts each (in 2-D the W
+ * components are ignored on input and zero on output).  With SFD (gatt_set_sfd, type > 0)
+ * the step maps the state and the mean, and the gatt_jvp / gatt_vjp vectors carry both:
+ * per member U, V, W, R, E, then the mean's U, V, W, R, E (nbatch*10*npts); those two need
+ * the mean set (gatt_upload_mean or a previous step), GATT_ERR_STATE otherwise.
+ *   gatt_rhs_jvp: dk = F'(q) dq of nseq2d / nseq3d (nseq.F90:10-323), nbatch*5*npts arrays
  *   gatt_rhs_vjp: lam = F'(q)^T a
  *   gatt_jvp:     dqN = (dPhi/dq) dq0 over nsteps steps of dt from the context state (which
  *                 advances to the end state, as gatt_run)
@@ -231,7 +235,7 @@ long long gatt_kernel_launches(gatt_ctx *ctx);
  * device time of one launch in ms[GATT_NPROF] and the launches per step in
  * launches[GATT_NPROF].  Advances the state like gatt_run.  gatt_profile_name(i) names
  * class i. */
-#define GATT_NPROF 15
+#define GATT_NPROF 17
 int gatt_profile_kernels(gatt_ctx *ctx, double t0, double dt, int nsteps, double *ms, double *launches);
 const char *gatt_profile_name(int cls);
 

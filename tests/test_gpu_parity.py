@@ -68,6 +68,9 @@ def get_case(name):
             _CASES[name] = cs.periodic_box(nxyz=(16, 288, 8))
         elif name == "box_x400":
             _CASES[name] = cs.periodic_box(nxyz=(400, 16, 8))
+        elif name == "box_yz32":
+            # y and z lines of equal length (one launch) and a partial x tile (24 of 32 lanes)
+            _CASES[name] = cs.periodic_box(nxyz=(24, 32, 32))
         elif name == "box_ragged":
             # 5040 points: the last 256-point chunk of the tensor-copy assembly is partial
             _CASES[name] = cs.periodic_box(nxyz=(20, 18, 14))
@@ -112,8 +115,8 @@ def test_line_solves(libs, monkeypatch, name, kind, solver):
     g.close()
 
 
-@pytest.mark.parametrize("name", ["box", "box_aniso", "box64", "lid", "lid64", "lid_tanh", "cavity2d", "cavity3d",
-                                  "cavity3d_32", "bl", "bl_cavity"])
+@pytest.mark.parametrize("name", ["box", "box_aniso", "box64", "box_yz32", "lid", "lid64", "lid_tanh", "cavity2d",
+                                  "cavity3d", "cavity3d_32", "bl", "bl_cavity"])
 def test_rhs(libs, name):
     c, g, o = pair(name)
     f = flow_for(c)
@@ -286,6 +289,31 @@ def test_assembly_paths_agree(libs, monkeypatch, name):
     for i in (1, 2):
         for k in KEYS:
             assert np.array_equal(out["pipe"][i][k], out["plain"][i][k]), (name, i, k)
+
+
+@pytest.mark.parametrize("name", ["box", "box64", "box_yz32", "box_aniso", "cavity3d", "bl"])
+def test_merged_yz_sweeps_match_separate_launches(libs, monkeypatch, name):
+    """The y and z derivative sweeps in one launch (the default where both directions' sets
+    allow it) and in two launches (GATT_MERGE_YZ=0, read when a context is created) solve
+    every line with the same arithmetic: states after three steps are equal bit for bit."""
+    from gatt_dns_b200.solver import GattDNS
+    c = get_case(name)
+    fa, fb = flow_for(c, seed=3), flow_for(c, seed=4)
+    dt = 0.2 * c.cfl_dt(fa["U"], fa["V"], fa["W"], 1.0)
+    out = {}
+    for mode in ("merged", "separate"):
+        if mode == "separate":
+            monkeypatch.setenv("GATT_MERGE_YZ", "0")
+        g = GattDNS(c, nbatch=2)
+        g.upload(fa, 0)
+        g.upload(fb, 1)
+        mc = g.run(3, 0.0, dt)
+        out[mode] = (mc, g.download(0), g.download(1))
+        g.close()
+    assert np.array_equal(out["merged"][0], out["separate"][0])
+    for i in (1, 2):
+        for k in KEYS:
+            assert np.array_equal(out["merged"][i][k], out["separate"][i][k]), (name, i, k)
 
 
 @pytest.mark.parametrize("name", ["lid", "cavity3d", "bl", "bl_cavity"])

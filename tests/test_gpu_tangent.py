@@ -199,18 +199,3 @@ def test_energy_gradient(cuda_lib, box):
     fd = (jp - jm) / (2 * h)
     ad = dot(grad, v)
     assert abs(ad - fd) < FD_TOL * abs(fd), (ad, fd)
-
-
-def test_unsupported_cases_are_refused(cuda_lib):
-    from gatt_dns_b200.solver import GattDNS
-    from gatt_dns_b200._lib import GattError
-    c = cs.lid_driven(n=24)  # 2-D
-    with GattDNS(c) as g:
-        f = cs.uniform_flow(c)
-        with pytest.raises(GattError):
-            g.rhs_jvp(f, f)
-    c = cs.cavity_channel(nx=24, ny=20, nz=8, sfd={"X": 0.05, "Delta": 10.0, "buffer": 6})  # SFD on
-    with GattDNS(c) as g:
-        f = cs.uniform_flow(c)
-        with pytest.raises(GattError):
-            g.jvp(f, 1, 0.0, 1e-3)
