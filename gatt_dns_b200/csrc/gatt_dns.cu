@@ -175,6 +175,10 @@ struct gatt_ctx {
     int *d_err = nullptr;
     bool pw_pipe = true;    // 3-D assembly fed by bulk copies (GATT_PW=plain: thread loads)
     bool merge_yz = true;   // y and z derivative sweeps in one launch where their sets allow (GATT_MERGE_YZ=0: no)
+    bool fuse_mc = true;    // max-change in the last filter sweep where nothing follows it (GATT_FUSE_MC=0: no)
+    bool visc_slabs = true; // stresses slab by slab, last first, after a merged y/z sweep (GATT_VISC_SLABS=0: no)
+    bool mc_done = false;   // set when a filter launch ran the max-change epilogue
+    bool yz_merged = false; // set when the last sweep_yz ran as one launch
     int bc_cluster = 0;     // CTAs per member for the boundary program (0: one CTA, k_bc)
     int bc_cluster_rec = 0, bc_cluster_tl = 0, bc_cluster_adj = 0;  // same, tape / tangent / adjoint
     long long bc_points = 0;  // point updates of one application of the program (sum over ops)
@@ -616,6 +620,7 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
     void *args[] = {&a, &map, &omap};
     TRY(before_launch(c, cls));
     CU(cudaLaunchKernel(k, dim3(grid), dim3(32 * m.P), args, smem, c->stream));
+    if (a.mc_acc) c->mc_done = true;
     return after_launch(c);
 }
 
@@ -624,7 +629,7 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
 // blend_dt: device dt for the filter blend (NULL = use `blend`).
 int sweep(gatt_ctx *c, int d, int kind, const double *in, long long in_bs, const int *in_slots,
           double *out, long long out_bs, const int *out_slots, int nf, int nmembers, double blend,
-          const double *blend_dt, int cls = PC_OTHER)
+          const double *blend_dt, int cls = PC_OTHER, const StateSet *mc_ref = nullptr)
 {
     const DevDir &m = c->mat[d][kind];
     if (!m.set || !c->lt_set[d]) return fail(GATT_ERR_STATE, "matrices not set for this direction");
@@ -650,6 +655,9 @@ int sweep(gatt_ctx *c, int d, int kind, const double *in, long long in_bs, const
     a.fd_ntiles = make_fastdiv(a.ntiles); a.fd_nf = make_fastdiv(nf); a.fd_tpr = make_fastdiv(a.tiles_per_row);
     a.err = c->d_err;
     a.ntypes = m.nTypes;
+    if (mc_ref && d > 0) {  // the max-change epilogue: only the pipelined y/z solver has it
+        a.mc_acc = c->acc; a.mc_ref = mc_ref->v[0]; a.mc_ref_bstride = mc_ref->bstride;
+    }
     if (m.family == FAM_PIPE && m.rpb) {
         int r = launch_psweep(c, m, d, a, nmembers, cls);
         if (r != GATT_ERR_STATE) return r;  // GATT_ERR_STATE: layout not expressible, use k_rsweep
@@ -731,8 +739,10 @@ int sweep_yz(gatt_ctx *c, const double *in, long long in_bs, const int *sy, cons
         a.fd_nout = make_fastdiv(c->nz + c->ny);
         a.err = c->d_err;
         const int r = launch_psweep(c, my, 1, a, nmembers, cls_yz, &mz);
+        c->yz_merged = r == GATT_OK;
         if (r != GATT_ERR_STATE) return r;  // GATT_ERR_STATE: layout refused, two launches
     }
+    c->yz_merged = false;
     TRY(sweep(c, 1, 0, in, in_bs, sy, out, out_bs, oy, nf, nmembers, 0, nullptr, cls_y));
     return sweep(c, 2, 0, in, in_bs, sz, out, out_bs, oz, nf, nmembers, 0, nullptr, cls_z);
 }
@@ -838,7 +848,17 @@ int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet
         TRY(sweep(c, 0, 0, qin, qbs, fin, d1, bd1, ox, 5, nmem, 0, nullptr, PC_D1X));
         TRY(sweep_yz(c, qin, qbs, fin, fin, d1, bd1, oy, oz, 5, nmem, PC_D1Y, PC_D1Z, PC_D1YZ));
         TRY(before_launch(c, PC_VISC));
-        k_visc3d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(c->ph, q, fset(c, d1, D3_N), fset(c, tq, T3_N), n);
+        if (c->yz_merged && c->visc_slabs) {
+            const int nsl = (c->nx + kLanes - 1) / kLanes;
+            const long long rows = (long long)nsl * c->ny * c->nz;
+            const int blocks = (int)std::min<long long>((rows + 7) / 8, (long long)c->nsm * 8);
+            k_visc3d_slabs<<<dim3(blocks, nmem), kBlock, 0, c->stream>>>(c->ph, q, fset(c, d1, D3_N),
+                                                                         fset(c, tq, T3_N), c->nx,
+                                                                         (long long)c->ny * c->nz, nsl);
+        } else {
+            k_visc3d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(c->ph, q, fset(c, d1, D3_N),
+                                                                          fset(c, tq, T3_N), n);
+        }
         TRY(after_launch(c));
         // second sweeps (nseq.F90:241-306)
         const int ix[4] = {T3_XX, T3_XY, T3_XZ, T3_QX}, sx[4] = {S3_TXXX, S3_TXYX, S3_TXZX, S3_HTX};
@@ -1173,15 +1193,23 @@ int apply_bc(gatt_ctx *c, const StateSet &q, int nmem)
 }
 
 // applyFilters2D/3D in place on set q (derivs.F90:303-552)
-int filter_set(gatt_ctx *c, const StateSet &q, int nmem, double blend, const double *blend_dt)
+// With mc_ref, the last filtered direction also reduces the max-change against mc_ref into
+// c->acc (when its launch can: c->mc_done tells).
+int filter_set(gatt_ctx *c, const StateSet &q, int nmem, double blend, const double *blend_dt,
+               const StateSet *mc_ref = nullptr)
 {
     const int f3[5] = {0, 1, 2, 3, 4}, f2[4] = {0, 1, 3, 4};
     const int *fl = c->is3d ? f3 : f2;
     const int nf = c->is3d ? 5 : 4;
     const int ndir = c->is3d ? 3 : 2;
+    int last = -1;
+    for (int d = 0; d < ndir; d++)
+        if (c->filt[d]) last = d;
+    c->mc_done = false;
     for (int d = 0; d < ndir; d++) {
         if (!c->filt[d]) continue;
-        TRY(sweep(c, d, 1, q.v[0], q.bstride, fl, q.v[0], q.bstride, fl, nf, nmem, blend, blend_dt, PC_FX + d));
+        TRY(sweep(c, d, 1, q.v[0], q.bstride, fl, q.v[0], q.bstride, fl, nf, nmem, blend, blend_dt, PC_FX + d,
+                  d == last ? mc_ref : nullptr));
     }
     return GATT_OK;
 }
@@ -1213,8 +1241,13 @@ int step_body(gatt_ctx *c)
         TRY(rhs_stage(c, s == 1 ? q0 : qs, q0, qs, s, nm, c->d1, c->tq, c->d2, c->delta));
         TRY(apply_bc(c, qst, nm));
     }
-    if (c->fct > 0) TRY(filter_set(c, qs, nm, 0.0, &c->d_params->dt));
-    else TRY(filter_set(c, qs, nm, 0.0, nullptr));
+    // nothing after the filter (no SFD, no boundary program): its last sweep can take the
+    // max-change (main.F90:413-418) in its epilogue; the state sets must be equally spaced
+    const bool mc_in_filter = c->fuse_mc && c->sfd_type == 0 && c->nops == 0 && c->is3d &&
+                              qs.v[1] - qs.v[0] == c->npts && q0.v[1] - q0.v[0] == c->npts;
+    if (c->fct > 0) TRY(filter_set(c, qs, nm, 0.0, &c->d_params->dt, mc_in_filter ? &q0 : nullptr));
+    else TRY(filter_set(c, qs, nm, 0.0, nullptr, mc_in_filter ? &q0 : nullptr));
+    const bool mc_done = mc_in_filter && c->mc_done;
     if (c->sfd_type > 0) {
         TRY(before_launch(c, PC_SFD));
         k_sfd<<<dim3(grid_for(c, c->npts), nm), kBlock, 0, c->stream>>>(qs, fset(c, c->mean, 5), c->chi, c->sfd_delta,
@@ -1222,9 +1255,11 @@ int step_body(gatt_ctx *c)
         TRY(after_launch(c));
     }
     TRY(apply_bc(c, qs, nm));
-    TRY(before_launch(c, PC_MAXCHANGE));
-    k_maxchange<<<dim3(grid_for(c, c->npts), nm), kBlock, 0, c->stream>>>(qs, q0, c->acc, c->npts);
-    TRY(after_launch(c));
+    if (!mc_done) {
+        TRY(before_launch(c, PC_MAXCHANGE));
+        k_maxchange<<<dim3(grid_for(c, c->npts), nm), kBlock, 0, c->stream>>>(qs, q0, c->acc, c->npts);
+        TRY(after_launch(c));
+    }
     TRY(before_launch(c, PC_MAXCHANGE));
     k_store_maxchange<<<1, 5 * nm < 1024 ? 5 * nm : 1024, 0, c->stream>>>(c->acc, c->hist, 5 * nm, c->d_params);
     return after_launch(c);
@@ -2164,6 +2199,10 @@ int gatt_create(gatt_ctx **out, int nx, int ny, int nz, int nbatch)
         c->pw_pipe = !(pw && !strcmp(pw, "plain"));
         const char *my = getenv("GATT_MERGE_YZ");
         c->merge_yz = !(my && !strcmp(my, "0"));
+        const char *fm = getenv("GATT_FUSE_MC");
+        c->fuse_mc = !(fm && !strcmp(fm, "0"));
+        const char *vs = getenv("GATT_VISC_SLABS");
+        c->visc_slabs = !(vs && !strcmp(vs, "0"));
     }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);

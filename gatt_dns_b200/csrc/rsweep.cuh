@@ -622,6 +622,32 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
                 store_block<XD, RPB, !PER>(w, Gl, lr.s, sp, blend_on, blend, [&](int jj) { return lds(sp + jj); },
                                            a.Nreal);
             }
+            if (a.mc_acc) {
+                // max |stored value - step start| over this warp's rows of the tile (the stage
+                // still holds the input: with the blend epilogue it is refilled only below)
+                unsigned long long mx = 0;
+                if (lr.valid) {
+                    const double *ref = a.mc_ref + (long long)b * a.mc_ref_bstride + (long long)a.in_slot[f] * a.npts +
+                                        lr.base;
+#pragma unroll
+                    for (int jj = 0; jj < RPB; jj++) {
+                        if (!PER && sp + jj >= a.Nreal) continue;
+                        double v = w[jj];
+                        if (blend_on) {
+                            const double o = lds(sp + jj);
+                            v = o + blend * (v - o);
+                        }
+                        const unsigned long long u = (unsigned long long)__double_as_longlong(
+                            fabs(v - ref[(long long)(sp + jj) * lr.s]));
+                        mx = u > mx ? u : mx;
+                    }
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    const unsigned long long u = __shfl_xor_sync(0xffffffffu, mx, o);
+                    mx = u > mx ? u : mx;
+                }
+                if (lane == 0) atomicMax(a.mc_acc + b * 5 + a.in_slot[f], mx);
+            }
             if (blend_on) {
                 __syncthreads();
                 if (threadIdx.x == 0 && j + nst * G < a.njobs) issue(ahead, s);

@@ -117,6 +117,12 @@ struct SweepArgs {
     int tx_extra;            // bytes added to every copy barrier's expected count: 0, except in
                              // gatt_selftest_pipeline_timeout (its waits must run out)
     int *err;                // set to 1 when a pipeline wait gives up (host-mapped)
+    // max-change epilogue (k_psweep, y/z form): the filter sweep that produces the step's final
+    // state also reduces max |out - ref| per member and field into mc_acc[member * 5 + field
+    // slot] (an unsigned 64-bit max on the IEEE bits, so a NaN wins); null: off
+    unsigned long long *mc_acc;
+    const double *mc_ref;    // the step's start state, field slots as in_slot
+    long long mc_ref_bstride;
 };
 
 __device__ __forceinline__ double sweep_blend(const SweepArgs &a)

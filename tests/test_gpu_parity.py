@@ -316,6 +316,32 @@ def test_merged_yz_sweeps_match_separate_launches(libs, monkeypatch, name):
             assert np.array_equal(out["merged"][i][k], out["separate"][i][k]), (name, i, k)
 
 
+@pytest.mark.parametrize("name", ["box", "box_yz32", "box_ragged"])
+def test_max_change_in_filter_matches_kernel(libs, monkeypatch, name):
+    """On cases where nothing follows the filter, its last sweep reduces the max-change in
+    its epilogue; GATT_FUSE_MC=0 (read when a context is created) keeps the separate
+    reduction kernel.  Both give the same max-change history and states, bit for bit."""
+    from gatt_dns_b200.solver import GattDNS
+    c = get_case(name)
+    fa, fb = flow_for(c, seed=3), flow_for(c, seed=4)
+    dt = 0.2 * c.cfl_dt(fa["U"], fa["V"], fa["W"], 1.0)
+    out = {}
+    for mode in ("fused", "kernel"):
+        if mode == "kernel":
+            monkeypatch.setenv("GATT_FUSE_MC", "0")
+        g = GattDNS(c, nbatch=2)
+        g.upload(fa, 0)
+        g.upload(fb, 1)
+        hist = [g.step(s * dt, dt) for s in range(3)]
+        out[mode] = (hist, g.download(0), g.download(1))
+        g.close()
+    for s in range(3):
+        assert np.array_equal(out["fused"][0][s], out["kernel"][0][s]), s
+    for i in (1, 2):
+        for k in KEYS:
+            assert np.array_equal(out["fused"][i][k], out["kernel"][i][k]), (name, i, k)
+
+
 @pytest.mark.parametrize("name", ["lid", "cavity3d", "bl", "bl_cavity"])
 def test_boundary_program_cluster_matches_single_cta(libs, monkeypatch, name):
     """The boundary program run by a cluster of CTAs per member (cluster barriers between
