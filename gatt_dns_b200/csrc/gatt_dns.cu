@@ -66,6 +66,8 @@ struct DevDir {
     int Np = 0;            // line length the pipelined solver runs: N, or N padded to 16 rows
     int rows = 0;          // rows of the kernel records uploaded (N, or Np for the padded solver)
     int rpb = 0;           // rows per block of the register-resident solver (0: shared-tile solver)
+    bool uband = false;    // cyclic, one type, every row the same band: the uniform-band solver
+    double band[16] = {};  // that band
     int family = 0;        // SweepFamily
     // the factors as given, repacked [type][row] ([type][row][diag] for R): kept to rebuild
     // the kernel records for another row-block partition (gatt_autotune)
@@ -176,9 +178,8 @@ struct gatt_ctx {
     bool pw_pipe = true;    // 3-D assembly fed by bulk copies (GATT_PW=plain: thread loads)
     bool merge_yz = true;   // y and z derivative sweeps in one launch where their sets allow (GATT_MERGE_YZ=0: no)
     bool fuse_mc = true;    // max-change in the last filter sweep where nothing follows it (GATT_FUSE_MC=0: no)
-    bool visc_slabs = true; // stresses slab by slab, last first, after a merged y/z sweep (GATT_VISC_SLABS=0: no)
+    bool uband_on = true;   // uniform-band solver where a set allows it (GATT_UBAND=0: no)
     bool mc_done = false;   // set when a filter launch ran the max-change epilogue
-    bool yz_merged = false; // set when the last sweep_yz ran as one launch
     int bc_cluster = 0;     // CTAs per member for the boundary program (0: one CTA, k_bc)
     int bc_cluster_rec = 0, bc_cluster_tl = 0, bc_cluster_adj = 0;  // same, tape / tangent / adjoint
     long long bc_points = 0;  // point updates of one application of the program (sum over ops)
@@ -320,6 +321,21 @@ void *pick_reg_kernel(int nR)
     default: return nullptr;
     }
 #undef GATT_REG_CASE
+}
+
+// The pipelined solver of cyclic lines whose rows all share one band (launch constants).
+template <bool XD>
+void *pick_ub_kernel(int nR)
+{
+    switch (nR) {
+    case 2: return (void *)k_psweep<XD, true, 2, kRPB, false, true>;
+    case 3: return (void *)k_psweep<XD, true, 3, kRPB, false, true>;
+    case 4: return (void *)k_psweep<XD, true, 4, kRPB, false, true>;
+    case 5: return (void *)k_psweep<XD, true, 5, kRPB, false, true>;
+    case 6: return (void *)k_psweep<XD, true, 6, kRPB, false, true>;
+    case 7: return (void *)k_psweep<XD, true, 7, kRPB, false, true>;
+    default: return nullptr;
+    }
 }
 
 // The pipelined x solver for more than 24 row blocks (800-thread bound).
@@ -468,6 +484,13 @@ int set_sweep_attributes()
                     CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
                     CU(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
                 }
+    for (int xd = 0; xd < 2; xd++)  // the uniform-band instantiations
+        for (int nR = 2; nR <= kMaxNRreg; nR++) {
+            void *k = xd ? pick_ub_kernel<true>(nR) : pick_ub_kernel<false>(nR);
+            if (!k) continue;
+            CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+            CU(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        }
     CU(cudaFuncSetAttribute((const void *)k_assemble3d_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)pw_smem_bytes(kPwStages)));
     return GATT_OK;
@@ -520,6 +543,14 @@ int upload_records(gatt_ctx *c, DevDir &m, int P, int rows = 0)
             }
         }
     }
+    // uniform band: cyclic, one type, every row's band equal to row 0's
+    m.uband = periodic && nTypes == 1 && W <= 16 && N == N0;
+    for (int r = 1; m.uband && r < N0; r++)
+        for (int k = 0; k < W; k++)
+            if (m.hR[(size_t)r * W + k] != m.hR[k]) m.uband = false;
+    memset(m.band, 0, sizeof(m.band));
+    if (m.uband)
+        for (int k = 0; k < W; k++) m.band[k] = m.hR[k];
     TRY(sync_stream(c));
     if (!m.Rm) CU(cudaMalloc(&m.Rm, hRm.size() * sizeof(double)));
     if (!m.Q) CU(cudaMalloc(&m.Q, hQ.size() * sizeof(double)));
@@ -538,7 +569,12 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
     const int N = m.rows;  // padded y/z lines: the box covers the padding (zero fill)
     const bool xd = d == 0;
     const int nt1 = m1 ? m1->nTypes : 0;  // part 1 (z lines of a y+z launch)
-    void *k = reg_kernel(true, xd, m.periodic != 0, m.nR, m.P > 24);  // 25 blocks: the 800-thread form
+    // uniform band (both parts the same band): launch constants instead of shared records
+    bool ub = m.uband && m.periodic && m.P <= 24 && c->uband_on;
+    if (ub && m1) ub = m1->uband && !memcmp(m.band, m1->band, sizeof(m.band));
+    void *k = ub ? (xd ? pick_ub_kernel<true>(m.nR) : pick_ub_kernel<false>(m.nR))
+                 : reg_kernel(true, xd, m.periodic != 0, m.nR, m.P > 24);  // 25 blocks: the 800-thread form
+    if (ub) memcpy(a.band, m.band, sizeof(a.band));
     if (!k) return GATT_ERR_STATE;
     // ring depth: the deepest ring that keeps the most CTAs resident (one stage suffices
     // when a tile's solve outlasts the next tile's copy)
@@ -739,10 +775,8 @@ int sweep_yz(gatt_ctx *c, const double *in, long long in_bs, const int *sy, cons
         a.fd_nout = make_fastdiv(c->nz + c->ny);
         a.err = c->d_err;
         const int r = launch_psweep(c, my, 1, a, nmembers, cls_yz, &mz);
-        c->yz_merged = r == GATT_OK;
         if (r != GATT_ERR_STATE) return r;  // GATT_ERR_STATE: layout refused, two launches
     }
-    c->yz_merged = false;
     TRY(sweep(c, 1, 0, in, in_bs, sy, out, out_bs, oy, nf, nmembers, 0, nullptr, cls_y));
     return sweep(c, 2, 0, in, in_bs, sz, out, out_bs, oz, nf, nmembers, 0, nullptr, cls_z);
 }
@@ -848,17 +882,7 @@ int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet
         TRY(sweep(c, 0, 0, qin, qbs, fin, d1, bd1, ox, 5, nmem, 0, nullptr, PC_D1X));
         TRY(sweep_yz(c, qin, qbs, fin, fin, d1, bd1, oy, oz, 5, nmem, PC_D1Y, PC_D1Z, PC_D1YZ));
         TRY(before_launch(c, PC_VISC));
-        if (c->yz_merged && c->visc_slabs) {
-            const int nsl = (c->nx + kLanes - 1) / kLanes;
-            const long long rows = (long long)nsl * c->ny * c->nz;
-            const int blocks = (int)std::min<long long>((rows + 7) / 8, (long long)c->nsm * 8);
-            k_visc3d_slabs<<<dim3(blocks, nmem), kBlock, 0, c->stream>>>(c->ph, q, fset(c, d1, D3_N),
-                                                                         fset(c, tq, T3_N), c->nx,
-                                                                         (long long)c->ny * c->nz, nsl);
-        } else {
-            k_visc3d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(c->ph, q, fset(c, d1, D3_N),
-                                                                          fset(c, tq, T3_N), n);
-        }
+        k_visc3d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(c->ph, q, fset(c, d1, D3_N), fset(c, tq, T3_N), n);
         TRY(after_launch(c));
         // second sweeps (nseq.F90:241-306)
         const int ix[4] = {T3_XX, T3_XY, T3_XZ, T3_QX}, sx[4] = {S3_TXXX, S3_TXYX, S3_TXZX, S3_HTX};
@@ -2201,8 +2225,8 @@ int gatt_create(gatt_ctx **out, int nx, int ny, int nz, int nbatch)
         c->merge_yz = !(my && !strcmp(my, "0"));
         const char *fm = getenv("GATT_FUSE_MC");
         c->fuse_mc = !(fm && !strcmp(fm, "0"));
-        const char *vs = getenv("GATT_VISC_SLABS");
-        c->visc_slabs = !(vs && !strcmp(vs, "0"));
+        const char *ubs = getenv("GATT_UBAND");
+        c->uband_on = !(ubs && !strcmp(ubs, "0"));
     }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);

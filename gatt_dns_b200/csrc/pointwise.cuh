@@ -116,31 +116,6 @@ __global__ void __launch_bounds__(256) k_visc3d(Phys ph, StateSet q, FieldSet d1
     }
 }
 
-// Stresses and heat fluxes, 3-D, one warp per row of 32 x-points, the rows taken x-slab by
-// x-slab (slab = 32 x-points, all y and z) from the last slab to the first.  The merged y/z
-// derivative sweep before it writes its gradients slab by slab, first to last, so the
-// gradients of the slabs it wrote last are read while still in L2.  Same arithmetic as
-// k_visc3d.
-__global__ void __launch_bounds__(256) k_visc3d_slabs(Phys ph, StateSet q, FieldSet d1, FieldSet tq, int nx,
-                                                      long long rows_per_slab, int nslabs)
-{
-    const int b = blockIdx.y;
-    const int lane = threadIdx.x & 31;
-    const double *E = q.v[4] + b * q.bstride;
-    const long long nrows = rows_per_slab * nslabs;
-    for (long long r = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); r < nrows;
-         r += (long long)gridDim.x * (blockDim.x >> 5)) {
-        const long long sl = r / rows_per_slab;
-        const int x = (int)(nslabs - 1 - sl) * 32 + lane;
-        if (x >= nx) continue;
-        const long long p = x + (long long)nx * (r - sl * rows_per_slab);
-        double o[T3_N];
-        visc3d_point(ph, E[p], [&](int i) { return d1.f(b, i)[p]; }, o);
-#pragma unroll
-        for (int i = 0; i < T3_N; i++) tq.f(b, i)[p] = o[i];
-    }
-}
-
 // Stresses and heat fluxes, 2-D (nseq.F90:77-85, 109-110)
 __global__ void k_visc2d(Phys ph, StateSet q, FieldSet d1, FieldSet tq, long long n)
 {

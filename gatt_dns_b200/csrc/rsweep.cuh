@@ -141,9 +141,10 @@ __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_
 // On entry w[k] = row p*RPB - (NR-1) + k of this thread's line; on return w[j] (j < RPB) =
 // the solution at row p*RPB + j.  Every thread of the CTA calls it (three or four barriers).
 // Rr: band rows of this block, Qt: the line type's row records, Qr = Qt + p*RPB records.
-template <bool PER, int NR, int RPB, bool LDG>
+template <bool PER, int NR, int RPB, bool LDG, bool UB = false>
 __device__ __forceinline__ void solve_block(double (&w)[RPB + 2 * (NR - 1)], const double *Rr, const double *Qt,
-                                            const double *Qr, double *xs, int lane, int p, int P)
+                                            const double *Qr, double *xs, int lane, int p, int P,
+                                            const double *band = nullptr)
 {
     constexpr int W = 2 * NR - 1;
     constexpr int H = NR - 1;
@@ -155,12 +156,18 @@ __device__ __forceinline__ void solve_block(double (&w)[RPB + 2 * (NR - 1)], con
 #pragma unroll
     for (int j = 0; j < RPB; j++) {
         double rc[W + 1];
-        const double2 *r2 = reinterpret_cast<const double2 *>(Rr + j * WP);
+        if constexpr (UB) {
+            // the same band on every row: launch constants (kernel parameter space)
 #pragma unroll
-        for (int v = 0; v < (W + 1) / 2; v++) {
-            const double2 x = ldc<LDG>(r2 + v);
-            rc[2 * v] = x.x;
-            rc[2 * v + 1] = x.y;
+            for (int v = 0; v < W; v++) rc[v] = band[v];
+        } else {
+            const double2 *r2 = reinterpret_cast<const double2 *>(Rr + j * WP);
+#pragma unroll
+            for (int v = 0; v < (W + 1) / 2; v++) {
+                const double2 x = ldc<LDG>(r2 + v);
+                rc[2 * v] = x.x;
+                rc[2 * v + 1] = x.y;
+            }
         }
         double acc = rc[NR - 1] * w[j + H];
 #pragma unroll
@@ -443,9 +450,11 @@ __global__ void __launch_bounds__(32 * kMaxP) k_rsweep(const SweepArgs a)
 // 256-thread CTAs resident (84 registers round up to two); the y/z 6-band filter spills at
 // 80 and keeps the plain 512-thread bound.  WIDE (x lines of 25 row blocks, up to 400 points):
 // an 800-thread bound, which holds a thread to 72 registers.
-template <bool XD, bool PER, int NR, int RPB, bool WIDE = false>
-__global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * kMaxP : 768)) k_psweep(const SweepArgs a, const __grid_constant__ CUtensorMap tmap,
-                                                                     const __grid_constant__ CUtensorMap omap)
+// UB: every row shares one band (a.band, launch constants; cyclic lines of one matrix type).
+template <bool XD, bool PER, int NR, int RPB, bool WIDE = false, bool UB = false>
+__global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * kMaxP : 768))
+    k_psweep(const __grid_constant__ SweepArgs a, const __grid_constant__ CUtensorMap tmap,
+             const __grid_constant__ CUtensorMap omap)
 {
     constexpr int H = NR - 1;
     constexpr int WP = (2 * NR - 1 + 3) / 4 * 4;
@@ -503,13 +512,13 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
             if (blockIdx.x + s * G < a.njobs) issue(job_at(a, blockIdx.x + s * G), s);
     // the coefficient records are read by every tile: copy them once while the first tiles land
     {
-        const int nR2 = a.ntypes * N * WP / 2, nQ2 = a.ntypes * N * kQ / 2;
+        const int nR2 = UB ? 0 : a.ntypes * N * WP / 2, nQ2 = a.ntypes * N * kQ / 2;
         const double2 *gR = reinterpret_cast<const double2 *>(a.Rm);
         const double2 *gQ = reinterpret_cast<const double2 *>(a.Q);
         for (int i = threadIdx.x; i < nR2; i += blockDim.x) reinterpret_cast<double2 *>(sRm)[i] = __ldg(gR + i);
         for (int i = threadIdx.x; i < nQ2; i += blockDim.x) reinterpret_cast<double2 *>(sQ)[i] = __ldg(gQ + i);
         if (!XD && a.parts == 2) {
-            const int mR2 = a.ntypes1 * N * WP / 2, mQ2 = a.ntypes1 * N * kQ / 2;
+            const int mR2 = UB ? 0 : a.ntypes1 * N * WP / 2, mQ2 = a.ntypes1 * N * kQ / 2;
             const double2 *hR = reinterpret_cast<const double2 *>(a.Rm1);
             const double2 *hQ = reinterpret_cast<const double2 *>(a.Q1);
             for (int i = threadIdx.x; i < mR2; i += blockDim.x) reinterpret_cast<double2 *>(sRm1)[i] = __ldg(hR + i);
@@ -592,7 +601,7 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
         // x: the stage also carries the results out, it is refilled after the stores
         if (!XD && !blend_on && threadIdx.x == 0 && j + nst * G < a.njobs) issue(ahead, s);
 
-        solve_block<PER, NR, RPB, false>(w, Rr, Qt, Qr, xs, lane, p, P);
+        solve_block<PER, NR, RPB, false, UB>(w, Rr, Qt, Qr, xs, lane, p, P, a.band);
         if (XD) {
             // results back into the stage (own rows, same swizzled places), then one tensor
             // store of the tile (lines past the last one are clipped by the copy engine)

@@ -120,6 +120,10 @@ struct SweepArgs {
     // max-change epilogue (k_psweep, y/z form): the filter sweep that produces the step's final
     // state also reduces max |out - ref| per member and field into mc_acc[member * 5 + field
     // slot] (an unsigned 64-bit max on the IEEE bits, so a NaN wins); null: off
+    // uniform band (k_psweep<..., UB = true>): every row of every line shares the band
+    // coefficients band[0 .. W) (cyclic lines of one matrix type); the kernel reads them as
+    // launch constants instead of per-row shared-memory records
+    double band[16];
     unsigned long long *mc_acc;
     const double *mc_ref;    // the step's start state, field slots as in_slot
     long long mc_ref_bstride;
