@@ -268,7 +268,7 @@ def arnoldi_sample(cs, GattDNS, case, base, members, m, nsteps, seed, label, dis
                           if world > 1 else "")}
 
 
-def adjoint_sample(cs, GattDNS, nsteps=20, every=5, shape=(400, 150, 64)):
+def adjoint_sample(cs, GattDNS, nsteps=200, every=20, shape=(400, 150, 64)):
     """Config 5 on its full grid, bounded sample: gradient of the perturbation kinetic energy
     J = 1/2 sum |u - u_base|^2 after nsteps steps with respect to the initial perturbation
     (seed 99, amplitude 1e-6), by the checkpointed adjoint; checked by a central difference
@@ -337,12 +337,18 @@ def kernel_functions(case, tuned):
     write once)."""
     fam_name = {"pipe": "k_psweep", "reg": "k_rsweep", "tile": "k_sweep"}
 
+    def uniform_band(m, kind):
+        # cyclic, one matrix type, every row the same band: the uniform-band instantiation
+        R = np.asarray(m.R if kind == 0 else m.Rf)
+        return bool(m.periodic) and m.nTypes == 1 and bool(np.all(R[:, :, 0] == R[0:1, :, 0]))
+
     def solver(d, kind):
         m = case.mats[d - 1]
         fam = tuned.get((d, kind), ("pipe",))[0]
         nR = m.nRHS if kind == 0 else m.nRHSf
-        return "%s<%s, %s, nR=%d>" % (fam_name[fam], "x" if d == 1 else "y/z",
-                                      "cyclic" if m.periodic else "banded", nR)
+        ub = ", uniform band" if fam == "pipe" and uniform_band(m, kind) else ""
+        return "%s<%s, %s, nR=%d%s>" % (fam_name[fam], "x" if d == 1 else "y/z",
+                                        "cyclic" if m.periodic else "banded", nR, ub)
 
     return {"sweep_d1_x": (solver(1, 0), 5 * 16), "sweep_d1_y": (solver(2, 0), 5 * 16),
             "sweep_d1_z": (solver(3, 0), 5 * 16), "sweep_d1_yz": (solver(2, 0), 10 * 16),
