@@ -179,6 +179,7 @@ struct gatt_ctx {
     bool merge_yz = true;   // y and z derivative sweeps in one launch where their sets allow (GATT_MERGE_YZ=0: no)
     bool fuse_mc = true;    // max-change in the last filter sweep where nothing follows it (GATT_FUSE_MC=0: no)
     bool uband_on = true;   // uniform-band solver where a set allows it (GATT_UBAND=0: no)
+    bool x_order = true;    // x tiles field-inner, last tile first (GATT_X_ORDER=0: tile-inner, first first)
     bool mc_done = false;   // set when a filter launch ran the max-change epilogue
     int bc_cluster = 0;     // CTAs per member for the boundary program (0: one CTA, k_bc)
     int bc_cluster_rec = 0, bc_cluster_tl = 0, bc_cluster_adj = 0;  // same, tape / tangent / adjoint
@@ -651,6 +652,12 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
         };
         if (!yzmap(&map, d)) return GATT_ERR_STATE;
         if (m1 && !yzmap(&omap, 2)) return GATT_ERR_STATE;  // part 1: the z lines
+    }
+    if (xd && c->x_order && a.nf > 1) {
+        // x tiles field-inner, last tile first: the cursor's fast index runs over the fields
+        a.xorder = 1; a.xtiles = a.ntiles;
+        a.ntiles = a.nf; a.nf = a.xtiles;
+        a.fd_ntiles = make_fastdiv(a.ntiles); a.fd_nf = make_fastdiv(a.nf);
     }
     const int grid = std::min(a.njobs, per_sm * c->nsm);
     void *args[] = {&a, &map, &omap};
@@ -2227,6 +2234,8 @@ int gatt_create(gatt_ctx **out, int nx, int ny, int nz, int nbatch)
         c->fuse_mc = !(fm && !strcmp(fm, "0"));
         const char *ubs = getenv("GATT_UBAND");
         c->uband_on = !(ubs && !strcmp(ubs, "0"));
+        const char *xos = getenv("GATT_X_ORDER");
+        c->x_order = !(xos && !strcmp(xos, "0"));
     }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);

@@ -324,6 +324,18 @@ __device__ __forceinline__ void job_advance(JobCursor &c, const JobStride &s, co
     c.part = 0;
 }
 
+// The (tile, field) a cursor stands for: itself, or, for x tiles taken field-inner and last
+// tile first (a.xorder), its fast index is the field and its slow index the reversed tile.
+__device__ __forceinline__ JobCursor xjob(const SweepArgs &a, JobCursor c)
+{
+    if (a.xorder) {
+        const int f = c.tile;
+        c.tile = a.xtiles - 1 - c.f;
+        c.f = f;
+    }
+    return c;
+}
+
 // Line of a tile lane from a cursor (line_of without divisions).
 template <bool XD>
 __device__ __forceinline__ LineRef line_at(const SweepArgs &a, const JobCursor &c, int lane)
@@ -493,7 +505,8 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
             bulk_wait_read0();  // the tile stored out of this stage has been read
             fence_proxy_async();
             mbar_expect_tx(bar, (uint32_t)(N * kLanes * sizeof(double) + a.tx_extra));
-            tma_load_5d(dst, &tmap, 0, c.tile * kLanes, 0, a.in_slot[c.f], c.b, bar);
+            const JobCursor cx = xjob(a, c);
+            tma_load_5d(dst, &tmap, 0, cx.tile * kLanes, 0, a.in_slot[cx.f], cx.b, bar);
         } else {
             fence_proxy_async();
             mbar_expect_tx(bar, (uint32_t)(N * kLanes * sizeof(double) + a.tx_extra));
@@ -548,9 +561,10 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
             cur = job_at(a, j);
             if (threadIdx.x == 0 && j + nst * G < a.njobs) ahead = job_at(a, j + nst * G);
         }
-        const int tile = cur.tile, f = cur.f, b = cur.b;
+        const JobCursor cj = XD ? xjob(a, cur) : cur;
+        const int tile = cj.tile, f = cj.f, b = cj.b;
         const bool p1 = !XD && cur.part;  // z lines of a y+z launch
-        const LineRef lr = line_at<XD>(a, cur, lane);
+        const LineRef lr = line_at<XD>(a, cj, lane);
         const int t = lr.valid ? (p1 ? a.ltype1 : a.ltype)[lr.L] : 0;
         const double *Qt = (p1 ? sQ1 : sQ) + (size_t)t * N * kQ;
         const double *Rr = (p1 ? sRm1 : sRm) + ((size_t)t * N + sp) * WP;

@@ -124,6 +124,11 @@ struct SweepArgs {
     // coefficients band[0 .. W) (cyclic lines of one matrix type); the kernel reads them as
     // launch constants instead of per-row shared-memory records
     double band[16];
+    // x tiles field-inner and last tile first (xorder = 1): the launch's job cursor then runs
+    // over (field, tile) instead of (tile, field) -- its "tiles" are the fields and its
+    // "fields" the xtiles tiles -- so that each tile's fields are taken together, starting
+    // from the points the preceding pointwise kernel wrote last (still in L2)
+    int xorder, xtiles;
     unsigned long long *mc_acc;
     const double *mc_ref;    // the step's start state, field slots as in_slot
     long long mc_ref_bstride;
