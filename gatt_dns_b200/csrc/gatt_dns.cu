@@ -581,8 +581,9 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
     // when a tile's solve outlasts the next tile's copy)
     int nst = 0, per_sm = 0;
     size_t smem = 0;
+    const int wps = ub ? 0 : m.Wp;  // the uniform-band solver keeps no band rows in shared memory
     for (int st = kMaxStages; st >= 1; st--) {
-        const size_t b = psweep_smem_bytes(xd, N, m.P, m.nTypes, m.Wp, st, nt1);
+        const size_t b = psweep_smem_bytes(xd, N, m.P, m.nTypes, wps, st, nt1);
         if (b > kMaxSmem) continue;
         const int r = resident_ctas(k, 32 * m.P, b);
         if (r > per_sm) { per_sm = r; nst = st; smem = b; }
@@ -592,7 +593,7 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
     // (128^3: x sweeps 7-14 % faster at two CTAs and two stages than at three and one)
     if (xd)
         for (int st = kMaxStages; st > nst; st--) {
-            const size_t b = psweep_smem_bytes(xd, N, m.P, m.nTypes, m.Wp, st);
+            const size_t b = psweep_smem_bytes(xd, N, m.P, m.nTypes, wps, st);
             const int r = b <= kMaxSmem ? resident_ctas(k, 32 * m.P, b) : 0;
             if (r >= 2) { per_sm = r; nst = st; smem = b; break; }
         }

@@ -481,10 +481,11 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
     // x: the swizzled ring starts on a 1 KB boundary (the host budgets the slack)
     double *psm = XD ? psm_raw + ((1024u - (smem_u32(psm_raw) & 1023u)) & 1023u) / sizeof(double) : psm_raw;
     double *xs = psm + nst * stage_d;
+    constexpr int WPs = UB ? 0 : WP;                     // band rows in shared memory (none: UB)
     double *sRm = xs + 3 * P * kLanes;                   // coefficient copy, all line types
-    double *sQ = sRm + (size_t)a.ntypes * N * WP;
+    double *sQ = sRm + (size_t)a.ntypes * N * WPs;
     double *sRm1 = sQ + (size_t)a.ntypes * N * kQ;       // part 1 (z lines of a y+z launch)
-    double *sQ1 = sRm1 + (size_t)(XD ? 0 : a.ntypes1) * N * WP;
+    double *sQ1 = sRm1 + (size_t)(XD ? 0 : a.ntypes1) * N * WPs;
     const uint32_t st0 = smem_u32(psm);
     const uint32_t bar0 = smem_u32(sQ1 + (size_t)(XD ? 0 : a.ntypes1) * N * kQ);
     const int G = gridDim.x;
