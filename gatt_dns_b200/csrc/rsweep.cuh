@@ -566,7 +566,8 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
         const int tile = cj.tile, f = cj.f, b = cj.b;
         const bool p1 = !XD && cur.part;  // z lines of a y+z launch
         const LineRef lr = line_at<XD>(a, cj, lane);
-        const int t = lr.valid ? (p1 ? a.ltype1 : a.ltype)[lr.L] : 0;
+        // one line type (every uniform-band set): no per-line type lookup
+        const int t = (UB || !lr.valid) ? 0 : (p1 ? a.ltype1 : a.ltype)[lr.L];
         const double *Qt = (p1 ? sQ1 : sQ) + (size_t)t * N * kQ;
         const double *Rr = (p1 ? sRm1 : sRm) + ((size_t)t * N + sp) * WP;
         const double *Qr = Qt + (size_t)sp * kQ;
