@@ -180,6 +180,8 @@ struct gatt_ctx {
     bool fuse_mc = true;    // max-change in the last filter sweep where nothing follows it (GATT_FUSE_MC=0: no)
     bool uband_on = true;   // uniform-band solver where a set allows it (GATT_UBAND=0: no)
     bool x_order = true;    // x tiles field-inner, last tile first (GATT_X_ORDER=0: tile-inner, first first)
+    bool visc_v2 = true;    // stresses two points per thread (GATT_VISC_V2=0: one)
+    bool fz_rev = true;     // last filter direction takes the fields in reverse order (GATT_FZ_REV=0: no)
     bool mc_done = false;   // set when a filter launch ran the max-change epilogue
     int bc_cluster = 0;     // CTAs per member for the boundary program (0: one CTA, k_bc)
     int bc_cluster_rec = 0, bc_cluster_tl = 0, bc_cluster_adj = 0;  // same, tape / tangent / adjoint
@@ -890,7 +892,13 @@ int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet
         TRY(sweep(c, 0, 0, qin, qbs, fin, d1, bd1, ox, 5, nmem, 0, nullptr, PC_D1X));
         TRY(sweep_yz(c, qin, qbs, fin, fin, d1, bd1, oy, oz, 5, nmem, PC_D1Y, PC_D1Z, PC_D1YZ));
         TRY(before_launch(c, PC_VISC));
-        k_visc3d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(c->ph, q, fset(c, d1, D3_N), fset(c, tq, T3_N), n);
+        if (c->visc_v2 && !(n & 1) && !(q.bstride & 1) && !((uintptr_t)q.v[4] & 15) && !((uintptr_t)d1 & 15) &&
+            !((uintptr_t)tq & 15))
+            k_visc3d_v2<<<dim3(grid_for(c, n / 2), nmem), kBlock, 0, c->stream>>>(c->ph, q, fset(c, d1, D3_N),
+                                                                             fset(c, tq, T3_N), n);
+        else
+            k_visc3d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(c->ph, q, fset(c, d1, D3_N),
+                                                                          fset(c, tq, T3_N), n);
         TRY(after_launch(c));
         // second sweeps (nseq.F90:241-306)
         const int ix[4] = {T3_XX, T3_XY, T3_XZ, T3_QX}, sx[4] = {S3_TXXX, S3_TXYX, S3_TXZX, S3_HTX};
@@ -1238,9 +1246,15 @@ int filter_set(gatt_ctx *c, const StateSet &q, int nmem, double blend, const dou
     for (int d = 0; d < ndir; d++)
         if (c->filt[d]) last = d;
     c->mc_done = false;
+    // a filter direction after another takes the fields in the reverse order: its first
+    // fields are the ones the previous direction wrote last (still in L2)
+    const int r3[5] = {4, 3, 2, 1, 0}, r2[4] = {4, 3, 1, 0};
+    const int *rl = c->is3d ? r3 : r2;
+    int nth = 0;
     for (int d = 0; d < ndir; d++) {
         if (!c->filt[d]) continue;
-        TRY(sweep(c, d, 1, q.v[0], q.bstride, fl, q.v[0], q.bstride, fl, nf, nmem, blend, blend_dt, PC_FX + d,
+        const int *sl = (c->fz_rev && (nth++ & 1)) ? rl : fl;
+        TRY(sweep(c, d, 1, q.v[0], q.bstride, sl, q.v[0], q.bstride, sl, nf, nmem, blend, blend_dt, PC_FX + d,
                   d == last ? mc_ref : nullptr));
     }
     return GATT_OK;
@@ -2237,6 +2251,10 @@ int gatt_create(gatt_ctx **out, int nx, int ny, int nz, int nbatch)
         c->uband_on = !(ubs && !strcmp(ubs, "0"));
         const char *xos = getenv("GATT_X_ORDER");
         c->x_order = !(xos && !strcmp(xos, "0"));
+        const char *v2s = getenv("GATT_VISC_V2");
+        c->visc_v2 = !(v2s && !strcmp(v2s, "0"));
+        const char *fzs = getenv("GATT_FZ_REV");
+        c->fz_rev = !(fzs && !strcmp(fzs, "0"));
     }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);

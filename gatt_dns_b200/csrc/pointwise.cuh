@@ -116,6 +116,27 @@ __global__ void __launch_bounds__(256) k_visc3d(Phys ph, StateSet q, FieldSet d1
     }
 }
 
+// Stresses and heat fluxes, 3-D, two consecutive points per thread through 16-byte loads and
+// stores (n even, every field 16-byte aligned); same arithmetic as k_visc3d.
+__global__ void __launch_bounds__(256) k_visc3d_v2(Phys ph, StateSet q, FieldSet d1, FieldSet tq, long long n)
+{
+    const int b = blockIdx.y;
+    const double2 *E = reinterpret_cast<const double2 *>(q.v[4] + b * q.bstride);
+    const long long n2 = n >> 1;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n2; p += (long long)gridDim.x * blockDim.x) {
+        double2 g[D3_N];
+#pragma unroll
+        for (int i = 0; i < D3_N; i++)
+            if (i != D3_RX && i != D3_RY && i != D3_RZ) g[i] = reinterpret_cast<const double2 *>(d1.f(b, i))[p];
+        const double2 e = E[p];
+        double o0[T3_N], o1[T3_N];
+        visc3d_point(ph, e.x, [&](int i) { return g[i].x; }, o0);
+        visc3d_point(ph, e.y, [&](int i) { return g[i].y; }, o1);
+#pragma unroll
+        for (int i = 0; i < T3_N; i++) reinterpret_cast<double2 *>(tq.f(b, i))[p] = make_double2(o0[i], o1[i]);
+    }
+}
+
 // Stresses and heat fluxes, 2-D (nseq.F90:77-85, 109-110)
 __global__ void k_visc2d(Phys ph, StateSet q, FieldSet d1, FieldSet tq, long long n)
 {

@@ -374,6 +374,30 @@ def test_x_tile_order_matches_tile_inner(libs, monkeypatch, name):
             assert np.array_equal(out["field_inner"][i][k], out["tile_inner"][i][k]), (name, i, k)
 
 
+@pytest.mark.parametrize("env", ["GATT_VISC_V2", "GATT_FZ_REV"])
+@pytest.mark.parametrize("name", ["box", "box_ragged", "box_odd", "cavity3d"])
+def test_stress_and_filter_order_variants_match(libs, monkeypatch, env, name):
+    """The two-points-per-thread stress kernel and the reversed field order of every second
+    filter direction (the defaults) against their plain forms (env var = 0): same arithmetic
+    on every point and line, so states after three steps are equal bit for bit."""
+    from gatt_dns_b200.solver import GattDNS
+    c = get_case(name)
+    f = flow_for(c, seed=3)
+    dt = 0.2 * c.cfl_dt(f["U"], f["V"], f["W"], 1.0)
+    out = {}
+    for mode in ("default", "plain"):
+        if mode == "plain":
+            monkeypatch.setenv(env, "0")
+        g = GattDNS(c)
+        g.upload(f)
+        mc = g.run(3, 0.0, dt)
+        out[mode] = (mc, g.download())
+        g.close()
+    assert np.array_equal(out["default"][0], out["plain"][0])
+    for k in KEYS:
+        assert np.array_equal(out["default"][1][k], out["plain"][1][k]), (name, env, k)
+
+
 @pytest.mark.parametrize("name", ["box", "box_yz32", "box_ragged"])
 def test_max_change_in_filter_matches_kernel(libs, monkeypatch, name):
     """On cases where nothing follows the filter, its last sweep reduces the max-change in
