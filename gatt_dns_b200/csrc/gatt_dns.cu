@@ -68,6 +68,7 @@ struct DevDir {
     int rpb = 0;           // rows per block of the register-resident solver (0: shared-tile solver)
     bool uband = false;    // cyclic, one type, every row the same band: the uniform-band solver
     double band[16] = {};  // that band
+    double cac[2] = {};    // and the corner couplings (cA, cC) of its row 0
     int family = 0;        // SweepFamily
     // the factors as given, repacked [type][row] ([type][row][diag] for R): kept to rebuild
     // the kernel records for another row-block partition (gatt_autotune)
@@ -181,6 +182,7 @@ struct gatt_ctx {
     bool uband_on = true;   // uniform-band solver where a set allows it (GATT_UBAND=0: no)
     bool x_order = true;    // x tiles field-inner, last tile first (GATT_X_ORDER=0: tile-inner, first first)
     bool visc_v2 = true;    // stresses two points per thread (GATT_VISC_V2=0: one)
+    bool x_compact = true;  // compact shared memory for the uniform-band x solver (GATT_X_COMPACT=0: no)
     bool fz_rev = true;     // last filter direction takes the fields in reverse order (GATT_FZ_REV=0: no)
     bool mc_done = false;   // set when a filter launch ran the max-change epilogue
     int bc_cluster = 0;     // CTAs per member for the boundary program (0: one CTA, k_bc)
@@ -552,8 +554,11 @@ int upload_records(gatt_ctx *c, DevDir &m, int P, int rows = 0)
         for (int k = 0; k < W; k++)
             if (m.hR[(size_t)r * W + k] != m.hR[k]) m.uband = false;
     memset(m.band, 0, sizeof(m.band));
-    if (m.uband)
+    if (m.uband) {
         for (int k = 0; k < W; k++) m.band[k] = m.hR[k];
+        m.cac[0] = m.hA[0];  // derivs.F90:792-793
+        m.cac[1] = m.hC[0];
+    }
     TRY(sync_stream(c));
     if (!m.Rm) CU(cudaMalloc(&m.Rm, hRm.size() * sizeof(double)));
     if (!m.Q) CU(cudaMalloc(&m.Q, hQ.size() * sizeof(double)));
@@ -577,7 +582,11 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
     if (ub && m1) ub = m1->uband && !memcmp(m.band, m1->band, sizeof(m.band));
     void *k = ub ? (xd ? pick_ub_kernel<true>(m.nR) : pick_ub_kernel<false>(m.nR))
                  : reg_kernel(true, xd, m.periodic != 0, m.nR, m.P > 24);  // 25 blocks: the 800-thread form
-    if (ub) memcpy(a.band, m.band, sizeof(a.band));
+    if (ub) {
+        memcpy(a.band, m.band, sizeof(a.band));
+        memcpy(a.cac, m.cac, sizeof(a.cac));
+    }
+    const bool cmp = ub && xd && c->x_compact;  // the compact shared-memory layout
     if (!k) return GATT_ERR_STATE;
     // ring depth: the deepest ring that keeps the most CTAs resident (one stage suffices
     // when a tile's solve outlasts the next tile's copy)
@@ -585,20 +594,23 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
     size_t smem = 0;
     const int wps = ub ? 0 : m.Wp;  // the uniform-band solver keeps no band rows in shared memory
     for (int st = kMaxStages; st >= 1; st--) {
-        const size_t b = psweep_smem_bytes(xd, N, m.P, m.nTypes, wps, st, nt1);
+        const size_t b = psweep_smem_bytes(xd, N, m.P, m.nTypes, wps, st, nt1, cmp);
         if (b > kMaxSmem) continue;
         const int r = resident_ctas(k, 32 * m.P, b);
         if (r > per_sm) { per_sm = r; nst = st; smem = b; }
     }
     // x tiles hold their stage through the solve and the tensor store, so only a second stage
-    // lets the next tile load meanwhile: take the deepest ring that keeps two CTAs per SM
-    // (128^3: x sweeps 7-14 % faster at two CTAs and two stages than at three and one)
-    if (xd)
-        for (int st = kMaxStages; st > nst; st--) {
-            const size_t b = psweep_smem_bytes(xd, N, m.P, m.nTypes, wps, st);
+    // lets the next tile load meanwhile: among rings of two stages or more, the most resident
+    // CTAs, then the deepest ring (128^3: x sweeps 7-14 % faster at two CTAs and two stages
+    // than at three and one)
+    if (xd) {
+        int best = 0;
+        for (int st = kMaxStages; st >= 2; st--) {
+            const size_t b = psweep_smem_bytes(xd, N, m.P, m.nTypes, wps, st, 0, cmp);
             const int r = b <= kMaxSmem ? resident_ctas(k, 32 * m.P, b) : 0;
-            if (r >= 2) { per_sm = r; nst = st; smem = b; break; }
+            if (r > best) { best = per_sm = r; nst = st; smem = b; }
         }
+    }
     if (nst == 0 || per_sm < 1) return GATT_ERR_STATE;
     a.nst = nst;
     // 16-byte aligned field starts, even strides (tensor maps)
@@ -2253,6 +2265,8 @@ int gatt_create(gatt_ctx **out, int nx, int ny, int nz, int nbatch)
         c->x_order = !(xos && !strcmp(xos, "0"));
         const char *v2s = getenv("GATT_VISC_V2");
         c->visc_v2 = !(v2s && !strcmp(v2s, "0"));
+        const char *xcs = getenv("GATT_X_COMPACT");
+        c->x_compact = !(xcs && !strcmp(xcs, "0"));
         const char *fzs = getenv("GATT_FZ_REV");
         c->fz_rev = !(fzs && !strcmp(fzs, "0"));
     }

@@ -38,12 +38,15 @@ constexpr unsigned long long kWaitNs = 1000000000ull;
 // records of every line type (band rows [nTypes][N][Wp], records [nTypes][N][kQ]), the
 // mbarriers.
 __host__ __device__ __forceinline__ size_t psweep_stage_doubles(bool, int N) { return (size_t)N * kLanes; }
+// cmp: the compact layout of the uniform-band x solver (records of kQc doubles, two exchange
+// regions, no alignment slack: its shared window must start on the 1 KB swizzle period).
 __host__ __device__ __forceinline__ size_t psweep_smem_bytes(bool xd, int N, int P, int ntypes, int Wp, int nst,
-                                                            int ntypes1 = 0)
+                                                            int ntypes1 = 0, bool cmp = false)
 {
-    return (nst * psweep_stage_doubles(xd, N) + 3 * (size_t)P * kLanes + (size_t)(ntypes + ntypes1) * N * (Wp + kQ)) *
+    return (nst * psweep_stage_doubles(xd, N) + (cmp ? 2 : 3) * (size_t)P * kLanes +
+            (size_t)(ntypes + ntypes1) * N * (Wp + (cmp ? 6 : kQ))) *
                sizeof(double) +
-           nst * 8 + (xd ? 1024 : 0);  // x: room to align the ring to the 1 KB swizzle period
+           nst * 8 + (xd && !cmp ? 1024 : 0);  // x: room to align the ring to the 1 KB swizzle period
 }
 
 // Coefficient load: read-only data path (global records) or plain (shared-memory copy).
@@ -141,14 +144,19 @@ __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_
 // On entry w[k] = row p*RPB - (NR-1) + k of this thread's line; on return w[j] (j < RPB) =
 // the solution at row p*RPB + j.  Every thread of the CTA calls it (three or four barriers).
 // Rr: band rows of this block, Qt: the line type's row records, Qr = Qt + p*RPB records.
-template <bool PER, int NR, int RPB, bool LDG, bool UB = false>
+// CMP (compact shared memory, the uniform-band x solver): records of kQc doubles per row, the
+// corner couplings (cA, cC) in cac[] (launch constants), two exchange regions of P x 32.
+constexpr int kQc = 6;
+template <bool PER, int NR, int RPB, bool LDG, bool UB = false, bool CMP = false>
 __device__ __forceinline__ void solve_block(double (&w)[RPB + 2 * (NR - 1)], const double *Rr, const double *Qt,
                                             const double *Qr, double *xs, int lane, int p, int P,
-                                            const double *band = nullptr)
+                                            const double *band = nullptr, const double *cac = nullptr)
 {
     constexpr int W = 2 * NR - 1;
     constexpr int H = NR - 1;
     constexpr int WP = (W + 3) / 4 * 4;
+    constexpr int kQ = CMP ? kQc : ::gatt::kQ;  // record stride
+    constexpr int DR = CMP ? 1 : 2;              // exchange region of the cyclic D-dot partials
 
     // ---- band product; forward recurrence (non-cyclic) or D-dot (cyclic) ----------------
     // row j's result goes to slot j: slot j is not read by rows after j.
@@ -186,11 +194,15 @@ __device__ __forceinline__ void solve_block(double (&w)[RPB + 2 * (NR - 1)], con
 
     if (PER) {
         // ---- x(1) = D . rhs, corner terms, reduced forward recurrence (derivs.F90:786-799)
-        xs[(2 * P + p) * kLanes + lane] = dot;
+        // (the compact layout keeps the partials in the backward region: they are read before
+        // the next barrier, and that region is written only after it)
+        xs[(DR * P + p) * kLanes + lane] = dot;
         __syncthreads();
-        double x1 = xs[(2 * P) * kLanes + lane];
-        for (int k = 1; k < P; k++) x1 = x1 + xs[(2 * P + k) * kLanes + lane];
-        const double2 cc = ldc<LDG>(reinterpret_cast<const double2 *>(Qt + kQcA));  // row 0: (cA, cC)
+        double x1 = xs[(DR * P) * kLanes + lane];
+        for (int k = 1; k < P; k++) x1 = x1 + xs[(DR * P + k) * kLanes + lane];
+        double2 cc;  // row 0: (cA, cC)
+        if constexpr (CMP) cc = make_double2(cac[0], cac[1]);
+        else cc = ldc<LDG>(reinterpret_cast<const double2 *>(Qt + kQcA));
         yprev = 0.0;
 #pragma unroll
         for (int j = 0; j < RPB; j++) {
@@ -478,13 +490,22 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
     const int sp = p * RPB;
     const size_t stage_d = psweep_stage_doubles(XD, N);
     const int nst = a.nst;
-    // x: the swizzled ring starts on a 1 KB boundary (the host budgets the slack)
-    double *psm = XD ? psm_raw + ((1024u - (smem_u32(psm_raw) & 1023u)) & 1023u) / sizeof(double) : psm_raw;
+    // compact layout: the uniform-band x solver (records of kQc doubles, two exchange regions)
+    constexpr bool CMP = UB && XD;
+    constexpr int KQS = CMP ? kQc : kQ;
+    // x: the swizzled ring starts on a 1 KB boundary (the host budgets the slack, except for
+    // the compact layout, which needs the shared window itself to start there)
+    const uint32_t pad = XD ? ((1024u - (smem_u32(psm_raw) & 1023u)) & 1023u) : 0u;
+    if (CMP && pad) {
+        if (threadIdx.x == 0) *(volatile int *)a.err = 2;
+        return;
+    }
+    double *psm = psm_raw + pad / sizeof(double);
     double *xs = psm + nst * stage_d;
     constexpr int WPs = UB ? 0 : WP;                     // band rows in shared memory (none: UB)
-    double *sRm = xs + 3 * P * kLanes;                   // coefficient copy, all line types
+    double *sRm = xs + (CMP ? 2 : 3) * P * kLanes;       // coefficient copy, all line types
     double *sQ = sRm + (size_t)a.ntypes * N * WPs;
-    double *sRm1 = sQ + (size_t)a.ntypes * N * kQ;       // part 1 (z lines of a y+z launch)
+    double *sRm1 = sQ + (size_t)a.ntypes * N * KQS;      // part 1 (z lines of a y+z launch)
     double *sQ1 = sRm1 + (size_t)(XD ? 0 : a.ntypes1) * N * WPs;
     const uint32_t st0 = smem_u32(psm);
     const uint32_t bar0 = smem_u32(sQ1 + (size_t)(XD ? 0 : a.ntypes1) * N * kQ);
@@ -526,11 +547,15 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
             if (blockIdx.x + s * G < a.njobs) issue(job_at(a, blockIdx.x + s * G), s);
     // the coefficient records are read by every tile: copy them once while the first tiles land
     {
-        const int nR2 = UB ? 0 : a.ntypes * N * WP / 2, nQ2 = a.ntypes * N * kQ / 2;
+        const int nR2 = UB ? 0 : a.ntypes * N * WP / 2, nQ2 = a.ntypes * N * KQS / 2;
         const double2 *gR = reinterpret_cast<const double2 *>(a.Rm);
         const double2 *gQ = reinterpret_cast<const double2 *>(a.Q);
         for (int i = threadIdx.x; i < nR2; i += blockDim.x) reinterpret_cast<double2 *>(sRm)[i] = __ldg(gR + i);
-        for (int i = threadIdx.x; i < nQ2; i += blockDim.x) reinterpret_cast<double2 *>(sQ)[i] = __ldg(gQ + i);
+        for (int i = threadIdx.x; i < nQ2; i += blockDim.x) {
+            // compact: the first kQc doubles of every kQ-double record
+            const int gi = CMP ? (i / (kQc / 2)) * (kQ / 2) + i % (kQc / 2) : i;
+            reinterpret_cast<double2 *>(sQ)[i] = __ldg(gQ + gi);
+        }
         if (!XD && a.parts == 2) {
             const int mR2 = UB ? 0 : a.ntypes1 * N * WP / 2, mQ2 = a.ntypes1 * N * kQ / 2;
             const double2 *hR = reinterpret_cast<const double2 *>(a.Rm1);
@@ -568,9 +593,9 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
         const LineRef lr = line_at<XD>(a, cj, lane);
         // one line type (every uniform-band set): no per-line type lookup
         const int t = (UB || !lr.valid) ? 0 : (p1 ? a.ltype1 : a.ltype)[lr.L];
-        const double *Qt = (p1 ? sQ1 : sQ) + (size_t)t * N * kQ;
+        const double *Qt = (p1 ? sQ1 : sQ) + (size_t)t * N * KQS;
         const double *Rr = (p1 ? sRm1 : sRm) + ((size_t)t * N + sp) * WP;
-        const double *Qr = Qt + (size_t)sp * kQ;
+        const double *Qr = Qt + (size_t)sp * KQS;
         const double *stg = psm + s * stage_d;
         const bool late = !mbar_wait(bar0 + 8 * s, par);
 
@@ -617,7 +642,7 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
         // x: the stage also carries the results out, it is refilled after the stores
         if (!XD && !blend_on && threadIdx.x == 0 && j + nst * G < a.njobs) issue(ahead, s);
 
-        solve_block<PER, NR, RPB, false, UB>(w, Rr, Qt, Qr, xs, lane, p, P, a.band);
+        solve_block<PER, NR, RPB, false, UB, CMP>(w, Rr, Qt, Qr, xs, lane, p, P, a.band, a.cac);
         if (XD) {
             // results back into the stage (own rows, same swizzled places), then one tensor
             // store of the tile (lines past the last one are clipped by the copy engine)

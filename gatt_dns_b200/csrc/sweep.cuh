@@ -124,6 +124,7 @@ struct SweepArgs {
     // coefficients band[0 .. W) (cyclic lines of one matrix type); the kernel reads them as
     // launch constants instead of per-row shared-memory records
     double band[16];
+    double cac[2];           // uniform-band cyclic sets: the corner couplings (cA, cC) of row 0
     // x tiles field-inner and last tile first (xorder = 1): the launch's job cursor then runs
     // over (field, tile) instead of (tile, field) -- its "tiles" are the fields and its
     // "fields" the xtiles tiles -- so that each tile's fields are taken together, starting
