@@ -183,6 +183,7 @@ struct gatt_ctx {
     bool x_order = true;    // x tiles field-inner, last tile first (GATT_X_ORDER=0: tile-inner, first first)
     bool visc_v2 = true;    // stresses two points per thread (GATT_VISC_V2=0: one)
     bool x_compact = true;  // compact shared memory for the uniform-band x solver (GATT_X_COMPACT=0: no)
+    bool x_wstore = true;   // x tiles stored chunk by chunk by their warps (GATT_X_WSTORE=0: by one thread)
     bool fz_rev = true;     // last filter direction takes the fields in reverse order (GATT_FZ_REV=0: no)
     bool mc_done = false;   // set when a filter launch ran the max-change epilogue
     int bc_cluster = 0;     // CTAs per member for the boundary program (0: one CTA, k_bc)
@@ -624,20 +625,23 @@ int launch_psweep(gatt_ctx *c, const DevDir &m, int d, SweepArgs &a, int nmember
         if ((N & 15) || (reinterpret_cast<uintptr_t>(a.out) & 15) || (a.out_bstride & 1)) return GATT_ERR_STATE;
         EncodeTiledFn enc = encode_tiled();
         if (!enc) return GATT_ERR_STATE;
-        auto xmap = [&](CUtensorMap *mp, const double *base, const int *slots, long long bstride) {
+        // the output map of warp stores copies one 16-row chunk (a box of {16, 32, 1})
+        a.xchunk_store = nst > 1 && c->x_wstore;
+        auto xmap = [&](CUtensorMap *mp, const double *base, const int *slots, long long bstride, bool chunk) {
             int nslots = 1;
             for (int f = 0; f < a.nf; f++) nslots = std::max(nslots, slots[f] + 1);
             const long long mstride = nmembers > 1 ? bstride : (long long)nslots * c->npts;
             cuuint64_t dims[5] = {16, (cuuint64_t)a.nlines, (cuuint64_t)(N / 16), (cuuint64_t)nslots,
                                   (cuuint64_t)nmembers};
             cuuint64_t strides[4] = {(cuuint64_t)N * 8, 128, (cuuint64_t)c->npts * 8, (cuuint64_t)mstride * 8};
-            cuuint32_t box[5] = {16, (cuuint32_t)kLanes, (cuuint32_t)(N / 16), 1, 1};
+            cuuint32_t box[5] = {16, (cuuint32_t)kLanes, chunk ? 1u : (cuuint32_t)(N / 16), 1, 1};
             cuuint32_t estr[5] = {1, 1, 1, 1, 1};
             return enc(mp, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<double *>(base), dims, strides, box, estr,
                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
         };
-        if (!xmap(&map, a.in, a.in_slot, a.in_bstride) || !xmap(&omap, a.out, a.out_slot, a.out_bstride))
+        if (!xmap(&map, a.in, a.in_slot, a.in_bstride, false) ||
+            !xmap(&omap, a.out, a.out_slot, a.out_bstride, a.xchunk_store != 0))
             return GATT_ERR_STATE;
     } else {
         // one box of N rows, or two of N/2 for lines past the copy engine's 256-row box
@@ -2267,6 +2271,8 @@ int gatt_create(gatt_ctx **out, int nx, int ny, int nz, int nbatch)
         c->visc_v2 = !(v2s && !strcmp(v2s, "0"));
         const char *xcs = getenv("GATT_X_COMPACT");
         c->x_compact = !(xcs && !strcmp(xcs, "0"));
+        const char *xws = getenv("GATT_X_WSTORE");
+        c->x_wstore = !(xws && !strcmp(xws, "0"));
         const char *fzs = getenv("GATT_FZ_REV");
         c->fz_rev = !(fzs && !strcmp(fzs, "0"));
     }

@@ -577,11 +577,15 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
     JobCursor cur = job_at(a, blockIdx.x), ahead = job_at(a, min(blockIdx.x + nst * G, a.njobs));
     int s = 0;
     uint32_t par = 0;
+    // x with two or more stages: every warp stores its own 16-row chunk of the solved tile (no
+    // block barrier before the store); the stage is refilled at the top of the next job, once
+    // every warp's store has read it (the refill still lands a whole job ahead of its use)
+    const bool wstore = XD && nst > 1 && a.xchunk_store;
     for (int j = blockIdx.x; j < a.njobs; j += G, s = (s + 1 == nst) ? 0 : s + 1, par ^= (s == 0) ? 1u : 0u) {
         if constexpr (kIncr) {
             if (j != (int)blockIdx.x) {
                 job_advance(cur, gs, a);
-                job_advance(ahead, gs, a);
+                if (!wstore) job_advance(ahead, gs, a);
             }
         } else {
             cur = job_at(a, j);
@@ -627,16 +631,23 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
             for (int kk = 0; kk < NW; kk++)
                 w[kk] = (kk >= H && kk < H + RPB) ? lds(sp - H + kk) : halo_row<PER>(sp - H + kk, N, lds);
         }
+        if (wstore && lane == 0) bulk_wait_read0();  // this warp's last store has read its stage
         if (__syncthreads_or(late)) {
-            // give up: report, let the other stage's copy land (bounded), leave
+            // give up: report, let the other stage's copy land (bounded; with warp stores its
+            // refill has not been issued yet), leave
             if (threadIdx.x == 0) {
                 *(volatile int *)a.err = 1;
                 const int s1 = (s + 1 == nst) ? 0 : s + 1;
-                if (nst > 1 && j + G < a.njobs) mbar_wait(bar0 + 8 * s1, par ^ (s1 == 0 ? 1u : 0u));
+                if (nst > 1 && !wstore && j + G < a.njobs) mbar_wait(bar0 + 8 * s1, par ^ (s1 == 0 ? 1u : 0u));
             }
-            if (XD && threadIdx.x < kLanes) bulk_wait0();  // stores already issued
+            if (XD && lane == 0) bulk_wait0();  // stores already issued
             __syncthreads();
             return;
+        }
+        if (wstore && j != (int)blockIdx.x) {
+            // the previous job's stage: its next tile is job j - G + nst * G (the cursor `ahead`)
+            if (threadIdx.x == 0 && j + (nst - 1) * G < a.njobs) issue(ahead, s == 0 ? nst - 1 : s - 1);
+            job_advance(ahead, gs, a);
         }
         // y/z: every warp has its rows, refill this stage now (blend keeps it for the epilogue);
         // x: the stage also carries the results out, it is refilled after the stores
@@ -658,13 +669,24 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
                 *reinterpret_cast<double2 *>(sw + xpair(q)) = v;
             }
             fence_proxy_async();
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                tma_store_5d(&omap, 0, tile * kLanes, 0, a.out_slot[f], b,
-                             st0 + (uint32_t)(s * stage_d * sizeof(double)));
-                bulk_commit();
+            if (wstore) {
+                // this warp's rows sp .. sp+15 are chunk p of the tile: 32 lines x 128 bytes
+                static_assert(!XD || RPB == 16, "x warp stores take one 16-row chunk per warp");
+                __syncwarp();
+                if (lane == 0) {
+                    tma_store_5d(&omap, 0, tile * kLanes, p, a.out_slot[f], b,
+                                 st0 + (uint32_t)(s * stage_d * sizeof(double)) + (uint32_t)p * (kLanes * 128));
+                    bulk_commit();
+                }
+            } else {
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    tma_store_5d(&omap, 0, tile * kLanes, 0, a.out_slot[f], b,
+                                 st0 + (uint32_t)(s * stage_d * sizeof(double)));
+                    bulk_commit();
+                }
+                if (threadIdx.x == 0 && j + nst * G < a.njobs) issue(ahead, s);
             }
-            if (threadIdx.x == 0 && j + nst * G < a.njobs) issue(ahead, s);
         } else {
             if (lr.valid) {
                 double *Gl = a.out + (long long)b * a.out_bstride +
@@ -704,7 +726,7 @@ __global__ void __launch_bounds__(WIDE ? 32 * kMaxPx : ((NR == 6 && !XD) ? 32 * 
             }
         }
     }
-    if (XD && threadIdx.x < kLanes) bulk_wait0();  // every store has landed before the CTA leaves
+    if (XD && lane == 0) bulk_wait0();  // every store has landed before the CTA leaves
 }
 
 }  // namespace gatt

@@ -130,6 +130,7 @@ struct SweepArgs {
     // "fields" the xtiles tiles -- so that each tile's fields are taken together, starting
     // from the points the preceding pointwise kernel wrote last (still in L2)
     int xorder, xtiles;
+    int xchunk_store;        // x, two or more stages: one tensor store per warp (output box of 16 rows)
     unsigned long long *mc_acc;
     const double *mc_ref;    // the step's start state, field slots as in_slot
     long long mc_ref_bstride;
