@@ -167,6 +167,10 @@ struct gatt_ctx {
     StepParams *d_params = nullptr;
     StepParams *h_params = nullptr;  // pinned, hist_cap entries
     cudaStream_t stream = nullptr;
+    // side stream: an x sweep runs on it beside the y/z sweeps of the same operand set (fork
+    // and join through the two events; captured as parallel graph branches)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool own_stream = false;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int graph_kernels[2] = {0, 0};
@@ -184,6 +188,7 @@ struct gatt_ctx {
     bool visc_v2 = true;    // stresses two points per thread (GATT_VISC_V2=0: one)
     bool x_compact = true;  // compact shared memory for the uniform-band x solver (GATT_X_COMPACT=0: no)
     bool x_wstore = true;   // x tiles stored chunk by chunk by their warps (GATT_X_WSTORE=0: by one thread)
+    bool fork_x = true;     // x sweeps beside the y/z sweeps (GATT_FORK_X=0: one after the other)
     bool fz_rev = true;     // last filter direction takes the fields in reverse order (GATT_FZ_REV=0: no)
     bool mc_done = false;   // set when a filter launch ran the max-change epilogue
     int bc_cluster = 0;     // CTAs per member for the boundary program (0: one CTA, k_bc)
@@ -890,6 +895,29 @@ int assemble3d(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSe
     return after_launch(c);
 }
 
+// The x sweep and the y/z sweeps of one operand set are independent: the x sweep runs on the
+// side stream, forked from and joined back into the context's stream, so that each one's
+// last partial wave of tiles overlaps the other (not while per-kernel events are recorded).
+template <typename F>
+int beside(gatt_ctx *c, F &&launch_x)
+{
+    if (!c->fork_x || c->profiling || !c->side) return launch_x();
+    CU(cudaEventRecord(c->ev_fork, c->stream));
+    CU(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+    std::swap(c->stream, c->side);
+    const int r = launch_x();
+    std::swap(c->stream, c->side);
+    TRY(r);
+    CU(cudaEventRecord(c->ev_join, c->side));
+    return GATT_OK;
+}
+int join_side(gatt_ctx *c)
+{
+    if (!c->fork_x || c->profiling || !c->side) return GATT_OK;
+    CU(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+    return GATT_OK;
+}
+
 // nseq2d/nseq3d on stage input q, fused with the RK4 update into out (mode).
 int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet &out, int mode, int nmem,
               double *d1, double *tq, double *d2, double *delta, bool assemble = true)
@@ -905,8 +933,9 @@ int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet
         const int ox[5] = {D3_UX, D3_VX, D3_WX, D3_RX, D3_EX};
         const int oy[5] = {D3_UY, D3_VY, D3_WY, D3_RY, D3_EY};
         const int oz[5] = {D3_UZ, D3_VZ, D3_WZ, D3_RZ, D3_EZ};
-        TRY(sweep(c, 0, 0, qin, qbs, fin, d1, bd1, ox, 5, nmem, 0, nullptr, PC_D1X));
+        TRY(beside(c, [&] { return sweep(c, 0, 0, qin, qbs, fin, d1, bd1, ox, 5, nmem, 0, nullptr, PC_D1X); }));
         TRY(sweep_yz(c, qin, qbs, fin, fin, d1, bd1, oy, oz, 5, nmem, PC_D1Y, PC_D1Z, PC_D1YZ));
+        TRY(join_side(c));
         TRY(before_launch(c, PC_VISC));
         if (c->visc_v2 && !(n & 1) && !(q.bstride & 1) && !((uintptr_t)q.v[4] & 15) && !((uintptr_t)d1 & 15) &&
             !((uintptr_t)tq & 15))
@@ -920,8 +949,9 @@ int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet
         const int ix[4] = {T3_XX, T3_XY, T3_XZ, T3_QX}, sx[4] = {S3_TXXX, S3_TXYX, S3_TXZX, S3_HTX};
         const int iy[4] = {T3_XY, T3_YY, T3_YZ, T3_QY}, sy[4] = {S3_TXYY, S3_TYYY, S3_TYZY, S3_HTY};
         const int iz[4] = {T3_XZ, T3_YZ, T3_ZZ, T3_QZ}, sz[4] = {S3_TXZZ, S3_TYZZ, S3_TZZZ, S3_HTZ};
-        TRY(sweep(c, 0, 0, tq, btq, ix, d2, bd2, sx, 4, nmem, 0, nullptr, PC_D2X));
+        TRY(beside(c, [&] { return sweep(c, 0, 0, tq, btq, ix, d2, bd2, sx, 4, nmem, 0, nullptr, PC_D2X); }));
         TRY(sweep_yz(c, tq, btq, iy, iz, d2, bd2, sy, sz, 4, nmem, PC_D2Y, PC_D2Z, PC_D2YZ));
+        TRY(join_side(c));
         if (!assemble) return GATT_OK;  // the gradients and second sweeps only (tangent / adjoint)
         return assemble3d(c, q, q0, out, mode, nmem, d1, d2, delta);
     }
@@ -2273,6 +2303,8 @@ int gatt_create(gatt_ctx **out, int nx, int ny, int nz, int nbatch)
         c->x_compact = !(xcs && !strcmp(xcs, "0"));
         const char *xws = getenv("GATT_X_WSTORE");
         c->x_wstore = !(xws && !strcmp(xws, "0"));
+        const char *fxs = getenv("GATT_FORK_X");
+        c->fork_x = !(fxs && !strcmp(fxs, "0"));
         const char *fzs = getenv("GATT_FZ_REV");
         c->fz_rev = !(fzs && !strcmp(fzs, "0"));
     }
@@ -2286,6 +2318,10 @@ int gatt_create(gatt_ctx **out, int nx, int ny, int nz, int nbatch)
         cudaError_t es = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
         if (es != cudaSuccess) rc = fail(GATT_ERR_CUDA, cudaGetErrorString(es));
         else c->own_stream = true;
+        if (es == cudaSuccess) es = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
+        if (es == cudaSuccess) es = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+        if (es == cudaSuccess) es = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+        if (es != cudaSuccess && rc == GATT_OK) rc = fail(GATT_ERR_CUDA, cudaGetErrorString(es));
     }
     if (rc == GATT_OK) {
         chk(alloc_fields(c, &c->qA, 5, nbatch));
@@ -2346,6 +2382,9 @@ void gatt_destroy(gatt_ctx *c)
     if (c->h_params) cudaFreeHost(c->h_params);
     if (c->h_err) cudaFreeHost(c->h_err);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    if (c->side) cudaStreamDestroy(c->side);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     delete c;
 }
 
