@@ -2310,7 +2310,7 @@ int gatt_create(gatt_ctx **out, int nx, int ny, int nz, int nbatch)
     }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);
     int rc = GATT_OK;
     auto chk = [&](int r) { if (rc == GATT_OK) rc = r; };
     if (e != cudaSuccess) rc = fail(GATT_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
