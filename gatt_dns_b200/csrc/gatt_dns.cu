@@ -171,6 +171,7 @@ struct gatt_ctx {
     // and join through the two events; captured as parallel graph branches)
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    double *tmp_side = nullptr;  // the side stream's scratch field (the global-memory line solver)
     bool own_stream = false;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int graph_kernels[2] = {0, 0};
@@ -188,7 +189,8 @@ struct gatt_ctx {
     bool visc_v2 = true;    // stresses two points per thread (GATT_VISC_V2=0: one)
     bool x_compact = true;  // compact shared memory for the uniform-band x solver (GATT_X_COMPACT=0: no)
     bool x_wstore = true;   // x tiles stored chunk by chunk by their warps (GATT_X_WSTORE=0: by one thread)
-    bool fork_x = true;     // x sweeps beside the y/z sweeps (GATT_FORK_X=0: one after the other)
+    bool fork_x = true;     // x sweeps beside the y/z sweeps, filter field chains side by side
+                            // (GATT_FORK_X=0: everything on one stream)
     bool fz_rev = true;     // last filter direction takes the fields in reverse order (GATT_FZ_REV=0: no)
     bool mc_done = false;   // set when a filter launch ran the max-change epilogue
     int bc_cluster = 0;     // CTAs per member for the boundary program (0: one CTA, k_bc)
@@ -895,6 +897,15 @@ int assemble3d(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSe
     return after_launch(c);
 }
 
+// Launches on the side stream: the context's stream and scratch field exchanged with the
+// side stream's for the lifetime of the scope (two streams never share the scratch field).
+struct OnSide {
+    gatt_ctx *c;
+    explicit OnSide(gatt_ctx *cc) : c(cc) { flip(); }
+    ~OnSide() { flip(); }
+    void flip() { std::swap(c->stream, c->side); std::swap(c->tmp, c->tmp_side); }
+};
+
 // The x sweep and the y/z sweeps of one operand set are independent: the x sweep runs on the
 // side stream, forked from and joined back into the context's stream, so that each one's
 // last partial wave of tiles overlaps the other (not while per-kernel events are recorded).
@@ -904,9 +915,11 @@ int beside(gatt_ctx *c, F &&launch_x)
     if (!c->fork_x || c->profiling || !c->side) return launch_x();
     CU(cudaEventRecord(c->ev_fork, c->stream));
     CU(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
-    std::swap(c->stream, c->side);
-    const int r = launch_x();
-    std::swap(c->stream, c->side);
+    int r;
+    {
+        OnSide on(c);
+        r = launch_x();
+    }
     TRY(r);
     CU(cudaEventRecord(c->ev_join, c->side));
     return GATT_OK;
@@ -1296,13 +1309,32 @@ int filter_set(gatt_ctx *c, const StateSet &q, int nmem, double blend, const dou
     // fields are the ones the previous direction wrote last (still in L2)
     const int r3[5] = {4, 3, 2, 1, 0}, r2[4] = {4, 3, 1, 0};
     const int *rl = c->is3d ? r3 : r2;
-    int nth = 0;
-    for (int d = 0; d < ndir; d++) {
-        if (!c->filt[d]) continue;
-        const int *sl = (c->fz_rev && (nth++ & 1)) ? rl : fl;
-        TRY(sweep(c, d, 1, q.v[0], q.bstride, sl, q.v[0], q.bstride, sl, nf, nmem, blend, blend_dt, PC_FX + d,
-                  d == last ? mc_ref : nullptr));
+    auto chain = [&](const int *fwd, const int *rev, int n) -> int {
+        int nth = 0;
+        for (int d = 0; d < ndir; d++) {
+            if (!c->filt[d]) continue;
+            const int *sl = (c->fz_rev && (nth++ & 1)) ? rev : fwd;
+            TRY(sweep(c, d, 1, q.v[0], q.bstride, sl, q.v[0], q.bstride, sl, n, nmem, blend, blend_dt, PC_FX + d,
+                      d == last ? mc_ref : nullptr));
+        }
+        return GATT_OK;
+    };
+    if (!c->fork_x || c->profiling || !c->side || !c->is3d) return chain(fl, rl, nf);
+    // 3-D: the fields' filters are independent -- U, V, W on the context's stream, R, E beside
+    // them on the side stream, so that each direction's last partial wave overlaps the other
+    // chain's launches
+    const int fa[3] = {0, 1, 2}, ra[3] = {2, 1, 0}, fb[2] = {3, 4}, rb[2] = {4, 3};
+    CU(cudaEventRecord(c->ev_fork, c->stream));
+    CU(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+    int r;
+    {
+        OnSide on(c);
+        r = chain(fb, rb, 2);
     }
+    TRY(r);
+    CU(cudaEventRecord(c->ev_join, c->side));
+    TRY(chain(fa, ra, 3));
+    CU(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
     return GATT_OK;
 }
 
@@ -2332,6 +2364,7 @@ int gatt_create(gatt_ctx **out, int nx, int ny, int nz, int nbatch)
         chk(alloc_fields(c, &c->d2, nd2(c), nbatch));
         chk(alloc_fields(c, &c->P, 1, nbatch));
         chk(alloc_fields(c, &c->tmp, 1, 1));
+        chk(alloc_fields(c, &c->tmp_side, 1, 1));
     }
     if (rc == GATT_OK) {
         cudaError_t ea = cudaMalloc(&c->acc, sizeof(unsigned long long) * 5 * nbatch);
@@ -2366,7 +2399,7 @@ void gatt_destroy(gatt_ctx *c)
         }
         cudaFree(c->ltype[d]);
     }
-    double *bufs[] = {c->qA, c->qB, c->delta, c->mean, c->d1, c->tq, c->d2, c->P, c->tmp, c->tin, c->tout, c->chi, c->hist,
+    double *bufs[] = {c->qA, c->qB, c->delta, c->mean, c->d1, c->tq, c->d2, c->P, c->tmp, c->tmp_side, c->tin, c->tout, c->chi, c->hist,
                       c->d_coef1, c->d_coef2, c->d_xs, c->arn_zeta, c->arn_B, c->arn_base, c->arn_um,
                       c->arn_part, c->arn_h};
     cudaFree(c->arn_region);
