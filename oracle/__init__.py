@@ -5,8 +5,10 @@ Fortran hot path (``source/Fortran/derivs.F90``, ``nseq.F90``, ``timeIntegration
 ``main.F90:357-465``).  Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline
 leg of ``bench.py`` may use it, and only as the checker or the timed CPU baseline.
 
-Parity status: unpinned against the reference binary (no tests or golden outputs ship
-with the reference, and it cannot be built here); pinned instead by known-answer tests
+Parity status: pinned to the reference's own Fortran by golden vectors
+(``tests/golden/reference_*.npz``, made by ``tests/golden/make_reference_golden.py``, which
+runs the unmodified ``derivs.F90``, ``nseq.F90`` and ``timeIntegration.F90`` through a
+Fortran-subset translator: the reference cannot be compiled here), and by known-answer tests
 (spectral accuracy on trigonometric fields, filter transfer function, conservation).
 """
 from __future__ import annotations

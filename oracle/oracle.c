@@ -1,7 +1,9 @@
 /*
  * CPU oracle for the GATT_DNS per-RK4-stage hot path -- TEST INFRASTRUCTURE ONLY.
- * See oracle.h for the contract and for why parity against the reference binary is
- * unpinned.  Every function cites the reference Fortran it restates; the element
+ * See oracle.h for the contract.  Pinned to the reference's own Fortran by golden vectors
+ * (tests/golden/reference_*.npz: the unmodified derivs.F90, nseq.F90 and
+ * timeIntegration.F90 run through a Fortran-subset translator).  Every function cites the
+ * reference Fortran it restates; the element
  * operation order follows the Fortran expressions left to right (built with
  * -ffp-contract=off so no multiply-add is fused).
  */

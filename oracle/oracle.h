@@ -7,11 +7,15 @@
  * __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it, and
  * only as the checker or as the timed CPU baseline -- never as the product.
  *
- * Parity status: UNPINNED against the reference binary.  The reference ships no
- * tests or golden outputs and cannot be built here (no Fortran compiler, no MPI,
- * no MATLAB), so this restatement is checked against known-answer tests
+ * Parity status: pinned to the reference's own Fortran.  The reference ships no tests
+ * or golden outputs and cannot be compiled here (no Fortran compiler, no MPI, no
+ * MATLAB), so tests/golden/make_reference_golden.py runs its unmodified derivs.F90,
+ * nseq.F90 and timeIntegration.F90 through a Fortran-subset translator on small cases
+ * and stores the outputs (tests/golden/reference_*.npz); tests/test_oracle_vs_reference.py
+ * holds this restatement to them (line solves of every direction and kind, right-hand
+ * side, boundary conditions, filters, one time step), besides known-answer tests
  * (spectral derivatives of trigonometric fields, filter transfer functions,
- * conservation on a periodic box) instead of reference output.
+ * conservation on a periodic box).
  *
  * Arrays are Fortran column-major (i fastest), index blocks and boundary boxes are
  * 1-based exactly as matrices.F90 / boundaryInfo.F90 declare them.
