@@ -50,6 +50,9 @@ def golden_cases():
                                       sfd={"X": 0.05, "Delta": 10.0, "buffer": 6}),
         "cavity2d": cs.cavity_channel(nx=24, ny=24, nz=1, sfd={"X": 0.05, "Delta": 10.0, "buffer": 6}),
         "lid": cs.lid_driven(n=24),
+        # break point at the leading edge, free-slip wall upstream, three x matrix types,
+        # buffer zones, SFD
+        "bl_cavity": cs.boundary_layer_cavity(nx=48, ny=32, buffers=((6, 5), (0, 6))),
     }
 
 

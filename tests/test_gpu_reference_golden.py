@@ -1,0 +1,92 @@
+"""The CUDA path against the reference's own Fortran (golden vectors), through the C-ABI.
+
+The fixtures of tests/golden (the reference's unmodified derivs.F90, nseq.F90 and
+timeIntegration.F90 run through a Fortran-subset translator, see
+tests/golden/make_reference_golden.py) compared directly with the GPU: line solves of every
+direction and kind and the right-hand side to 1e-12 relative, boundary conditions and
+filters to 1e-12, one time step (RK4, filters, SFD, boundary conditions, maxChange) to 1e-11.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+NAMES = ["box", "cavity3d", "cavity2d", "lid", "bl_cavity"]
+KEYS = ("U", "V", "W", "R", "E")
+
+
+def rel(a, b):
+    s = np.max(np.abs(b))
+    return float(np.max(np.abs(np.asarray(a) - b)) / (s if s > 0 else 1.0))
+
+
+@pytest.fixture(scope="module", params=NAMES)
+def gold(request, cuda_lib):
+    sys.path.insert(0, GOLD)
+    import make_reference_golden as mk
+    from gatt_dns_b200.solver import GattDNS
+    case = mk.golden_cases()[request.param]
+    z = np.load(os.path.join(GOLD, "reference_%s.npz" % request.param))
+    assert str(z["checksum"]) == mk.matrices_checksum(case), "case builder changed: regenerate the fixtures"
+    g = GattDNS(case)
+    yield request.param, case, z, g
+    g.close()
+
+
+def _flow(z):
+    return {k: np.asfortranarray(z["flow_" + k]) for k in KEYS}
+
+
+def test_line_solves(gold):
+    name, case, z, g = gold
+    for d in range(1, 4 if case.is3d else 3):
+        for kind in ("deriv", "filter"):
+            assert rel(g.calc_derivs(z["F"], d, kind), z["%s_%d" % (kind, d)]) < 1e-12, (name, d, kind)
+
+
+def test_rhs(gold):
+    name, case, z, g = gold
+    out = g.nseq(_flow(z))
+    for k in (KEYS if case.is3d else ("U", "V", "R", "E")):
+        assert rel(out[k], z["rhs_" + k]) < 1e-12, (name, k)
+
+
+def test_boundary_conditions(gold):
+    name, case, z, g = gold
+    g.upload(_flow(z))
+    g.apply_bound_cond(float(z["t"]))
+    out = g.download()
+    for k in KEYS:
+        assert rel(out[k], z["bc_" + k]) < 1e-12, (name, k)
+
+
+def test_filters(gold):
+    name, case, z, g = gold
+    for blend, key in ((-1.0, "filter_"), (0.3, "filterblend_")):
+        g.upload(_flow(z))
+        g.apply_filters(blend)
+        out = g.download()
+        for k in (KEYS if case.is3d else ("U", "V", "R", "E")):
+            assert rel(out[k], z[key + k]) < 1e-12, (name, blend, k)
+
+
+def test_time_step(gold):
+    name, case, z, g = gold
+    f = _flow(z)
+    g.upload(f)
+    if case.sfd_type:
+        g.upload_mean(f)
+    mc = g.step(float(z["t"]), float(z["dt"]))[0]
+    assert np.allclose(mc, z["step_maxchange"], rtol=1e-10, atol=1e-14), (name, mc, z["step_maxchange"])
+    out = g.download()
+    for k in KEYS:
+        got = g.download_wnew() if (k == "W" and not case.is3d) else out[k]
+        assert rel(got, z["step_" + k]) < 1e-11, (name, k)
+    if case.sfd_type:
+        m = g.download_mean()
+        for k in (KEYS if case.is3d else ("U", "V", "R", "E")):
+            assert rel(m[k], z["step_mean_" + k]) < 1e-11, (name, k)

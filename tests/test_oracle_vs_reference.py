@@ -2,9 +2,10 @@
 
 tests/golden/reference_<case>.npz were made by tests/golden/make_reference_golden.py, which
 runs the reference's unmodified derivs.F90, nseq.F90 and timeIntegration.F90 (and the
-lid-driven disturbance) through a Fortran-subset translator on small cases: the line solves
-of every direction and kind, the right-hand side, the boundary conditions, the filters with
-and without the blend, and one time step as main.F90 sequences it.  Here the oracle runs the
+lid-driven disturbance) through a Fortran-subset translator on small cases (periodic box,
+3-D and 2-D cavity channels with SFD, lid-driven cavity, boundary layer over a cavity): the
+line solves of every direction and kind, the right-hand side, the boundary conditions, the
+filters with and without the blend, and one time step as main.F90 sequences it.  Here the oracle runs the
 same cases on the same inputs and must agree to 1e-12 relative (max-norm per field; the
 translated Fortran evaluates every expression in the reference's operation order, so the
 only differences are the oracle's own evaluation order where it fuses loops).
@@ -33,7 +34,7 @@ def rel(a, b):
     return float(np.max(np.abs(np.asarray(a) - b)) / (s if s > 0 else 1.0))
 
 
-NAMES = ["box", "cavity3d", "cavity2d", "lid"]
+NAMES = ["box", "cavity3d", "cavity2d", "lid", "bl_cavity"]
 
 
 @pytest.mark.parametrize("name", NAMES)
