@@ -46,8 +46,8 @@ TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dram_traffic_periodic_box_128.txt
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
-    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--n", type=int, default=N_GRID)
     p.add_argument("--no-clocks", action="store_true")
