@@ -27,6 +27,7 @@ SIGNATURES = {
     "gatt_set_matrices": (_c_int, [_c_void_p, _c_int, _c_int, _c_int, _c_int, _c_int, _pd, _pd, _pd, _pd, _pd,
                                    _c_int, _pi]),
     "gatt_set_filter": (_c_int, [_c_void_p, _c_int, _c_int, _c_int, _c_double]),
+    "gatt_set_time_stepping": (_c_int, [_c_void_p, _c_int]),
     "gatt_set_neumann": (_c_int, [_c_void_p, _c_int, _pd, _c_int, _pd]),
     "gatt_set_bc": (_c_int, [_c_void_p, _c_int, _c_int, _c_int, _pi, _pd, _pi]),
     "gatt_set_corners": (_c_int, [_c_void_p, _c_int, _pi, _pi, _pi]),

@@ -80,6 +80,8 @@ class Case:
     sfd_delta: float = 0.0
     sfd_X: float = 0.0
     sfd_chi: Optional[np.ndarray] = None
+    # parameters.F90 timeStepping (main.F90:304-352): 1 RK4, 2 Euler, 3 SSPRK3
+    time_stepping: int = 1
     flowRegion: Optional[np.ndarray] = None
     dxmin: Tuple[float, float, float] = (0.0, 0.0, 0.0)
 

@@ -189,6 +189,7 @@ struct gatt_ctx {
     bool visc_v2 = true;    // stresses two points per thread (GATT_VISC_V2=0: one)
     bool x_compact = true;  // compact shared memory for the uniform-band x solver (GATT_X_COMPACT=0: no)
     bool x_wstore = true;   // x tiles stored chunk by chunk by their warps (GATT_X_WSTORE=0: by one thread)
+    int time_stepping = 1;  // parameters.F90 timeStepping: 1 RK4, 2 Euler, 3 SSPRK3
     bool fork_x = true;     // x sweeps beside the y/z sweeps, filter field chains side by side
                             // (GATT_FORK_X=0: everything on one stream)
     bool fz_rev = true;     // last filter direction takes the fields in reverse order (GATT_FZ_REV=0: no)
@@ -856,7 +857,7 @@ int launch_assemble3d_pipe(gatt_ctx *c, const StateSet &q, const StateSet &q0, c
     a.njobs = a.nchunks * nmem;
     a.nst = kPwStages;
     a.mode = mode;
-    a.use_delta = delta.p && mode >= RK_STAGE2;
+    a.use_delta = delta.p && mode_reads_delta(mode);
     a.use_q0 = 0;
     if (mode != RK_STORE_RHS)
         for (int f = 0; f < 5; f++)
@@ -1361,9 +1362,21 @@ int step_body(gatt_ctx *c)
     if (!c->is3d) qst.v[2] = q0.v[2];
     const int nm = c->nb;
     CU(cudaMemsetAsync(c->acc, 0, sizeof(unsigned long long) * 5 * nm, c->stream));
-    for (int s = 1; s <= 4; s++) {
-        TRY(rhs_stage(c, s == 1 ? q0 : qs, q0, qs, s, nm, c->d1, c->tq, c->d2, c->delta));
+    // the time integrator (main.F90:304-352 by timeStepping): every stage forms the RHS of its
+    // input, updates the stage state and applies the boundary conditions
+    if (c->time_stepping == 2) {  // EULER_2D/3D (timeIntegration.F90:158-223, 500-567)
+        TRY(rhs_stage(c, q0, q0, qs, RK_EULER, nm, c->d1, c->tq, c->d2, c->delta));
         TRY(apply_bc(c, qst, nm));
+    } else if (c->time_stepping == 3) {  // SSPRK3_2D/3D (timeIntegration.F90:225-336, 569-680)
+        for (int s = 0; s < 3; s++) {
+            TRY(rhs_stage(c, s == 0 ? q0 : qs, q0, qs, SSP_STAGE1 + s, nm, c->d1, c->tq, c->d2, c->delta));
+            TRY(apply_bc(c, qst, nm));
+        }
+    } else {  // RK4_2D/3D (timeIntegration.F90:8-156, 338-498)
+        for (int s = 1; s <= 4; s++) {
+            TRY(rhs_stage(c, s == 1 ? q0 : qs, q0, qs, s, nm, c->d1, c->tq, c->d2, c->delta));
+            TRY(apply_bc(c, qst, nm));
+        }
     }
     // nothing after the filter (no SFD, no boundary program): its last sweep can take the
     // max-change (main.F90:413-418) in its epilogue; the state sets must be equally spaced
@@ -1720,6 +1733,8 @@ int diff_nv(const gatt_ctx *c) { return diff_sfd(c) ? 10 : 5; }
 int check_diff(gatt_ctx *c, bool adjoint, bool step = false)
 {
     TRY(check_ready(c, true));
+    if (step && c->time_stepping != 1)
+        return fail(GATT_ERR_STATE, "the tangent-linear and adjoint steps are those of RK4 (timeStepping 1)");
     if (c->bc_dirty) TRY(build_bc_program(c));
     if (step && diff_sfd(c) && (!c->mean || !c->mean_init))
         return fail(GATT_ERR_STATE, "SFD: upload the mean (gatt_upload_mean) or run a step before the tangent/adjoint");
@@ -2541,6 +2556,15 @@ int gatt_set_matrices(gatt_ctx *c, int dir, int kind, int periodic, int nRHS, in
         for (uint8_t t : lt) mx = t > mx ? t : mx;
         c->lt_max[d] = mx;
     }
+    invalidate_graphs(c);
+    return GATT_OK;
+}
+
+int gatt_set_time_stepping(gatt_ctx *c, int scheme)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    if (scheme < 1 || scheme > 3) return fail(GATT_ERR_BADARG, "timeStepping must be 1 (RK4), 2 (Euler) or 3 (SSPRK3)");
+    c->time_stepping = scheme;
     invalidate_graphs(c);
     return GATT_OK;
 }

@@ -37,7 +37,19 @@ struct StepParams {
 };
 
 // RK4 stage modes for the assembly epilogue (timeIntegration.F90:380-487)
-enum { RK_STORE_RHS = 0, RK_STAGE1 = 1, RK_STAGE2 = 2, RK_STAGE3 = 3, RK_STAGE4 = 4 };
+// RK_EULER: the one stage of EULER_2D/3D; SSP_STAGE1..3: SSPRK3_2D/3D (timeIntegration.F90).
+enum { RK_STORE_RHS = 0, RK_STAGE1 = 1, RK_STAGE2 = 2, RK_STAGE3 = 3, RK_STAGE4 = 4, RK_EULER = 5,
+       SSP_STAGE1 = 6, SSP_STAGE2 = 7, SSP_STAGE3 = 8 };
+
+// Whether a stage update reads / writes the increment accumulator delta.
+__host__ __device__ __forceinline__ bool mode_reads_delta(int m)
+{
+    return m == RK_STAGE2 || m == RK_STAGE3 || m == RK_STAGE4 || m == SSP_STAGE2 || m == SSP_STAGE3;
+}
+__host__ __device__ __forceinline__ bool mode_writes_delta(int m)
+{
+    return m == RK_STAGE1 || m == RK_STAGE2 || m == RK_STAGE3 || m == SSP_STAGE1 || m == SSP_STAGE2;
+}
 
 struct FieldSet {
     double *p;            // base
@@ -164,6 +176,12 @@ __device__ __forceinline__ void rk_update(int mode, double dt, double k, double 
     case RK_STAGE2: *delta = *delta + dt / 3.0 * k; *qn = q0 + dt / 2.0 * k; break;
     case RK_STAGE3: *delta = *delta + dt / 3.0 * k; *qn = q0 + dt * k; break;
     case RK_STAGE4: *qn = q0 + *delta + dt / 6.0 * k; break;
+    // timeIntegration.F90:553-557 (Euler); 623-627, 648-652, 673-677 (SSPRK3: delta holds k1,
+    // then k1 + k2; U + dt*(Uk1 + Uk2)/4 and U + dt*(Uk1 + Uk2 + 4*Uk3)/6 left to right)
+    case RK_EULER: *qn = q0 + dt * k; break;
+    case SSP_STAGE1: *delta = k; *qn = q0 + dt * k; break;
+    case SSP_STAGE2: *delta = *delta + k; *qn = q0 + dt * *delta / 4.0; break;
+    case SSP_STAGE3: *qn = q0 + dt * (*delta + 4.0 * k) / 6.0; break;
     }
 }
 
@@ -242,9 +260,9 @@ __global__ void __launch_bounds__(256, 3) k_assemble3d(Phys ph, StateSet q, Stat
             double *dl = delta.p ? delta.f(b, f) + p : nullptr;
             double q0v = (mode != RK_STORE_RHS) ? q0.v[f][b * q0.bstride + p] : 0.0;
             double res;
-            double dtmp = (dl && mode >= RK_STAGE2) ? *dl : 0.0;  // stage 1 overwrites delta
+            double dtmp = (dl && mode_reads_delta(mode)) ? *dl : 0.0;  // stage 1 overwrites delta
             rk_update(mode, dt, k[f], q0v, &dtmp, &res);
-            if (dl && mode != RK_STAGE4 && mode != RK_STORE_RHS) *dl = dtmp;
+            if (dl && mode_writes_delta(mode)) *dl = dtmp;
             out.v[f][b * out.bstride + p] = res;
         }
     }
@@ -284,9 +302,9 @@ __global__ void k_assemble2d(Phys ph, StateSet q, StateSet q0, StateSet out, Fie
             double *dl = delta.p ? delta.f(b, f) + p : nullptr;
             double q0v = (mode != RK_STORE_RHS) ? q0.v[f][b * q0.bstride + p] : 0.0;
             double res;
-            double dtmp = (dl && mode >= RK_STAGE2) ? *dl : 0.0;  // stage 1 overwrites delta
+            double dtmp = (dl && mode_reads_delta(mode)) ? *dl : 0.0;  // stage 1 overwrites delta
             rk_update(mode, dt, k[f], q0v, &dtmp, &res);
-            if (dl && mode != RK_STAGE4 && mode != RK_STORE_RHS) *dl = dtmp;
+            if (dl && mode_writes_delta(mode)) *dl = dtmp;
             out.v[f][b * out.bstride + p] = res;
         }
     }

@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(2 * kPwC, 1) k_assemble3d_pipe(Phys ph, StateS
                 double dtmp = a.use_delta ? S[(A3_NIN + 5 + v) * kPwC] : 0.0;  // stage 1 overwrites delta
                 double res;
                 rk_update(mode, dt, kv, q0v, &dtmp, &res);
-                if (delta.p && mode != RK_STAGE4 && mode != RK_STORE_RHS) delta.f(b, v)[p] = dtmp;
+                if (delta.p && mode_writes_delta(mode)) delta.f(b, v)[p] = dtmp;
                 out.v[v][b * out.bstride + p] = res;
             };
             if (energy) {

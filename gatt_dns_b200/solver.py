@@ -79,6 +79,7 @@ class GattDNS:
                            "gatt_set_matrices")
         fd = c.filterDirections
         _lib.check(L.gatt_set_filter(self.h, fd[0], fd[1], fd[2], c.filterCharTime), "gatt_set_filter")
+        _lib.check(L.gatt_set_time_stepping(self.h, int(getattr(c, "time_stepping", 1))), "gatt_set_time_stepping")
         bc = c.bc
         n1, n2 = _f64(bc.neumannCoeffs), _f64(bc.neumann2Coeffs)
         _lib.check(L.gatt_set_neumann(self.h, n1.size, _dp(n1) if n1.size else None, n2.size,

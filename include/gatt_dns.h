@@ -83,6 +83,12 @@ int gatt_set_matrices(gatt_ctx *ctx, int dir, int kind, int periodic, int nRHS, 
 /* filterX/Y/Z and FilterCharTime of matrices.F90 / parameters.F90 (-1 = no blend). */
 int gatt_set_filter(gatt_ctx *ctx, int filterX, int filterY, int filterZ, double filterCharTime);
 
+/* timeStepping of parameters.F90, the integrator main.F90:304-352 selects: 1 RK4 (RK4_2D/3D,
+ * the default), 2 Euler (EULER_2D/3D), 3 SSPRK3 (SSPRK3_2D/3D; timeIntegration.F90).
+ * GATT_ERR_BADARG for any other value.  The tangent-linear and adjoint steps (gatt_jvp,
+ * gatt_vjp) are RK4's and return GATT_ERR_STATE under the other two. */
+int gatt_set_time_stepping(gatt_ctx *ctx, int timeStepping);
+
 /* neumannCoeffs / neumann2Coeffs of matrices.F90 (getBoundaryConditions.m:75-80). */
 int gatt_set_neumann(gatt_ctx *ctx, int neumannLength, const double *neumannCoeffs,
                      int neumann2Length, const double *neumann2Coeffs);

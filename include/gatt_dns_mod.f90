@@ -63,6 +63,12 @@ module gatt_dns
             real(c_double), value :: filterCharTime
             integer(c_int) :: gatt_set_filter
         end function
+        function gatt_set_time_stepping(ctx, timeStepping) bind(C, name='gatt_set_time_stepping')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: ctx
+            integer(c_int), value :: timeStepping
+            integer(c_int) :: gatt_set_time_stepping
+        end function
         function gatt_set_neumann(ctx, n1, c1, n2, c2) bind(C, name='gatt_set_neumann')
             import :: c_int, c_ptr, c_double
             type(c_ptr), value :: ctx

@@ -44,7 +44,8 @@ class _Case(ctypes.Structure):
                 ("cN", ctypes.c_int), ("cL", _pi), ("cD", _pi), ("cAdiabatic", _pi),
                 ("nDist", ctypes.c_int), ("distType", _pi), ("distVar", _pi), ("distInd", _pi),
                 ("distX", _pd), ("distXoff", _pi), ("distPar", _pd),
-                ("sfdType", ctypes.c_int), ("sfdDelta", ctypes.c_double), ("sfdChi", _pd)]
+                ("sfdType", ctypes.c_int), ("sfdDelta", ctypes.c_double), ("sfdChi", _pd),
+                ("timeStepping", ctypes.c_int)]
 
 
 def build():
@@ -147,6 +148,7 @@ class Oracle:
             par = self._hold(np.array([d["par"][0] for d in bc.disturbances], dtype=np.float64))
             c.distType, c.distVar, c.distInd = (a.ctypes.data_as(_pi) for a in (typ, var, ind))
             c.distX, c.distXoff, c.distPar = X.ctypes.data_as(_pd), off.ctypes.data_as(_pi), par.ctypes.data_as(_pd)
+        c.timeStepping = int(getattr(case, "time_stepping", 1))
         c.sfdType = case.sfd_type
         c.sfdDelta = case.sfd_delta
         if case.sfd_type:

@@ -491,6 +491,63 @@ void orc_rk4(const orc_case *c, const double *U, const double *V, double *W, con
     orc_apply_bc(c, Un, Vn, Wst, Rn, En, t + dt);
 }
 
+/* Euler: timeIntegration.F90:158-223 (2-D) and 500-567 (3-D).  The 3-D form applies the
+ * boundary conditions at t, the 2-D form at t + dt (no time-dependent boundary data here). */
+void orc_euler(const orc_case *c, const double *U, const double *V, double *W, const double *R,
+               const double *E, double *Un, double *Vn, double *Wn, double *Rn, double *En,
+               double t, double dt)
+{
+    const long n = (long)c->nx * c->ny * c->nz;
+    const int is3d = c->nz > 1;
+    const double *q0[5] = {U, V, is3d ? W : NULL, R, E};
+    double *qn[5] = {Un, Vn, is3d ? Wn : NULL, Rn, En};
+    double *k[5];
+    for (int f = 0; f < 5; f++) k[f] = work_field(SLOT_RK + f, n);
+    orc_nseq(c, U, V, W, R, E, k[0], k[1], k[2], k[3], k[4]);
+    for (int f = 0; f < 5; f++) {
+        if (!is3d && f == 2) continue;
+        #pragma omp parallel for schedule(static)
+        for (long p = 0; p < n; p++) qn[f][p] = q0[f][p] + dt * k[f][p];
+    }
+    orc_apply_bc(c, Un, Vn, is3d ? Wn : W, Rn, En, is3d ? t : t + dt);
+}
+
+/* SSPRK3: timeIntegration.F90:225-336 (2-D) and 569-680 (3-D): k1 at the step start, k2 at
+ * q0 + dt k1, k3 at q0 + dt (k1 + k2) / 4, result q0 + dt (k1 + k2 + 4 k3) / 6, boundary
+ * conditions after every stage.  acc holds k1, then k1 + k2. */
+void orc_ssprk3(const orc_case *c, const double *U, const double *V, double *W, const double *R,
+                const double *E, double *Un, double *Vn, double *Wn, double *Rn, double *En,
+                double t, double dt)
+{
+    const long n = (long)c->nx * c->ny * c->nz;
+    const int is3d = c->nz > 1;
+    const double *q0[5] = {U, V, is3d ? W : NULL, R, E};
+    double *qn[5] = {Un, Vn, is3d ? Wn : NULL, Rn, En};
+    double *k[5], *acc[5];
+    for (int f = 0; f < 5; f++) { k[f] = work_field(SLOT_RK + f, n); acc[f] = work_field(SLOT_RK + 5 + f, n); }
+    double *Wst = is3d ? Wn : W;
+    orc_nseq(c, U, V, W, R, E, k[0], k[1], k[2], k[3], k[4]);
+    for (int s = 1; s <= 3; s++) {
+        if (s > 1) orc_nseq(c, Un, Vn, Wst, Rn, En, k[0], k[1], k[2], k[3], k[4]);
+        for (int f = 0; f < 5; f++) {
+            if (!is3d && f == 2) continue;
+            #pragma omp parallel for schedule(static)
+            for (long p = 0; p < n; p++) {
+                if (s == 1) {
+                    acc[f][p] = k[f][p];
+                    qn[f][p] = q0[f][p] + dt * k[f][p];
+                } else if (s == 2) {
+                    acc[f][p] = acc[f][p] + k[f][p];
+                    qn[f][p] = q0[f][p] + dt * acc[f][p] / 4.0;
+                } else {
+                    qn[f][p] = q0[f][p] + dt * (acc[f][p] + 4.0 * k[f][p]) / 6.0;
+                }
+            }
+        }
+        orc_apply_bc(c, Un, Vn, Wst, Rn, En, s == 2 ? t + dt / 2.0 : t + dt);
+    }
+}
+
 /* ------------------------------------------------------------------------- */
 /* Filters: derivs.F90:303-552                                                */
 /* ------------------------------------------------------------------------- */
@@ -528,7 +585,10 @@ void orc_step(const orc_case *c, double *U, double *V, double *W, double *R, dou
     const int is3d = c->nz > 1;
     double *Un = work_field(SLOT_STEP, n), *Vn = work_field(SLOT_STEP + 1, n), *Rn = work_field(SLOT_STEP + 2, n),
            *En = work_field(SLOT_STEP + 3, n);
-    orc_rk4(c, U, V, W, R, E, Un, Vn, Wn, Rn, En, t, dt);
+    /* main.F90:304-352: the time integrator by parameters.F90 timeStepping */
+    if (c->timeStepping == 2) orc_euler(c, U, V, W, R, E, Un, Vn, Wn, Rn, En, t, dt);
+    else if (c->timeStepping == 3) orc_ssprk3(c, U, V, W, R, E, Un, Vn, Wn, Rn, En, t, dt);
+    else orc_rk4(c, U, V, W, R, E, Un, Vn, Wn, Rn, En, t, dt);
     /* main.F90:357-378 -- the filter receives dt/FilterCharTime */
     orc_filters(c, Un, Vn, Wn, Rn, En, dt / c->filterCharTime);
     /* main.F90:381-402 */

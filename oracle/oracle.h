@@ -65,6 +65,7 @@ typedef struct {
     int sfdType;                     /* 0 off, 1 constant, 2 field */
     double sfdDelta;
     const double *sfdChi;            /* nx*ny*nz field (type 1: filled by caller) */
+    int timeStepping;                /* parameters.F90 timeStepping: 1 (or 0) RK4, 2 Euler, 3 SSPRK3 */
 } orc_case;
 
 int orc_num_threads(void);

@@ -14,7 +14,8 @@ seeded field in every direction (``calcDerivsX/Y/Z``, derivs.F90:9-110); the rig
 (``nseq2d`` / ``nseq3d``, nseq.F90:10-323); the boundary conditions (``applyBoundCond``,
 nseq.F90:327-518); the filters with and without the blend (``applyFilters2D/3D``,
 derivs.F90:303-552); and one time step as main.F90:306-418 sequences it (``RK4_2D/3D``, the
-filters with dt/FilterCharTime, SFD, ``applyBoundCond`` at t + dt, maxChange).  The SFD
+filters with dt/FilterCharTime, SFD, ``applyBoundCond`` at t + dt, maxChange), and on most
+cases the same step with ``EULER_2D/3D`` and ``SSPRK3_2D/3D`` as the integrator.  The SFD
 update and the maxChange reduction are main-program lines, restated here in numpy with
 their line numbers; everything else is the reference's code.
 
@@ -54,6 +55,10 @@ def golden_cases():
         # buffer zones, SFD
         "bl_cavity": cs.boundary_layer_cavity(nx=48, ny=32, buffers=((6, 5), (0, 6))),
     }
+
+
+# cases that also hold one Euler and one SSPRK3 step (timeIntegration.F90:158-336, 500-680)
+SCHEME_CASES = ("box", "cavity2d", "lid", "bl_cavity")
 
 
 def matrices_checksum(case):
@@ -205,15 +210,18 @@ def run_filters(fns, case, flow, blend):
     return f
 
 
-def run_step(fns, case, flow, t, dt):
-    """main.F90:306-418 for one step: RK4, the filters, SFD, boundary conditions, maxChange."""
+def run_step(fns, case, flow, t, dt, scheme="rk4", prefix="step_"):
+    """main.F90:306-418 for one step: the time integrator (timeStepping 1 RK4, 2 EULER, 3
+    SSPRK3), the filters, SFD, boundary conditions, maxChange."""
     U, V, W, R, E = (flow[k].copy() for k in ("U", "V", "W", "R", "E"))
     Un, Vn, Wn, Rn, En = (np.zeros_like(U) for _ in range(5))  # Wnew = 0 (main.F90:186)
     mean = {k: flow[k].copy() for k in ("U", "V", "W", "R", "E")}
     if case.is3d:
-        fns["rk4_3d"](U, V, W, R, E, Un, Vn, Wn, Rn, En, t, dt, *_phys(case), *_coef_list(case, 0), *_bc_list(case))
+        fns[scheme + "_3d"](U, V, W, R, E, Un, Vn, Wn, Rn, En, t, dt, *_phys(case), *_coef_list(case, 0),
+                            *_bc_list(case))
     else:
-        fns["rk4_2d"](U, V, W, R, E, Un, Vn, Rn, En, t, dt, *_phys(case), *_coef_list(case, 0), *_bc_list(case))
+        fns[scheme + "_2d"](U, V, W, R, E, Un, Vn, Rn, En, t, dt, *_phys(case), *_coef_list(case, 0),
+                            *_bc_list(case))
     # filters with dt/FilterCharTime (main.F90:358-377)
     new = {"U": Un, "V": Vn, "W": Wn, "R": Rn, "E": En}
     f = run_filters(fns, case, new, dt / case.filterCharTime)
@@ -232,10 +240,10 @@ def run_step(fns, case, flow, t, dt):
     # maxChange (main.F90:413-418, restated)
     old = {"U": U, "V": V, "W": W, "R": R, "E": E}
     mc = np.array([np.max(np.abs(new[k] - old[k])) for k in ("U", "V", "W", "R", "E")])
-    out = {"step_" + k: new[k] for k in new}
-    out["step_maxchange"] = mc
+    out = {prefix + k: new[k] for k in new}
+    out[prefix + "maxchange"] = mc
     if case.sfd_type > 0:
-        out.update({"step_mean_" + k: mean[k] for k in mean})
+        out.update({prefix + "mean_" + k: mean[k] for k in mean})
     return out
 
 
@@ -256,6 +264,9 @@ def make(name, case, root):
     rec.update({"filter_" + k: v for k, v in run_filters(fns, case, flow, -1.0).items()})
     rec.update({"filterblend_" + k: v for k, v in run_filters(fns, case, flow, 0.3).items()})
     rec.update(run_step(fns, case, flow, t, dt))
+    if name in SCHEME_CASES:
+        rec.update(run_step(fns, case, flow, t, dt, "euler", "euler_"))
+        rec.update(run_step(fns, case, flow, t, dt, "ssprk3", "ssprk3_"))
     path = os.path.join(HERE, "reference_%s.npz" % name)
     np.savez_compressed(path, **rec)
     return path

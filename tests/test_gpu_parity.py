@@ -179,6 +179,37 @@ def test_step(libs, name):
     g.close()
 
 
+@pytest.mark.parametrize("scheme", [2, 3])
+@pytest.mark.parametrize("name", ["box", "cavity3d", "lid", "bl_cavity", "box_ragged"])
+def test_euler_and_ssprk3_match_oracle(libs, name, scheme):
+    """timeStepping 2 (Euler) and 3 (SSPRK3): three steps against the oracle, and the
+    tangent-linear and adjoint steps refused (they are RK4's)."""
+    import dataclasses
+    from gatt_dns_b200 import _lib
+    from gatt_dns_b200.solver import GattDNS
+    from oracle import Oracle
+    c = dataclasses.replace(get_case(name), time_stepping=scheme)
+    g, o = GattDNS(c), Oracle(c)
+    f = flow_for(c, seed=4)
+    dt = 0.1 * c.cfl_dt(f["U"], f["V"], f["W"], 1.0)
+    g.upload(f)
+    st = o.new_state(f)
+    for s in range(3):
+        mg = g.step(s * dt, dt)[0]
+        mo = o.step(st, s * dt, dt)
+        assert np.allclose(mg, mo, rtol=1e-10, atol=1e-15), (name, scheme, s, mg, mo)
+    a = g.download()
+    for k in fields(c):
+        assert rel(a[k], st[k]) < STEP_TOL * 10, (name, scheme, k, rel(a[k], st[k]))
+    if c.sfd_type:
+        m = g.download_mean()
+        for k in fields(c):
+            assert rel(m[k], st["m" + k]) < STEP_TOL * 10
+    with pytest.raises(_lib.GattError):
+        g.jvp(g.download(), 1, 0.0, dt)
+    g.close()
+
+
 def test_lid_driven_100_steps(libs):
     c, g, o = pair("lid")
     f = cs.uniform_flow(c)

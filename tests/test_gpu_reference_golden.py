@@ -90,3 +90,29 @@ def test_time_step(gold):
         m = g.download_mean()
         for k in (KEYS if case.is3d else ("U", "V", "R", "E")):
             assert rel(m[k], z["step_mean_" + k]) < 1e-11, (name, k)
+
+
+@pytest.mark.parametrize("scheme", [2, 3])
+@pytest.mark.parametrize("name", ["box", "cavity2d", "lid", "bl_cavity"])
+def test_euler_and_ssprk3_steps(cuda_lib, name, scheme):
+    """timeStepping 2 (EULER_2D/3D) and 3 (SSPRK3_2D/3D) against the reference's own
+    integrators (gatt_set_time_stepping)."""
+    import dataclasses
+    sys.path.insert(0, GOLD)
+    import make_reference_golden as mk
+    from gatt_dns_b200.solver import GattDNS
+    case = dataclasses.replace(mk.golden_cases()[name], time_stepping=scheme)
+    z = np.load(os.path.join(GOLD, "reference_%s.npz" % name))
+    key = {2: "euler_", 3: "ssprk3_"}[scheme]
+    g = GattDNS(case)
+    f = _flow(z)
+    g.upload(f)
+    if case.sfd_type:
+        g.upload_mean(f)
+    mc = g.step(float(z["t"]), float(z["dt"]))[0]
+    assert np.allclose(mc, z[key + "maxchange"], rtol=1e-10, atol=1e-14), (name, scheme, mc)
+    out = g.download()
+    for k in KEYS:
+        got = g.download_wnew() if (k == "W" and not case.is3d) else out[k]
+        assert rel(got, z[key + k]) < 1e-11, (name, scheme, k)
+    g.close()

@@ -99,3 +99,22 @@ def test_time_step_matches_reference(oracle_lib, name):
             if k == "W" and not case.is3d:
                 continue
             assert rel(st["m" + k], z["step_mean_" + k]) < TOL, (name, k)
+
+
+@pytest.mark.parametrize("scheme", [2, 3])
+@pytest.mark.parametrize("name", ["box", "cavity2d", "lid", "bl_cavity"])
+def test_euler_and_ssprk3_steps_match_reference(oracle_lib, name, scheme):
+    """timeStepping 2 (EULER_2D/3D) and 3 (SSPRK3_2D/3D) in the same main-loop step."""
+    import dataclasses
+    import oracle
+    mk, case, z = _load(name)
+    case = dataclasses.replace(case, time_stepping=scheme)
+    key = {2: "euler_", 3: "ssprk3_"}[scheme]
+    o = oracle.Oracle(case)
+    flow = {k: z["flow_" + k] for k in ("U", "V", "W", "R", "E")}
+    st = o.new_state(flow)
+    mc = o.step(st, float(z["t"]), float(z["dt"]))
+    for k in ("U", "V", "W", "R", "E"):
+        got = st["Wnew"] if (k == "W" and not case.is3d) else st[k]
+        assert rel(got, z[key + k]) < TOL, (name, scheme, k)
+    assert np.allclose(mc, z[key + "maxchange"], rtol=1e-10, atol=1e-14), (name, scheme, mc)
