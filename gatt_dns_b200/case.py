@@ -82,6 +82,9 @@ class Case:
     sfd_chi: Optional[np.ndarray] = None
     # parameters.F90 timeStepping (main.F90:304-352): 1 RK4, 2 Euler, 3 SSPRK3
     time_stepping: int = 1
+    # forcings of runForcings2D/3D.F90 (disturbances with forcing = true): dicts with
+    # type ("pressureGradient" | "turbulenceGenerator"), ind (1-based box, 6 ints), par
+    forcings: Optional[list] = None
     flowRegion: Optional[np.ndarray] = None
     dxmin: Tuple[float, float, float] = (0.0, 0.0, 0.0)
 
@@ -512,10 +515,9 @@ def _dxmin(X, Y, Z):
 # ---------------------------------------------------------------------------
 
 def periodic_box(n=128, Re=1600.0, Ma=0.3, Pr=0.71, gamma=1.4, T0=300.0, filter_alpha=0.49, deriv="SL4",
-                 nxyz=None):
-    """Triply periodic box on [0, 2*pi)^3 (``source/boundaries/periodicBox.m``)."""
+                 nxyz=None, L=2 * math.pi):
+    """Triply periodic box on [0, L)^3 (``source/boundaries/periodicBox.m``)."""
     nx, ny, nz = nxyz if nxyz else (n, n, n)
-    L = 2 * math.pi
     X = generate_mesh(0, L, nx, periodic=True, fix_periodic_domain_size=True)
     Y = generate_mesh(0, L, ny, periodic=True, fix_periodic_domain_size=True)
     Z = generate_mesh(0, L, nz, periodic=True, fix_periodic_domain_size=True)
@@ -528,6 +530,17 @@ def periodic_box(n=128, Re=1600.0, Ma=0.3, Pr=0.71, gamma=1.4, T0=300.0, filter_
                          mx.fortran_round(n1), mx.fortran_round(n2))
     return Case(name="periodic_box_%dx%dx%d" % (nx, ny, nz), nx=nx, ny=ny, nz=nz, Re=Re, Ma=Ma, Pr=Pr,
                 gamma=gamma, T0=T0, X=X, Y=Y, Z=Z, mats=mats, bc=bc, flowRegion=fr, dxmin=_dxmin(X, Y, Z))
+
+
+def turbulence_box(n=64, Re=1000.0, Ma=0.1, epsilon=1.0, L=1.0, nxyz=None, deriv="SL6", filter_alpha=0.499):
+    """The forced turbulence box of ``examples/turbulenceBox.m``: a periodic box on [0, L)^3,
+    SL6 derivatives, filter strength 0.499, and the ``turbulenceGenerator`` forcing over the
+    whole domain with par = [epsilon, e0], e0 = 1/((gamma^2 - gamma) Ma^2)."""
+    c = periodic_box(n=n, Re=Re, Ma=Ma, nxyz=nxyz, L=L, deriv=deriv, filter_alpha=filter_alpha)
+    e0 = 1.0 / ((c.gamma ** 2 - c.gamma) * Ma ** 2)
+    c.forcings = [{"type": "turbulenceGenerator", "ind": [1, c.nx, 1, c.ny, 1, c.nz], "par": [epsilon, e0]}]
+    c.name = "turbulence_box_%dx%dx%d" % (c.nx, c.ny, c.nz)
+    return c
 
 
 def lid_driven(n=128, Re=1000.0, Ma=0.5, Pr=0.71, gamma=1.4, T0=300.0, filter_alpha=0.49, deriv="SL4",

@@ -45,7 +45,8 @@ class _Case(ctypes.Structure):
                 ("nDist", ctypes.c_int), ("distType", _pi), ("distVar", _pi), ("distInd", _pi),
                 ("distX", _pd), ("distXoff", _pi), ("distPar", _pd),
                 ("sfdType", ctypes.c_int), ("sfdDelta", ctypes.c_double), ("sfdChi", _pd),
-                ("timeStepping", ctypes.c_int)]
+                ("timeStepping", ctypes.c_int),
+                ("nForce", ctypes.c_int), ("forceType", _pi), ("forceInd", _pi), ("forcePar", _pd)]
 
 
 def build():
@@ -149,6 +150,14 @@ class Oracle:
             c.distType, c.distVar, c.distInd = (a.ctypes.data_as(_pi) for a in (typ, var, ind))
             c.distX, c.distXoff, c.distPar = X.ctypes.data_as(_pd), off.ctypes.data_as(_pi), par.ctypes.data_as(_pd)
         c.timeStepping = int(getattr(case, "time_stepping", 1))
+        fr = list(getattr(case, "forcings", None) or [])
+        c.nForce = len(fr)
+        if fr:
+            code = {"pressureGradient": 1, "turbulenceGenerator": 2}
+            ft = self._hold(np.array([code[f["type"]] for f in fr], dtype=np.int32))
+            fi = self._hold(np.asfortranarray(np.array([f["ind"] for f in fr], dtype=np.int32)))
+            fp = self._hold(np.array([list(f["par"]) + [0.0] * (2 - len(f["par"])) for f in fr], dtype=np.float64))
+            c.forceType, c.forceInd, c.forcePar = ft.ctypes.data_as(_pi), fi.ctypes.data_as(_pi), fp.ctypes.data_as(_pd)
         c.sfdType = case.sfd_type
         c.sfdDelta = case.sfd_delta
         if case.sfd_type:

@@ -243,12 +243,69 @@ static void nseq3d(const orc_case *c, const double *U, const double *V, const do
     }
 }
 
+/* The forcings of runForcings2D/3D.F90 (writeFortranDisturbances.m writes one call per
+ * forcing, on its box), in order, on the right-hand side nseq has formed. */
+static void forcings(const orc_case *c, const double *U, const double *V, const double *W, const double *R,
+                     const double *E, double *dU, double *dV, double *dW, double *dE)
+{
+    const long nx = c->nx, nxy = (long)c->nx * c->ny;
+    for (int f = 0; f < c->nForce; f++) {
+        int b[6];
+        for (int q = 0; q < 6; q++) b[q] = c->forceInd[f + (long)q * c->nForce] - 1;
+        const double *par = c->forcePar + 2 * f;
+        if (c->forceType[f] == 1) {
+            /* pressureGradient.F90: du = du + dpdx/r */
+            for (int k = b[4]; k <= b[5]; k++)
+                for (int j = b[2]; j <= b[3]; j++)
+                    for (int i = b[0]; i <= b[1]; i++) {
+                        const long p = i + j * nx + k * nxy;
+                        dU[p] = dU[p] + par[0] / R[p];
+                    }
+        } else if (c->forceType[f] == 2) {
+            /* turbulenceGenerator.F90 on one rank: sums in array-element order, then
+             * du = du + 0.25*epsilon*N/ET_sum*u - gamma*U_sum/N (gamma = 10*epsilon) */
+            double ET = 0, Us = 0, Vs = 0, Ws = 0, Es = 0;
+            long N = 0;
+            for (int k = b[4]; k <= b[5]; k++)
+                for (int j = b[2]; j <= b[3]; j++)
+                    for (int i = b[0]; i <= b[1]; i++) {
+                        const long p = i + j * nx + k * nxy;
+                        ET = ET + (U[p] * U[p] + V[p] * V[p] + W[p] * W[p]);
+                        N++;
+                    }
+            for (int k = b[4]; k <= b[5]; k++)
+                for (int j = b[2]; j <= b[3]; j++)
+                    for (int i = b[0]; i <= b[1]; i++) Us = Us + U[i + j * nx + k * nxy];
+            for (int k = b[4]; k <= b[5]; k++)
+                for (int j = b[2]; j <= b[3]; j++)
+                    for (int i = b[0]; i <= b[1]; i++) Vs = Vs + V[i + j * nx + k * nxy];
+            for (int k = b[4]; k <= b[5]; k++)
+                for (int j = b[2]; j <= b[3]; j++)
+                    for (int i = b[0]; i <= b[1]; i++) Ws = Ws + W[i + j * nx + k * nxy];
+            for (int k = b[4]; k <= b[5]; k++)
+                for (int j = b[2]; j <= b[3]; j++)
+                    for (int i = b[0]; i <= b[1]; i++) Es = Es + E[i + j * nx + k * nxy];
+            const double eps = par[0], e0 = par[1], gamma = 10 * eps, Nd = (double)N;
+            for (int k = b[4]; k <= b[5]; k++)
+                for (int j = b[2]; j <= b[3]; j++)
+                    for (int i = b[0]; i <= b[1]; i++) {
+                        const long p = i + j * nx + k * nxy;
+                        dU[p] = dU[p] + 0.25 * eps * Nd / ET * U[p] - gamma * Us / Nd;
+                        dV[p] = dV[p] + 0.25 * eps * Nd / ET * V[p] - gamma * Vs / Nd;
+                        dW[p] = dW[p] + 0.25 * eps * Nd / ET * W[p] - gamma * Ws / Nd;
+                        dE[p] = dE[p] - gamma * (Es / Nd - e0);
+                    }
+        }
+    }
+}
+
 void orc_nseq(const orc_case *c, const double *U, const double *V, const double *W,
               const double *R, const double *E,
               double *dU, double *dV, double *dW, double *dR, double *dE)
 {
     if (c->nz == 1) nseq2d(c, U, V, R, E, dU, dV, dR, dE);
     else nseq3d(c, U, V, W, R, E, dU, dV, dW, dR, dE);
+    if (c->nForce > 0) forcings(c, U, V, W, R, E, dU, dV, dW, dE);
 }
 
 /* ------------------------------------------------------------------------- */

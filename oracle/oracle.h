@@ -66,6 +66,12 @@ typedef struct {
     double sfdDelta;
     const double *sfdChi;            /* nx*ny*nz field (type 1: filled by caller) */
     int timeStepping;                /* parameters.F90 timeStepping: 1 (or 0) RK4, 2 Euler, 3 SSPRK3 */
+    /* forcings of runForcings2D/3D.F90, applied at the end of nseq (nseq.F90:137, 321) in
+     * order: type 1 = pressureGradient (par dpdx; dU += dpdx/R), 2 = turbulenceGenerator
+     * (par epsilon, e0; on U, V, W, E); forceInd (nForce,6) col-major 1-based boxes */
+    int nForce;
+    const int *forceType, *forceInd;
+    const double *forcePar;          /* two per forcing */
 } orc_case;
 
 int orc_num_threads(void);

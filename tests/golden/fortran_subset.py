@@ -244,6 +244,13 @@ def _min(*a):
     return r
 
 
+def _sum(a):
+    """Fortran sum: the elements added one after the other in array-element (column-major)
+    order, as a sequential loop does (numpy's own reduction adds pairwise)."""
+    a = _np.asarray(a)
+    return _np.cumsum(_np.ravel(a, order="F"))[-1] if a.size else 0.0
+
+
 def _frange(a, b, s=1):
     return range(int(a), int(b) + (1 if s > 0 else -1), int(s))
 
@@ -251,8 +258,13 @@ def _frange(a, b, s=1):
 _INTRINSIC = {
     "modulo": "_modulo", "mod": "_mod", "sqrt": "_np.sqrt", "dsqrt": "_np.sqrt", "abs": "_np.abs",
     "dabs": "_np.abs", "max": "_max", "min": "_min", "dble": "_np.float64", "exp": "_np.exp",
-    "dexp": "_np.exp", "tanh": "_np.tanh", "sin": "_np.sin", "cos": "_np.cos",
+    "dexp": "_np.exp", "tanh": "_np.tanh", "sin": "_np.sin", "cos": "_np.cos", "sum": "_sum",
+    "dsin": "_np.sin", "dcos": "_np.cos",
 }
+
+# subroutines whose second argument receives the first (MPI reductions on one rank): their
+# results are scalars, which a Python call could not write back
+_COPY_OUT = ("mpi_allreduce", "mpi_reduce")
 
 
 def _pyname(n):
@@ -475,6 +487,9 @@ def translate_subroutine(sub, globals_arrays, trace=None):
             if "(" in rest:
                 nm = rest[:rest.index("(")].strip()
                 args = _split_top(rest[rest.index("(") + 1:_close_paren(rest, rest.index("("))])
+                if nm in _COPY_OUT:
+                    w(f"{emit(parse_expr(args[1]), sc)} = {emit(parse_expr(args[0]), sc)}")
+                    return
                 w(f"{_pyname(nm)}({', '.join(emit(parse_expr(a), sc) for a in args)})")
             else:
                 w(f"{_pyname(rest)}()")
@@ -599,7 +614,7 @@ def build(sources, globals_arrays, externals, trace=None, include_texts=None):
             names.append(sub.name)
     src = "\n".join(py)
     ns = {"_np": _np, "_div": _div, "_modulo": _modulo, "_mod": _mod, "_max": _max, "_min": _min,
-          "_frange": _frange, "_trace": trace if trace is not None else []}
+          "_frange": _frange, "_sum": _sum, "_trace": trace if trace is not None else []}
     ns.update({_pyname(k): v for k, v in globals_arrays.items()})
     ns.update({_pyname(k): v for k, v in externals.items()})
     exec(compile(src, "<fortran_subset>", "exec"), ns)

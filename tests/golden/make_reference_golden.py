@@ -54,11 +54,21 @@ def golden_cases():
         # break point at the leading edge, free-slip wall upstream, three x matrix types,
         # buffer zones, SFD
         "bl_cavity": cs.boundary_layer_cavity(nx=48, ny=32, buffers=((6, 5), (0, 6))),
+        # runForcings: turbulenceGenerator over the whole box (examples/turbulenceBox.m), and
+        # pressureGradient on part of the 2-D cavity channel
+        "turb_box": cs.turbulence_box(nxyz=(16, 12, 8)),
+        "cavity2d_dpdx": _with_forcing(cs.cavity_channel(nx=24, ny=24, nz=1, sfd={"X": 0.05, "Delta": 10.0, "buffer": 6}),
+                                       {"type": "pressureGradient", "ind": [3, 20, 2, 23, 1, 1], "par": [0.008]}),
     }
 
 
+def _with_forcing(case, f):
+    case.forcings = [f]
+    return case
+
+
 # cases that also hold one Euler and one SSPRK3 step (timeIntegration.F90:158-336, 500-680)
-SCHEME_CASES = ("box", "cavity2d", "lid", "bl_cavity")
+SCHEME_CASES = ("box", "cavity2d", "lid", "bl_cavity", "turb_box")
 
 
 def matrices_checksum(case):
@@ -69,6 +79,27 @@ def matrices_checksum(case):
         for a in (m.A, m.B, m.C, m.D, m.R, m.Af, m.Bf, m.Cf, m.Df, m.Rf, np.asarray(m.blocks)):
             h.update(np.ascontiguousarray(np.asarray(a, dtype=np.float64)).tobytes())
     return h.hexdigest()
+
+
+def forcing_include(case):
+    """runForcings2D/3D.F90 as writeFortranDisturbances.m:19-94 writes it for one rank
+    (forcing disturbances: no t; the variables, then their right-hand sides d<var>)."""
+    lines = ["    select case (nrank)", "        case (0)"]
+    for f in getattr(case, "forcings", None) or []:
+        i1, i2, j1, j2, k1, k2 = (int(x) for x in f["ind"])
+        X = np.asarray(case.X, dtype=np.float64)[i1 - 1:i2]
+        Y = np.asarray(case.Y, dtype=np.float64)[j1 - 1:j2]
+        Z = np.asarray(case.Z, dtype=np.float64)[k1 - 1:k2]
+        arr = lambda v: "(/" + ",".join("%.20fd0" % x for x in v) + "/)"  # noqa: E731
+        var = {"pressureGradient": "RU", "turbulenceGenerator": "UVWE"}[f["type"]]
+        s = "            call %s(%d,%d,%d,%s,%s,%s" % (f["type"], i2 - i1 + 1, j2 - j1 + 1, k2 - k1 + 1,
+                                                      arr(X), arr(Y), arr(Z))
+        box = "(%d:%d,%d:%d,%d:%d)" % (i1, i2, j1, j2, k1, k2)
+        s += "".join(",%s%s" % (v, box) for v in var) + "".join(",d%s%s" % (v, box) for v in var)
+        s += "".join(",%.20fd0" % p for p in f["par"])
+        lines.append(s + ")")
+    lines.append("    end select")
+    return "\n".join(lines) + "\n"
 
 
 def disturbance_include(case):
@@ -94,7 +125,8 @@ def reference(case, root):
     nx, ny, nz = case.nx, case.ny, case.nz
     src = os.path.join(root, "source")
     texts = [open(os.path.join(src, "Fortran", f)).read() for f in ("derivs.F90", "nseq.F90", "timeIntegration.F90")]
-    texts.append(open(os.path.join(src, "disturbances", "lidDrivenMovement.F90")).read())
+    for f in ("lidDrivenMovement", "pressureGradient", "turbulenceGenerator"):
+        texts.append(open(os.path.join(src, "disturbances", f + ".F90")).read())
     one = np.array([1, 1, 1])
     size = np.array([nx, ny, nz])
     g = {"xstart": one, "ystart": one, "zstart": one, "xend": size, "yend": size, "zend": size,
@@ -104,8 +136,13 @@ def reference(case, root):
         b[...] = a
 
     ext = {"transpose_x_to_y": copy, "transpose_y_to_x": copy, "transpose_y_to_z": copy,
-           "transpose_z_to_y": copy, "nrank": 0}
-    inc = {"rundisturbances.f90": disturbance_include(case)}
+           "transpose_z_to_y": copy, "nrank": 0, "mpi_real8": 0, "mpi_int": 0, "mpi_sum": 0,
+           "mpi_comm_world": 0}
+    # the generator writes the forcing calls into the include of the case's dimension and
+    # leaves the other one empty (writeFortranDisturbances.m:11-17)
+    inc = {"rundisturbances.f90": disturbance_include(case),
+           "runforcings3d.f90": forcing_include(case) if case.is3d else "",
+           "runforcings2d.f90": "" if case.is3d else forcing_include(case)}
     fns, _, _ = fs.build(texts, g, ext, include_texts=inc)
     return fns
 

@@ -15,7 +15,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-NAMES = ["box", "cavity3d", "cavity2d", "lid", "bl_cavity"]
+NAMES = ["box", "cavity3d", "cavity2d", "lid", "bl_cavity", "turb_box", "cavity2d_dpdx"]
 KEYS = ("U", "V", "W", "R", "E")
 
 
@@ -93,7 +93,7 @@ def test_time_step(gold):
 
 
 @pytest.mark.parametrize("scheme", [2, 3])
-@pytest.mark.parametrize("name", ["box", "cavity2d", "lid", "bl_cavity"])
+@pytest.mark.parametrize("name", ["box", "cavity2d", "lid", "bl_cavity", "turb_box"])
 def test_euler_and_ssprk3_steps(cuda_lib, name, scheme):
     """timeStepping 2 (EULER_2D/3D) and 3 (SSPRK3_2D/3D) against the reference's own
     integrators (gatt_set_time_stepping)."""

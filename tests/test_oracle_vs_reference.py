@@ -34,7 +34,7 @@ def rel(a, b):
     return float(np.max(np.abs(np.asarray(a) - b)) / (s if s > 0 else 1.0))
 
 
-NAMES = ["box", "cavity3d", "cavity2d", "lid", "bl_cavity"]
+NAMES = ["box", "cavity3d", "cavity2d", "lid", "bl_cavity", "turb_box", "cavity2d_dpdx"]
 
 
 @pytest.mark.parametrize("name", NAMES)
@@ -102,7 +102,7 @@ def test_time_step_matches_reference(oracle_lib, name):
 
 
 @pytest.mark.parametrize("scheme", [2, 3])
-@pytest.mark.parametrize("name", ["box", "cavity2d", "lid", "bl_cavity"])
+@pytest.mark.parametrize("name", ["box", "cavity2d", "lid", "bl_cavity", "turb_box"])
 def test_euler_and_ssprk3_steps_match_reference(oracle_lib, name, scheme):
     """timeStepping 2 (EULER_2D/3D) and 3 (SSPRK3_2D/3D) in the same main-loop step."""
     import dataclasses
