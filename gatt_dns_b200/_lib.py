@@ -33,6 +33,8 @@ SIGNATURES = {
     "gatt_set_corners": (_c_int, [_c_void_p, _c_int, _pi, _pi, _pi]),
     "gatt_add_disturbance": (_c_int, [_c_void_p, _c_int, _c_int, _pi, _pd, _c_int, _pd]),
     "gatt_clear_disturbances": (_c_int, [_c_void_p]),
+    "gatt_add_forcing": (_c_int, [_c_void_p, _c_int, _pi, _c_int, _pd]),
+    "gatt_clear_forcings": (_c_int, [_c_void_p]),
     "gatt_set_sfd": (_c_int, [_c_void_p, _c_int, _c_double, _c_double, _pd]),
     "gatt_upload": (_c_int, [_c_void_p, _c_int, _pd, _pd, _pd, _pd, _pd]),
     "gatt_download": (_c_int, [_c_void_p, _c_int, _pd, _pd, _pd, _pd, _pd]),

@@ -190,6 +190,9 @@ struct gatt_ctx {
     bool x_compact = true;  // compact shared memory for the uniform-band x solver (GATT_X_COMPACT=0: no)
     bool x_wstore = true;   // x tiles stored chunk by chunk by their warps (GATT_X_WSTORE=0: by one thread)
     int time_stepping = 1;  // parameters.F90 timeStepping: 1 RK4, 2 Euler, 3 SSPRK3
+    Forcings fc{};          // runForcings (fc.n = 0: none); boxes 0-based
+    double *fsum = nullptr, *fpart = nullptr;  // turbulence box sums, per-CTA partials
+    int fblocks = 0;        // CTAs of the sums kernel (fixed: the sums do not depend on timing)
     bool fork_x = true;     // x sweeps beside the y/z sweeps, filter field chains side by side
                             // (GATT_FORK_X=0: everything on one stream)
     bool fz_rev = true;     // last filter direction takes the fields in reverse order (GATT_FZ_REV=0: no)
@@ -844,6 +847,30 @@ bool pw_map(const gatt_ctx *c, CUtensorMap *map, const double *const *base, int 
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// The forcings as the assembly kernels take them, and the box sums of the turbulence
+// forcings over stage input q (runForcings: turbulenceGenerator sums its input fields).
+Forcings forcing_args(const gatt_ctx *c)
+{
+    Forcings f = c->fc;
+    f.sums = c->fsum;
+    f.nx = c->nx;
+    f.ny = c->ny;
+    return f;
+}
+
+int forcing_sums(gatt_ctx *c, const StateSet &q, int nmem)
+{
+    bool turb = false;
+    for (int f = 0; f < c->fc.n; f++) turb |= c->fc.type[f] == FORCE_TURBULENCE;
+    if (!turb) return GATT_OK;
+    TRY(before_launch(c, PC_OTHER));
+    k_forcing_sums<<<dim3(c->fblocks, nmem), 256, 0, c->stream>>>(q, forcing_args(c), c->fpart);
+    TRY(after_launch(c));
+    TRY(before_launch(c, PC_OTHER));
+    k_forcing_final<<<nmem, 32, 0, c->stream>>>(c->fpart, c->fblocks, c->fsum);
+    return after_launch(c);
+}
+
 // 3-D assembly fed by tensor copies (pwpipe.cuh).  Returns GATT_ERR_STATE without launching
 // when a set's layout does not fit the tensor maps; the caller then runs k_assemble3d.
 int launch_assemble3d_pipe(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet &out,
@@ -863,6 +890,7 @@ int launch_assemble3d_pipe(gatt_ctx *c, const StateSet &q, const StateSet &q0, c
         for (int f = 0; f < 5; f++)
             if (q0.v[f] != q.v[f] || q0.bstride != q.bstride) a.use_q0 = 1;
     a.err = c->d_err;
+    a.fs = forcing_args(c);
     PwMaps maps;
     memset(&maps, 0, sizeof(maps));
     const double *qb[5], *q0b[5], *d1b[D3_N], *d2b[S3_N], *dlb[5];
@@ -890,11 +918,12 @@ int assemble3d(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSe
 {
     const long long n = c->npts;
     const FieldSet fd = fset(c, delta, 5), f1 = fset(c, d1, D3_N), f2 = fset(c, d2, S3_N);
+    TRY(forcing_sums(c, q, nmem));
     const int pr = launch_assemble3d_pipe(c, q, q0, out, fd, f1, f2, mode, nmem);
     if (pr != GATT_ERR_STATE) return pr;
     TRY(before_launch(c, PC_ASSEMBLE));
     k_assemble3d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(c->ph, q, q0, out, fd, f1, f2, n, mode,
-                                                                      c->d_params);
+                                                                      c->d_params, forcing_args(c));
     return after_launch(c);
 }
 
@@ -984,7 +1013,8 @@ int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet
     TRY(sweep(c, 1, 0, tq, btq, iy, d2, bd2, sy, 3, nmem, 0, nullptr, PC_D2Y));
     TRY(before_launch(c, PC_ASSEMBLE));
     k_assemble2d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(
-        c->ph, q, q0, out, fset(c, delta, 5), fset(c, d1, D2_N), fset(c, tq, T2_N), fset(c, d2, S2_N), n, mode, sp);
+        c->ph, q, q0, out, fset(c, delta, 5), fset(c, d1, D2_N), fset(c, tq, T2_N), fset(c, d2, S2_N), n, mode, sp,
+        forcing_args(c));
     return after_launch(c);
 }
 
@@ -1735,6 +1765,7 @@ int check_diff(gatt_ctx *c, bool adjoint, bool step = false)
     TRY(check_ready(c, true));
     if (step && c->time_stepping != 1)
         return fail(GATT_ERR_STATE, "the tangent-linear and adjoint steps are those of RK4 (timeStepping 1)");
+    if (c->fc.n > 0) return fail(GATT_ERR_STATE, "the tangent-linear and adjoint do not cover forcings");
     if (c->bc_dirty) TRY(build_bc_program(c));
     if (step && diff_sfd(c) && (!c->mean || !c->mean_init))
         return fail(GATT_ERR_STATE, "SFD: upload the mean (gatt_upload_mean) or run a step before the tangent/adjoint");
@@ -2427,6 +2458,7 @@ void gatt_destroy(gatt_ctx *c)
     for (double *p : dbufs) cudaFree(p);
     for (double *p : bufs) cudaFree(p);
     cudaFree(c->d_ops); cudaFree(c->acc); cudaFree(c->d_params);
+    cudaFree(c->fsum); cudaFree(c->fpart);
     if (c->h_params) cudaFreeHost(c->h_params);
     if (c->h_err) cudaFreeHost(c->h_err);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -2636,6 +2668,43 @@ int gatt_add_disturbance(gatt_ctx *c, int type, int var, const int *ind, const d
     d.par = par[0];
     c->dists.push_back(d);
     c->bc_dirty = true;
+    invalidate_graphs(c);
+    return GATT_OK;
+}
+
+int gatt_add_forcing(gatt_ctx *c, int type, const int *ind, int npar, const double *par)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    if (type != GATT_FORCE_PRESSURE_GRADIENT && type != GATT_FORCE_TURBULENCE)
+        return fail(GATT_ERR_BADARG, "forcing type must be GATT_FORCE_PRESSURE_GRADIENT or GATT_FORCE_TURBULENCE");
+    if (c->fc.n >= kMaxForcings) return fail(GATT_ERR_BADARG, "at most 4 forcings");
+    if (type == GATT_FORCE_TURBULENCE && !c->is3d)
+        return fail(GATT_ERR_BADARG, "turbulenceGenerator acts on U, V, W, E: 3-D only");
+    const int need = type == GATT_FORCE_TURBULENCE ? 2 : 1;
+    if (!ind || npar < need || !par) return fail(GATT_ERR_BADARG, "forcing needs its box and parameters");
+    const int lim[3] = {c->nx, c->ny, c->nz};
+    for (int d = 0; d < 3; d++)
+        if (ind[2 * d] < 1 || ind[2 * d + 1] > lim[d] || ind[2 * d] > ind[2 * d + 1])
+            return fail(GATT_ERR_BADARG, "forcing box outside the grid");
+    if (!c->fsum) {
+        c->fblocks = 2 * c->nsm;
+        CU(cudaMalloc(&c->fsum, sizeof(double) * (size_t)c->nb * kMaxForcings * 5));
+        CU(cudaMalloc(&c->fpart, sizeof(double) * (size_t)c->nb * kMaxForcings * c->fblocks * 5));
+    }
+    const int f = c->fc.n++;
+    c->fc.type[f] = type;
+    for (int q = 0; q < 6; q++) c->fc.box[f][q] = ind[q] - 1;
+    c->fc.par[f][0] = par[0];
+    c->fc.par[f][1] = need > 1 ? par[1] : 0.0;
+    c->fc.N[f] = (double)((long long)(ind[1] - ind[0] + 1) * (ind[3] - ind[2] + 1) * (ind[5] - ind[4] + 1));
+    invalidate_graphs(c);
+    return GATT_OK;
+}
+
+int gatt_clear_forcings(gatt_ctx *c)
+{
+    if (!c) return fail(GATT_ERR_BADARG, "null context");
+    c->fc.n = 0;
     invalidate_graphs(c);
     return GATT_OK;
 }

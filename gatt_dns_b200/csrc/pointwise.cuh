@@ -41,6 +41,49 @@ struct StepParams {
 enum { RK_STORE_RHS = 0, RK_STAGE1 = 1, RK_STAGE2 = 2, RK_STAGE3 = 3, RK_STAGE4 = 4, RK_EULER = 5,
        SSP_STAGE1 = 6, SSP_STAGE2 = 7, SSP_STAGE3 = 8 };
 
+// ---- forcings (runForcings2D/3D.F90: disturbances with forcing = true) ---------------------
+// Applied to the right-hand side nseq forms, in order, on 0-based inclusive boxes:
+// FORCE_PRESSURE_GRADIENT (pressureGradient.F90): du = du + dpdx/r; FORCE_TURBULENCE
+// (turbulenceGenerator.F90, one rank): with the box sums ET = sum(u u + v v + w w), U..E of
+// the right-hand side's input state and N points, du = du + 0.25*eps*N/ET*u - gamma*Usum/N
+// (gamma = 10 eps, likewise v, w) and de = de - gamma*(Esum/N - e0).
+constexpr int kMaxForcings = 4;
+enum { FORCE_PRESSURE_GRADIENT = 1, FORCE_TURBULENCE = 2 };
+struct Forcings {
+    int n;
+    int type[kMaxForcings];
+    int box[kMaxForcings][6];
+    double par[kMaxForcings][2];
+    double N[kMaxForcings];   // points of each box
+    const double *sums;       // [member][kMaxForcings][5]: ET, U, V, W, E sums (turbulence)
+    int nx, ny;
+};
+
+// k[] in U, V, W, R, E order; mom / en: apply the momentum (U, V, W) / energy rows only.
+__device__ __forceinline__ void apply_forcings(const Forcings &fs, int b, long long p, double u, double v,
+                                               double w, double r, double e, double k[5], bool mom, bool en)
+{
+    const int i = (int)(p % fs.nx);
+    const long long jk = p / fs.nx;
+    const int j = (int)(jk % fs.ny), kz = (int)(jk / fs.ny);
+    for (int f = 0; f < fs.n; f++) {
+        const int *bx = fs.box[f];
+        if (i < bx[0] || i > bx[1] || j < bx[2] || j > bx[3] || kz < bx[4] || kz > bx[5]) continue;
+        if (fs.type[f] == FORCE_PRESSURE_GRADIENT) {
+            if (mom) k[0] = k[0] + fs.par[f][0] / r;
+        } else if (fs.type[f] == FORCE_TURBULENCE) {
+            const double *S = fs.sums + ((size_t)b * kMaxForcings + f) * 5;
+            const double eps = fs.par[f][0], e0 = fs.par[f][1], gamma = 10 * eps, N = fs.N[f];
+            if (mom) {
+                k[0] = k[0] + 0.25 * eps * N / S[0] * u - gamma * S[1] / N;
+                k[1] = k[1] + 0.25 * eps * N / S[0] * v - gamma * S[2] / N;
+                k[2] = k[2] + 0.25 * eps * N / S[0] * w - gamma * S[3] / N;
+            }
+            if (en) k[4] = k[4] - gamma * (S[4] / N - e0);
+        }
+    }
+}
+
 // Whether a stage update reads / writes the increment accumulator delta.
 __host__ __device__ __forceinline__ bool mode_reads_delta(int m)
 {
@@ -64,6 +107,58 @@ struct StateSet {
     double *v[5];
     long long bstride;
 };
+
+// Box sums of every turbulence forcing: each CTA (blockIdx.x of gridDim.x, member
+// blockIdx.y) sums its grid-stride share of the box points in a fixed order into
+// part[((b * kMaxForcings + f) * gridDim.x + cta) * 5 + q]; k_forcing_final adds the CTAs'
+// partials in CTA order, so the sums do not depend on timing.
+__global__ void __launch_bounds__(256) k_forcing_sums(StateSet q, Forcings fs, double *part)
+{
+    __shared__ double red[5][256];
+    const int b = blockIdx.y;
+    const double *U = q.v[0] + b * q.bstride, *V = q.v[1] + b * q.bstride, *W = q.v[2] + b * q.bstride;
+    const double *E = q.v[4] + b * q.bstride;
+    for (int f = 0; f < fs.n; f++) {
+        if (fs.type[f] != FORCE_TURBULENCE) continue;
+        const int *bx = fs.box[f];
+        const long long ni = bx[1] - bx[0] + 1, nj = bx[3] - bx[2] + 1, nk = bx[5] - bx[4] + 1;
+        const long long m = ni * nj * nk;
+        double s[5] = {0, 0, 0, 0, 0};
+        for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < m; t += (long long)gridDim.x * blockDim.x) {
+            const long long i = bx[0] + t % ni, j = bx[2] + (t / ni) % nj, kz = bx[4] + t / (ni * nj);
+            const long long p = i + fs.nx * (j + (long long)fs.ny * kz);
+            const double u = U[p], v = V[p], w = W[p];
+            s[0] += u * u + v * v + w * w;
+            s[1] += u;
+            s[2] += v;
+            s[3] += w;
+            s[4] += E[p];
+        }
+        for (int c = 0; c < 5; c++) red[c][threadIdx.x] = s[c];
+        __syncthreads();
+        for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+            if ((int)threadIdx.x < h)
+                for (int c = 0; c < 5; c++) red[c][threadIdx.x] += red[c][threadIdx.x + h];
+            __syncthreads();
+        }
+        if (threadIdx.x < 5)
+            part[(((size_t)b * kMaxForcings + f) * gridDim.x + blockIdx.x) * 5 + threadIdx.x] = red[threadIdx.x][0];
+        __syncthreads();
+    }
+}
+
+__global__ void k_forcing_final(const double *part, int nblocks, double *sums)
+{
+    // one thread per (member, forcing, quantity): blockIdx.x = member
+    const int t = threadIdx.x;  // f * 5 + q
+    if (t >= kMaxForcings * 5) return;
+    const int f = t / 5, qd = t % 5;
+    const double *pp = part + ((size_t)blockIdx.x * kMaxForcings + f) * nblocks * 5 + qd;
+    double s = 0;
+    for (int c = 0; c < nblocks; c++) s += pp[(size_t)c * 5];
+    sums[((size_t)blockIdx.x * kMaxForcings + f) * 5 + qd] = s;
+}
+
 
 __device__ __forceinline__ double sutherland_mu(const Phys &ph, double E)
 {
@@ -245,7 +340,7 @@ __device__ __forceinline__ void assemble3d_rhs(const Phys &ph, Ld ld, double k[5
 // q: stage input; q0: step start; out: stage output (may alias q: pointwise in place).
 __global__ void __launch_bounds__(256, 3) k_assemble3d(Phys ph, StateSet q, StateSet q0, StateSet out, FieldSet delta,
                                                        FieldSet d1, FieldSet d2, long long n, int mode,
-                                                       const StepParams *sp)
+                                                       const StepParams *sp, Forcings fs)
 {
     const int b = blockIdx.y;
     const double dt = sp ? sp->dt : 0.0;
@@ -255,6 +350,7 @@ __global__ void __launch_bounds__(256, 3) k_assemble3d(Phys ph, StateSet q, Stat
         };
         double k[5];
         assemble3d_rhs(ph, ld, k);
+        if (fs.n) apply_forcings(fs, b, p, ld(A3_Q + 0), ld(A3_Q + 1), ld(A3_Q + 2), ld(A3_Q + 3), ld(A3_Q + 4), k, true, true);
 #pragma unroll
         for (int f = 0; f < 5; f++) {
             double *dl = delta.p ? delta.f(b, f) + p : nullptr;
@@ -271,7 +367,7 @@ __global__ void __launch_bounds__(256, 3) k_assemble3d(Phys ph, StateSet q, Stat
 // 2-D assembly (nseq.F90:126-132) fused with the RK4 stage update.  W is left alone.
 __global__ void k_assemble2d(Phys ph, StateSet q, StateSet q0, StateSet out, FieldSet delta,
                              FieldSet d1, FieldSet tq, FieldSet d2, long long n, int mode,
-                             const StepParams *sp)
+                             const StepParams *sp, Forcings fs)
 {
     const int b = blockIdx.y;
     const double dt = sp ? sp->dt : 0.0;
@@ -295,7 +391,8 @@ __global__ void k_assemble2d(Phys ph, StateSet q, StateSet q0, StateSet out, Fie
         const double kE = -(dex * u + dey * v)
                         + (-P * (dux + dvy) + tq.f(b, T2_XX)[p] * dux + tq.f(b, T2_YY)[p] * dvy
                            + tq.f(b, T2_XY)[p] * (dvx + duy) - d2.f(b, S2_HTX)[p] - d2.f(b, S2_HTY)[p]) / r;
-        const double k[5] = {kU, kV, 0.0, kR, kE};
+        double k[5] = {kU, kV, 0.0, kR, kE};
+        if (fs.n) apply_forcings(fs, b, p, u, v, 0.0, r, e, k, true, true);  // pressure gradient (2-D)
 #pragma unroll
         for (int f = 0; f < 5; f++) {
             if (f == 2) continue;

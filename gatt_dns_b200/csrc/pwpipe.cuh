@@ -53,6 +53,7 @@ struct PwArgs {
     int use_delta;      // increments read (stages 2-4)
     int mode;           // RK_* of the stage update
     int *err;           // set to 1 when a wait gives up
+    Forcings fs;        // runForcings (none: fs.n = 0)
 };
 
 __global__ void __launch_bounds__(2 * kPwC, 1) k_assemble3d_pipe(Phys ph, StateSet out, FieldSet delta, PwArgs a,
@@ -131,10 +132,14 @@ __global__ void __launch_bounds__(2 * kPwC, 1) k_assemble3d_pipe(Phys ph, StateS
                 out.v[v][b * out.bstride + p] = res;
             };
             if (energy) {
-                epi(4, assemble3d_energy(ph, ld));
+                double kk[5];
+                kk[4] = assemble3d_energy(ph, ld);
+                if (a.fs.n) apply_forcings(a.fs, b, p, ld(0), ld(1), ld(2), ld(3), ld(4), kk, false, true);
+                epi(4, kk[4]);
             } else {
-                double kk[4];
+                double kk[5];
                 assemble3d_mom(ph, ld, kk);
+                if (a.fs.n) apply_forcings(a.fs, b, p, ld(0), ld(1), ld(2), ld(3), ld(4), kk, true, false);
 #pragma unroll
                 for (int v = 0; v < 4; v++) epi(v, kk[v]);
             }

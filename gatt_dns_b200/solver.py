@@ -20,6 +20,7 @@ _pi = ctypes.POINTER(ctypes.c_int)
 
 KIND = {"d": 0, "n": 1, "s": 2}
 DIST_TYPE = {"lidDrivenMovement": 1}
+FORCE_TYPE = {"pressureGradient": 1, "turbulenceGenerator": 2}  # GATT_FORCE_*
 
 
 def _dp(a):
@@ -110,6 +111,11 @@ class GattDNS:
             par = _f64(d["par"])
             _lib.check(L.gatt_add_disturbance(self.h, DIST_TYPE[d["type"]], VAR_INDEX[d["var"]], _ip(ind), _dp(x),
                                               par.size, _dp(par)), "gatt_add_disturbance")
+        for f in getattr(c, "forcings", None) or []:
+            ind = np.ascontiguousarray(np.asarray(f["ind"], dtype=np.int32))
+            par = _f64(f["par"])
+            _lib.check(L.gatt_add_forcing(self.h, FORCE_TYPE[f["type"]], _ip(ind), par.size, _dp(par)),
+                       "gatt_add_forcing")
         if c.sfd_type > 0:
             chi = _f64(c.sfd_chi) if c.sfd_chi is not None else None
             _lib.check(L.gatt_set_sfd(self.h, c.sfd_type, c.sfd_delta, c.sfd_X, _dp(chi)), "gatt_set_sfd")

@@ -112,6 +112,20 @@ int gatt_add_disturbance(gatt_ctx *ctx, int type, int var, const int *ind, const
                          int npar, const double *par);
 int gatt_clear_disturbances(gatt_ctx *ctx);
 
+/* Forcings: the disturbances with forcing = true, which writeFortranDisturbances.m writes
+ * into runForcings2D/3D.F90 and nseq2d/3d applies to the right-hand side it has formed
+ * (nseq.F90:137, 321), in the order they are added, each on the 1-based box ind[6]:
+ * GATT_FORCE_PRESSURE_GRADIENT = pressureGradient.F90 (par[0] = dpdx; dU += dpdx/R);
+ * GATT_FORCE_TURBULENCE = turbulenceGenerator.F90 (par = {epsilon, e0}; 3-D only; box sums
+ * of U*U + V*V + W*W, U, V, W, E of the right-hand side's input, then dU += 0.25*epsilon*
+ * N/ET*U - 10*epsilon*Usum/N, likewise V and W, and dE -= 10*epsilon*(Esum/N - e0); one GPU
+ * holds the whole box, as one rank does).  At most 4.  The tangent-linear and adjoint entry
+ * points refuse contexts with forcings (GATT_ERR_STATE). */
+#define GATT_FORCE_PRESSURE_GRADIENT 1
+#define GATT_FORCE_TURBULENCE 2
+int gatt_add_forcing(gatt_ctx *ctx, int type, const int *ind, int npar, const double *par);
+int gatt_clear_forcings(gatt_ctx *ctx);
+
 /* SFD (main.F90:122-164, 381-402): type 0 off, 1 constant chi = chiValue, 2 field chi
  * (nx*ny*nz, from calcSFDregion.m).  Delta <= 0 freezes the mean flow. */
 int gatt_set_sfd(gatt_ctx *ctx, int type, double Delta, double chiValue, const double *chi);

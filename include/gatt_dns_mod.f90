@@ -104,6 +104,19 @@ module gatt_dns
             type(c_ptr), value :: ctx
             integer(c_int) :: gatt_clear_disturbances
         end function
+        function gatt_add_forcing(ctx, ftype, ind, npar, par) bind(C, name='gatt_add_forcing')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: ctx
+            integer(c_int), value :: ftype, npar
+            integer(c_int), dimension(6) :: ind
+            real(c_double), dimension(*) :: par
+            integer(c_int) :: gatt_add_forcing
+        end function
+        function gatt_clear_forcings(ctx) bind(C, name='gatt_clear_forcings')
+            import :: c_int, c_ptr
+            type(c_ptr), value :: ctx
+            integer(c_int) :: gatt_clear_forcings
+        end function
         function gatt_set_sfd(ctx, stype, Delta, chiValue, chi) bind(C, name='gatt_set_sfd')
             import :: c_int, c_ptr, c_double
             type(c_ptr), value :: ctx

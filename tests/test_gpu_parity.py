@@ -210,6 +210,50 @@ def test_euler_and_ssprk3_match_oracle(libs, name, scheme):
     g.close()
 
 
+@pytest.mark.parametrize("name", ["turb_box", "cavity2d_dpdx", "turb_box_multi"])
+def test_forcings_match_oracle(libs, name):
+    """runForcings: turbulenceGenerator over the whole box, pressureGradient on part of the
+    2-D cavity channel, and two forcings on sub-boxes; two batch members with different
+    flows (their box sums differ), three steps against the oracle; the tangent-linear and
+    adjoint refused."""
+    from gatt_dns_b200 import _lib
+    from gatt_dns_b200.solver import GattDNS
+    from oracle import Oracle
+    if name == "turb_box":
+        c = cs.turbulence_box(nxyz=(32, 24, 16))
+    elif name == "turb_box_multi":
+        c = cs.turbulence_box(nxyz=(24, 20, 16))
+        c.forcings = [{"type": "turbulenceGenerator", "ind": [3, 20, 1, 20, 2, 15], "par": [0.5, c.forcings[0]["par"][1]]},
+                      {"type": "pressureGradient", "ind": [1, 24, 5, 12, 1, 16], "par": [0.02]}]
+    else:
+        c = get_case("cavity2d")
+        import dataclasses
+        c = dataclasses.replace(c, forcings=[{"type": "pressureGradient", "ind": [3, 40, 2, 39, 1, 1], "par": [0.008]}])
+    g, o = GattDNS(c, nbatch=2), Oracle(c)
+    fa, fb = flow_for(c, seed=6), flow_for(c, seed=7)
+    dt = 0.1 * c.cfl_dt(fa["U"], fa["V"], fa["W"], 1.0)
+    g.upload(fa, 0)
+    g.upload(fb, 1)
+    if c.sfd_type:
+        g.upload_mean(fa, 0)
+        g.upload_mean(fb, 1)
+    sa, sb = o.new_state(fa), o.new_state(fb)
+    for s in range(3):
+        mg = g.step(s * dt, dt)
+        ma, mb = o.step(sa, s * dt, dt), o.step(sb, s * dt, dt)
+        # turbulence forcing: box sums added in another order (see test_gpu_reference_golden)
+        tol = 1e-8 if name.startswith("turb") else 1e-10
+        assert np.allclose(mg[0], ma, rtol=tol, atol=1e-15), (name, s, mg[0], ma)
+        assert np.allclose(mg[1], mb, rtol=tol, atol=1e-15), (name, s, mg[1], mb)
+    for b, st in ((0, sa), (1, sb)):
+        a = g.download(b)
+        for k in fields(c):
+            assert rel(a[k], st[k]) < STEP_TOL * 10, (name, b, k, rel(a[k], st[k]))
+    with pytest.raises(_lib.GattError):
+        g.jvp(g.download(0), 1, 0.0, dt)
+    g.close()
+
+
 def test_lid_driven_100_steps(libs):
     c, g, o = pair("lid")
     f = cs.uniform_flow(c)

@@ -37,6 +37,16 @@ def gold(request, cuda_lib):
     g.close()
 
 
+def _mc_rtol(case):
+    """Max-change tolerance: 1e-10, or 1e-8 with a turbulence forcing, whose box sums the GPU
+    adds in per-CTA partials instead of one after the other: a sum of N values of E ~ e0
+    rounds differently by up to N eps relative, and the forcing multiplies Esum/N - e0 (a
+    small difference of large numbers) by 10 epsilon; measured 1.1e-10 on the energy
+    max-change of the 16x12x8 box, 1.7e-13 on the state."""
+    forced = any(f["type"] == "turbulenceGenerator" for f in (getattr(case, "forcings", None) or []))
+    return 1e-8 if forced else 1e-10
+
+
 def _flow(z):
     return {k: np.asfortranarray(z["flow_" + k]) for k in KEYS}
 
@@ -81,7 +91,7 @@ def test_time_step(gold):
     if case.sfd_type:
         g.upload_mean(f)
     mc = g.step(float(z["t"]), float(z["dt"]))[0]
-    assert np.allclose(mc, z["step_maxchange"], rtol=1e-10, atol=1e-14), (name, mc, z["step_maxchange"])
+    assert np.allclose(mc, z["step_maxchange"], rtol=_mc_rtol(case), atol=1e-14), (name, mc, z["step_maxchange"])
     out = g.download()
     for k in KEYS:
         got = g.download_wnew() if (k == "W" and not case.is3d) else out[k]
@@ -110,7 +120,7 @@ def test_euler_and_ssprk3_steps(cuda_lib, name, scheme):
     if case.sfd_type:
         g.upload_mean(f)
     mc = g.step(float(z["t"]), float(z["dt"]))[0]
-    assert np.allclose(mc, z[key + "maxchange"], rtol=1e-10, atol=1e-14), (name, scheme, mc)
+    assert np.allclose(mc, z[key + "maxchange"], rtol=_mc_rtol(case), atol=1e-14), (name, scheme, mc)
     out = g.download()
     for k in KEYS:
         got = g.download_wnew() if (k == "W" and not case.is3d) else out[k]
