@@ -1,7 +1,8 @@
 """Read and write the generated Fortran include files of a reference case.
 
 The reference MATLAB preprocessing writes ``<case>/bin/parameters.F90``, ``matrices.F90``,
-``boundaryInfo.F90`` and ``runDisturbances.F90`` (``source/writeFortranParameters.m``,
+``boundaryInfo.F90``, ``runDisturbances.F90`` and ``runForcings2D/3D.F90``
+(``source/writeFortranParameters.m``,
 ``writeFortranMatrices.m``, ``writeFortranBoundaries.m``, ``writeFortranDisturbances.m``)
 and compiles them into the solver.  This module parses those files into a
 :class:`~gatt_dns_b200.case.Case` so an existing case directory drives the GPU path
@@ -264,6 +265,47 @@ def write_run_disturbances_f90(case: Case, path):
         f.write("    end select\n")
 
 
+_FORCING_VARS = {"pressureGradient": "RU", "turbulenceGenerator": "UVWE"}
+
+
+def write_run_forcings_f90(case: Case, path):
+    """runForcings2D/3D.F90 lines for the forcings of a case (writeFortranDisturbances.m:35-90
+    with forcing = true: no t; each variable's box, then its right-hand side's d<var>)."""
+    with open(path, "w") as f:
+        f.write("    select case (nrank)\n        case (0)\n")
+        for d in getattr(case, "forcings", None) or []:
+            i = [int(v) for v in d["ind"]]
+            X, Y, Z = case.X[i[0] - 1:i[1]], case.Y[i[2] - 1:i[3]], case.Z[i[4] - 1:i[5]]
+            args = "%d,%d,%d,(/%s/),(/%s/),(/%s/)" % (
+                i[1] - i[0] + 1, i[3] - i[2] + 1, i[5] - i[4] + 1, ",".join(_fmt(v) for v in X),
+                ",".join(_fmt(v) for v in Y), ",".join(_fmt(v) for v in Z))
+            box = "(%d:%d,%d:%d,%d:%d)" % tuple(i)
+            var = _FORCING_VARS[d["type"]]
+            args += "".join(",%s%s" % (v, box) for v in var) + "".join(",d%s%s" % (v, box) for v in var)
+            args += "".join("," + _fmt(p) for p in d["par"])
+            f.write("            call %s(%s)\n" % (d["type"], args))
+        f.write("    end select\n")
+
+
+def read_run_forcings_f90(path):
+    """Forcing calls of rank 0 (pressureGradient and turbulenceGenerator)."""
+    text = open(path).read()
+    if "case" not in text:
+        return []
+    r0, _ = _rank0(text)
+    out = []
+    for m in re.finditer(r"call\s+(\w+)\s*\((.*)\)\s*$", r0, re.M):
+        name, args = m.group(1), m.group(2)
+        if name not in _FORCING_VARS:
+            continue
+        boxes = list(re.finditer(r",d?[UVWRE]\((\d+):(\d+),(\d+):(\d+),(\d+):(\d+)\)", args))
+        ind = np.array([int(boxes[0].group(k)) for k in range(1, 7)], dtype=np.int32)
+        tail = args[boxes[-1].end():]
+        par = [_to_float(t) for t in tail.split(",") if t.strip()]
+        out.append(dict(type=name, ind=ind, par=par))
+    return out
+
+
 def read_run_disturbances_f90(path):
     """Disturbance calls of rank 0 (only lidDrivenMovement is supported by the GPU path)."""
     text = open(path).read()
@@ -298,11 +340,17 @@ def case_from_fortran_dir(bin_dir, name="reference_case", sfd_chi=None):
     rd = os.path.join(bin_dir, "runDisturbances.F90")
     if os.path.exists(rd):
         bc.disturbances = [d for d in read_run_disturbances_f90(rd) if d["type"] == "lidDrivenMovement"]
+    forcings = []
+    for nm in ("runForcings3D.F90", "runForcings2D.F90"):
+        rf = os.path.join(bin_dir, nm)
+        if os.path.exists(rf):
+            forcings += read_run_forcings_f90(rf)
     dxmin = tuple(p.get("dxmin", [0.0, 0.0, 0.0]))
     c = Case(name=name, nx=nx, ny=ny, nz=nz, Re=p["Re"], Ma=p["Ma"], Pr=p["Pr"], gamma=p["gamma"], T0=p["T0"],
              X=np.arange(1, nx + 1, dtype=float), Y=np.arange(1, ny + 1, dtype=float),
              Z=np.arange(1, nz + 1, dtype=float), mats=mats, bc=bc, filterDirections=filt,
-             filterCharTime=p.get("FilterCharTime", -1.0), dxmin=dxmin)
+             filterCharTime=p.get("FilterCharTime", -1.0), dxmin=dxmin,
+             time_stepping=int(p.get("timeStepping", 1)), forcings=forcings or None)
     sfd = p.get("SFD", 0)
     if sfd:
         c.sfd_type, c.sfd_delta, c.sfd_X = sfd, p.get("SFD_Delta", 0.0), p.get("SFD_X_val", 0.0)
@@ -322,3 +370,5 @@ def write_parameters_f90(case: Case, path, dt=1.0, max_cfl=1.0):
         f.write("    real*8 :: FilterCharTime = %s\n" % _fmt(case.filterCharTime))
         f.write("    real*8,dimension(3) :: dxmin = (/%s,%s,%s/)\n\n" % tuple(_fmt(v) for v in case.dxmin))
         f.write("    integer :: p_row = 1\n    integer :: p_col = 1\n")
+        # writeFortranParameters.m:50-57: RK4 1, Euler 2, SSPRK3 3
+        f.write("    integer :: timeStepping = %d\n" % int(getattr(case, "time_stepping", 1)))

@@ -36,6 +36,7 @@ sys.path.insert(0, os.path.join(HERE, "..", ".."))
 
 import fortran_subset as fs  # noqa: E402
 from gatt_dns_b200 import case as cs  # noqa: E402
+from gatt_dns_b200 import fortran_io as fio  # noqa: E402
 
 VARS = ("U", "V", "W", "P", "E")
 
@@ -81,44 +82,24 @@ def matrices_checksum(case):
     return h.hexdigest()
 
 
+def _emitted(writer, case):
+    """The text the repository's emitter writes (gatt_dns_b200.fortran_io), so that the
+    reference runs on the emitter's include files and the fixtures check the emitter too."""
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "inc.F90")
+        writer(case, path)
+        return open(path).read()
+
+
 def forcing_include(case):
-    """runForcings2D/3D.F90 as writeFortranDisturbances.m:19-94 writes it for one rank
-    (forcing disturbances: no t; the variables, then their right-hand sides d<var>)."""
-    lines = ["    select case (nrank)", "        case (0)"]
-    for f in getattr(case, "forcings", None) or []:
-        i1, i2, j1, j2, k1, k2 = (int(x) for x in f["ind"])
-        X = np.asarray(case.X, dtype=np.float64)[i1 - 1:i2]
-        Y = np.asarray(case.Y, dtype=np.float64)[j1 - 1:j2]
-        Z = np.asarray(case.Z, dtype=np.float64)[k1 - 1:k2]
-        arr = lambda v: "(/" + ",".join("%.20fd0" % x for x in v) + "/)"  # noqa: E731
-        var = {"pressureGradient": "RU", "turbulenceGenerator": "UVWE"}[f["type"]]
-        s = "            call %s(%d,%d,%d,%s,%s,%s" % (f["type"], i2 - i1 + 1, j2 - j1 + 1, k2 - k1 + 1,
-                                                      arr(X), arr(Y), arr(Z))
-        box = "(%d:%d,%d:%d,%d:%d)" % (i1, i2, j1, j2, k1, k2)
-        s += "".join(",%s%s" % (v, box) for v in var) + "".join(",d%s%s" % (v, box) for v in var)
-        s += "".join(",%.20fd0" % p for p in f["par"])
-        lines.append(s + ")")
-    lines.append("    end select")
-    return "\n".join(lines) + "\n"
+    """runForcings2D/3D.F90 (writeFortranDisturbances.m:19-94, forcing = true), one rank."""
+    return _emitted(fio.write_run_forcings_f90, case)
 
 
 def disturbance_include(case):
-    """runDisturbances.F90 as writeFortranDisturbances.m:19-94 writes it for one rank."""
-    lines = ["    select case (nrank)", "        case (0)"]
-    for d in case.bc.disturbances:
-        i1, i2, j1, j2, k1, k2 = (int(x) for x in d["ind"])
-        X = np.asarray(d["X"], dtype=np.float64)
-        Y = np.asarray(case.Y, dtype=np.float64)[j1 - 1:j2]
-        Z = np.asarray(case.Z, dtype=np.float64)[k1 - 1:k2]
-        typ = {1: "lidDrivenMovement"}.get(d["type"], d["type"]) if not isinstance(d["type"], str) else d["type"]
-        arr = lambda v: "(/" + ",".join("%.20fd0" % x for x in v) + "/)"  # noqa: E731
-        s = "            call %s(%d,%d,%d,%s,%s,%s,t" % (typ, i2 - i1 + 1, j2 - j1 + 1, k2 - k1 + 1, arr(X), arr(Y), arr(Z))
-        s += ",%s(%d:%d,%d:%d,%d:%d)" % (d["var"], i1, i2, j1, j2, k1, k2)
-        for p in d["par"]:
-            s += ",%.20fd0" % p
-        lines.append(s + ")")
-    lines.append("    end select")
-    return "\n".join(lines) + "\n"
+    """runDisturbances.F90 (writeFortranDisturbances.m:19-94), one rank."""
+    return _emitted(fio.write_run_disturbances_f90, case)
 
 
 def reference(case, root):

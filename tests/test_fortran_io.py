@@ -49,3 +49,24 @@ def test_periodic_and_corner_round_trip(tmp_path):
         _same_mats(a, b)
     assert np.array_equal(r.bc.cL, c.bc.cL) and np.array_equal(r.bc.cD, c.bc.cD)
     assert np.array_equal(r.bc.cAdiabatic, c.bc.cAdiabatic)
+
+
+def test_forcings_and_time_stepping_round_trip(tmp_path):
+    """runForcings3D.F90 (turbulenceGenerator, pressureGradient) and parameters.F90's
+    timeStepping through the emitter and the reader; the golden vectors run the reference
+    on these same emitted files (tests/golden/make_reference_golden.py)."""
+    import dataclasses
+    c = cs.turbulence_box(nxyz=(12, 10, 8))
+    c.forcings.append({"type": "pressureGradient", "ind": [2, 11, 1, 10, 3, 6], "par": [0.125]})
+    c = dataclasses.replace(c, time_stepping=3)
+    fio.write_parameters_f90(c, tmp_path / "parameters.F90")
+    fio.write_matrices_f90(c, tmp_path / "matrices.F90")
+    fio.write_boundary_info_f90(c, tmp_path / "boundaryInfo.F90")
+    fio.write_run_forcings_f90(c, tmp_path / "runForcings3D.F90")
+    (tmp_path / "runForcings2D.F90").write_text("")
+    r = fio.case_from_fortran_dir(str(tmp_path))
+    assert r.time_stepping == 3
+    assert len(r.forcings) == 2
+    for a, b in zip(c.forcings, r.forcings):
+        assert a["type"] == b["type"] and np.array_equal(np.asarray(a["ind"]), b["ind"])
+        assert np.array_equal(np.asarray(a["par"], dtype=float), np.asarray(b["par"], dtype=float))
