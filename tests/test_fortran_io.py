@@ -56,7 +56,7 @@ def test_forcings_and_time_stepping_round_trip(tmp_path):
     timeStepping through the emitter and the reader; the golden vectors run the reference
     on these same emitted files (tests/golden/make_reference_golden.py)."""
     import dataclasses
-    c = cs.turbulence_box(nxyz=(12, 10, 8))
+    c = cs.turbulence_box(nxyz=(16, 12, 8))
     c.forcings.append({"type": "pressureGradient", "ind": [2, 11, 1, 10, 3, 6], "par": [0.125]})
     c = dataclasses.replace(c, time_stepping=3)
     fio.write_parameters_f90(c, tmp_path / "parameters.F90")
