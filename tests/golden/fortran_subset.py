@@ -12,13 +12,15 @@ Covered: subroutines with explicit-shape, automatic and assumed-shape array dumm
 lower bounds), real*8 / integer declarations, whole-array and array-section assignments
 (evaluated element by element with numpy, the same IEEE operations in the same order as
 the Fortran expression tree), do loops with steps, if / else if / else blocks, one-line ifs,
-select case, call, array constructors, and the intrinsics modulo, mod, sqrt / dsqrt, abs,
-max, min, dble.  Array
-sections passed to a subroutine are numpy views, so intent(inout) dummies write through.
-``include`` lines are spliced in from texts the caller supplies (the generated disturbance
-hook, written the way the reference's generator writes it) or dropped (the forcing hooks:
-the golden cases have no forcing).  Default-real literals are single precision, as in
-Fortran.  Not covered (absent from these files): strings, pointers, where / forall.
+select case, call, array constructors, SAVE variables (with initialisers) and allocatable
+arrays with allocate, and the intrinsics modulo, mod, sqrt / dsqrt, abs, max, min, dble,
+sum (added in array-element order), atan / datan, sin / dsin.  Array sections passed to a
+subroutine are numpy views, so intent(inout) dummies write through; MPI reductions on one
+rank copy their input to their output.  ``include`` lines are spliced in from texts the
+caller supplies (the generated disturbance and forcing hooks, written by the repository's
+emitter the way the reference's generator writes them) or dropped.  Default-real literals
+and variables are single precision, as in Fortran.  Not covered (absent from these files):
+strings, pointers, complex numbers, where / forall.
 """
 from __future__ import annotations
 
@@ -251,6 +253,11 @@ def _sum(a):
     return _np.cumsum(_np.ravel(a, order="F"))[-1] if a.size else 0.0
 
 
+def _r4(v):
+    """A value stored in a default-real (single-precision) variable."""
+    return float(_np.float32(v)) if _np.ndim(v) == 0 else _np.asarray(v, dtype=_np.float32).astype(_np.float64)
+
+
 def _frange(a, b, s=1):
     return range(int(a), int(b) + (1 if s > 0 else -1), int(s))
 
@@ -259,7 +266,7 @@ _INTRINSIC = {
     "modulo": "_modulo", "mod": "_mod", "sqrt": "_np.sqrt", "dsqrt": "_np.sqrt", "abs": "_np.abs",
     "dabs": "_np.abs", "max": "_max", "min": "_min", "dble": "_np.float64", "exp": "_np.exp",
     "dexp": "_np.exp", "tanh": "_np.tanh", "sin": "_np.sin", "cos": "_np.cos", "sum": "_sum",
-    "dsin": "_np.sin", "dcos": "_np.cos",
+    "dsin": "_np.sin", "dcos": "_np.cos", "datan": "_np.arctan", "atan": "_np.arctan",
 }
 
 # subroutines whose second argument receives the first (MPI reductions on one rank): their
@@ -277,6 +284,8 @@ class Scope:
     def __init__(self, globals_arrays):
         self.arrays = dict(globals_arrays)  # name -> list of lower-bound code strings
         self.ints = set()
+        self.r4 = set()                     # default-real (single precision) variables
+        self.saved = {}                     # SAVE variable -> its module-level Python name
 
     def lb(self, name, k):
         return self.arrays[name][k]
@@ -295,7 +304,7 @@ def emit(e, sc):
     if k == "bool":
         return "True" if e.a else "False"
     if k == "name":
-        return _pyname(e.a)
+        return sc.saved.get(e.a, _pyname(e.a))
     if k == "paren":
         return "(" + emit(e.a, sc) + ")"
     if k == "neg":
@@ -326,7 +335,7 @@ def emit(e, sc):
                     subs.append(f"{lo}:{hi}")
                 else:
                     subs.append(f"({emit(s, sc)})-1" if not off else f"({emit(s, sc)})-{off}")
-            return f"{_pyname(name)}[{', '.join(subs)}]"
+            return f"{sc.saved.get(name, _pyname(name))}[{', '.join(subs)}]"
         fn = _INTRINSIC.get(name, _pyname(name))
         return f"{fn}({', '.join(emit(s, sc) for s in args)})"
     raise ValueError(k)
@@ -377,6 +386,8 @@ def _assign_split(s):
 
 
 _DECL = re.compile(r"^(real\s*\*\s*8|real|integer|double\s+precision|logical)\b")
+SAVED_INIT = {}    # module-level name of a SAVE variable -> its initialiser (Fortran text) or None
+ALLOC_DTYPE = {}   # (subroutine, allocatable array) -> numpy dtype of its allocation
 
 
 def _parse_dims(spec):
@@ -452,22 +463,37 @@ def translate_subroutine(sub, globals_arrays, trace=None):
             typ = md.group(1)
             attrs, _, ents = s.partition("::")
             dims = None
-            for at in _split_top(attrs)[1:]:
+            alist = _split_top(attrs)[1:]
+            save = "save" in alist
+            alloc = "allocatable" in alist
+            for at in alist:
                 if at.startswith("dimension"):
                     dims = _parse_dims(at[at.index("(") + 1:_close_paren(at, at.index("("))])
             for ent in _split_top(ents):
+                init = None
+                if "=" in ent and "(" not in ent.split("=")[0]:
+                    ent, init = (x.strip() for x in ent.split("=", 1))
                 nm, edims = ent, dims
                 if "(" in ent:
                     nm = ent[:ent.index("(")].strip()
                     edims = _parse_dims(ent[ent.index("(") + 1:_close_paren(ent, ent.index("("))])
                 if typ.startswith("integer"):
                     sc.ints.add(nm)
+                if typ == "real":
+                    sc.r4.add(nm)
+                if save or init is not None:  # SAVE (an initialiser implies it): module-level state
+                    gname = "_sv_%s_%s" % (sub.name, nm)
+                    sc.saved[nm] = gname
+                    SAVED_INIT[gname] = None if init is None else init
                 if edims is None:
                     continue
                 lbs = []
                 for lo, hi in edims:
                     lbs.append("1" if lo in ("", "1") else emit(parse_expr(lo), sc))
                 sc.arrays[nm] = lbs
+                if alloc:
+                    ALLOC_DTYPE[(sub.name, nm)] = "_np.int64" if typ.startswith("integer") else "_np.float64"
+                    continue
                 if nm not in sub.args:  # automatic local array
                     shape = ", ".join(f"({emit(parse_expr(hi), sc)})-({emit(parse_expr(lo), sc)})+1"
                                       for lo, hi in edims)
@@ -475,6 +501,8 @@ def translate_subroutine(sub, globals_arrays, trace=None):
                     pro.append(f"{_pyname(nm)} = _np.zeros(({shape},), dtype={dt})")
             continue
         body.append(s)
+    if sc.saved:
+        w("global " + ", ".join(sorted(sc.saved.values())))
     for p in pro:
         w(p)
     if trace is not None:
@@ -497,6 +525,17 @@ def translate_subroutine(sub, globals_arrays, trace=None):
         if s == "return":
             w("return")
             return
+        m = re.match(r"^allocate\s*\((.*)\)$", s)
+        if m:
+            for ent in _split_top(m.group(1)):
+                nm = ent[:ent.index("(")].strip()
+                dims = _split_top(ent[ent.index("(") + 1:_close_paren(ent, ent.index("("))])
+                shape = ", ".join(emit(parse_expr(d), sc) for d in dims)
+                dt = ALLOC_DTYPE.get((sub.name, nm), "_np.float64")
+                w(f"{sc.saved.get(nm, _pyname(nm))} = _np.zeros(({shape},), dtype={dt})")
+            return
+        if s.startswith("deallocate"):
+            return
         if s == "cycle":
             w("continue")
             return
@@ -510,7 +549,9 @@ def translate_subroutine(sub, globals_arrays, trace=None):
         r = emit(parse_expr(rhs), sc)
         le = parse_expr(lhs)
         if le.kind == "name" and le.a in sc.arrays:
-            w(f"{_pyname(le.a)}[...] = {r}")
+            w(f"{sc.saved.get(le.a, _pyname(le.a))}[...] = {r}")
+        elif le.kind == "name" and le.a in sc.r4:
+            w(f"{emit(le, sc)} = _r4({r})")
         else:
             w(f"{emit(le, sc)} = {r}")
 
@@ -605,6 +646,8 @@ def build(sources, globals_arrays, externals, trace=None, include_texts=None):
     the sources call but do not define; include_texts: lower-cased include file name -> text
     spliced in where the sources include it."""
     py, names, includes = [], [], []
+    SAVED_INIT.clear()
+    ALLOC_DTYPE.clear()
     glb = {k: ["1"] * _np.ndim(v) for k, v in globals_arrays.items()}
     for text in sources:
         subs, inc = split_subroutines(logical_lines(text), include_texts)
@@ -612,9 +655,12 @@ def build(sources, globals_arrays, externals, trace=None, include_texts=None):
         for sub in subs:
             py.append(translate_subroutine(sub, glb, trace))
             names.append(sub.name)
-    src = "\n".join(py)
+    inits = []
+    for gname, init in SAVED_INIT.items():
+        inits.append("%s = %s" % (gname, "None" if init is None else emit(parse_expr(init), Scope({}))))
+    src = "\n".join(inits) + "\n\n" + "\n".join(py)
     ns = {"_np": _np, "_div": _div, "_modulo": _modulo, "_mod": _mod, "_max": _max, "_min": _min,
-          "_frange": _frange, "_sum": _sum, "_trace": trace if trace is not None else []}
+          "_frange": _frange, "_sum": _sum, "_r4": _r4, "_trace": trace if trace is not None else []}
     ns.update({_pyname(k): v for k, v in globals_arrays.items()})
     ns.update({_pyname(k): v for k, v in externals.items()})
     exec(compile(src, "<fortran_subset>", "exec"), ns)

@@ -5,8 +5,9 @@ runs the reference's unmodified derivs.F90, nseq.F90 and timeIntegration.F90 (an
 lid-driven disturbance) through a Fortran-subset translator on small cases (periodic box,
 3-D and 2-D cavity channels with SFD, lid-driven cavity, boundary layer over a cavity): the
 line solves of every direction and kind, the right-hand side, the boundary conditions, the
-filters with and without the blend, and one time step as main.F90 sequences it.  Here the oracle runs the
-same cases on the same inputs and must agree to 1e-12 relative (max-norm per field; the
+filters with and without the blend, and one time step as main.F90 sequences it, with each
+of its three integrators and with the reference's forcings.  Here the oracle runs the same
+cases on the same inputs and must agree to 1e-12 relative (max-norm per field; the
 translated Fortran evaluates every expression in the reference's operation order, so the
 only differences are the oracle's own evaluation order where it fuses loops).
 """
