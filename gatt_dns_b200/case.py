@@ -50,7 +50,9 @@ class BoundaryInfo:
     cAdiabatic: np.ndarray = field(default_factory=lambda: np.zeros((0,), np.int32))
     neumannCoeffs: np.ndarray = field(default_factory=lambda: np.zeros(0))
     neumann2Coeffs: np.ndarray = field(default_factory=lambda: np.zeros(0))
-    # disturbances: dicts with keys type ('lidDrivenMovement'), var, ind (6,), X (box x coords), par (list)
+    # disturbances: dicts with keys type ('lidDrivenMovement', 'periodicSine', 'holdInlet'), var
+    # (the variables in the reference call's order, e.g. 'U' or 'UVRWE'), ind (6,), X (box x
+    # coords), par (list)
     disturbances: List[dict] = field(default_factory=list)
 
     def count(self, kind, var):
@@ -684,12 +686,13 @@ def boundary_layer_isothermal(nx, ny, nz=1, Re=1000.0, Ma=0.5, Pr=0.71, gamma=1.
     E0 = 1.0 / ((gamma ** 2 - gamma) * Ma ** 2)
     P0 = (gamma - 1) * E0
     items = []
-    # inflow (:4-78; the mesh starts at x <= 0)
-    if X[0] > 0:
-        raise ValueError("the inflow hold of boundaryLayerIsothermal.m:53-66 (X(1) > 0) is not restated")
+    # inflow (:4-78): Dirichlet u, v, w, e when the mesh starts at x <= 0; otherwise the
+    # holdInlet disturbance keeps the inflow plane at its first values (:53-66)
     inflow = [1, 1, 1, ny, 1, nz]
-    for v, val in (("u", 1.0), ("v", 0.0), ("w", 0.0), ("e", E0)):
-        items.append((v, "dir", "xi", val, list(inflow)))
+    hold = X[0] > 0
+    if not hold:
+        for v, val in (("u", 1.0), ("v", 0.0), ("w", 0.0), ("e", E0)):
+            items.append((v, "dir", "xi", val, list(inflow)))
     items.append(("p", "neu", "xi", 0.0, list(inflow)))
     # outflow (:80-138) and outer flow (:141-201)
     outflow = [nx, nx, 1, ny, 1, nz]
@@ -737,6 +740,9 @@ def boundary_layer_isothermal(nx, ny, nz=1, Re=1000.0, Ma=0.5, Pr=0.71, gamma=1.
         items.append(("e", "dir", "yi", E0, w))
     n1, n2 = mx.neumann_coefficients(6, 2)
     bc = init_boundaries(items, corners, mx.fortran_round(n1), mx.fortran_round(n2))
+    if hold:  # par 0: the density is not held
+        bc.disturbances.append(dict(type="holdInlet", var="UVRWE", ind=np.array(inflow, dtype=np.int32),
+                                    X=np.asarray(X[:1], dtype=np.float64), par=[0.0]))
     bufs = [{"i": sig(bxi, 30) if bxi else {"n": 0}, "f": sig(bxf, 15) if bxf else {"n": 0}},
             {"i": sig(byi, 30) if byi else {"n": 0}, "f": sig(byf, 30) if byf else {"n": 0}},
             {"i": {"n": 0}, "f": {"n": 0}}]
@@ -751,6 +757,25 @@ def boundary_layer_isothermal(nx, ny, nz=1, Re=1000.0, Ma=0.5, Pr=0.71, gamma=1.
         case.sfd_type, case.sfd_X, case.sfd_delta = 2, sfd[0], sfd[1]
         case.sfd_chi = sfd_region((nx, ny, nz), ((bxi, bxf), (byi, byf), (0, 0)), sfd[0])
     return case
+
+
+def add_disturbance(case: Case, dtype, var, ind, par):
+    """Append a disturbance to the case (a flowType.disturb entry with active = true and
+    forcing = false): dtype 'lidDrivenMovement', 'periodicSine' or 'holdInlet', var the
+    variables of the call ('V', or 'UVRWE' for holdInlet), ind the 1-based box
+    [i1 i2 j1 j2 k1 k2], par the parameters ([U0]; [omega, amplitude]; [holdDensity]).  The
+    box's x coordinates come from the mesh, as writeFortranDisturbances.m:40-50 writes them."""
+    ind = np.asarray(ind, dtype=np.int32)
+    case.bc.disturbances.append(dict(type=dtype, var=var, ind=ind, X=np.asarray(case.X[ind[0] - 1:ind[1]], dtype=np.float64),
+                                     par=[float(p) for p in par]))
+    return case
+
+
+def periodic_sine_strip(case: Case, i1, i2, omega=7.0, amp=0.02, var="V"):
+    """A periodicSine disturbance (blowing and suction) of `var` on the plate row of a
+    boundary layer, x nodes i1..i2, all z."""
+    j = int(np.nonzero(np.asarray(case.Y) >= 0)[0][0]) + 1
+    return add_disturbance(case, "periodicSine", var, [i1, i2, j, j, 1, case.nz], [omega, amp])
 
 
 def boundary_layer_cavity(nx=800, ny=300, nz=1, buffers=((40, 30), (0, 40)), sfd=(0.02, 15.0), **kw):

@@ -1,6 +1,7 @@
 // Boundary conditions on the device: applyBoundCond (reference
 // source/Fortran/nseq.F90:327-599) and the generated disturbance calls
-// (runDisturbances.F90; source/disturbances/lidDrivenMovement.F90).
+// (runDisturbances.F90; source/disturbances/lidDrivenMovement.F90, periodicSine.F90,
+// source/Fortran/holdInlet.F90).
 //
 // The reference applies its lists strictly in order (Dirichlet U,V,W,E,P; Neumann
 // U,V,W,E,P; corners; null second derivative U,V,W,E,P; disturbances), and later
@@ -34,7 +35,9 @@ enum BcOpCode {
     OP_R0 = 10,        // R(box) = 0
     OP_R_ADD_P = 11,   // R(box) += P
     OP_R_DIV_E = 12,   // R(box) = R/E/aux
-    OP_LID = 13        // lidDrivenMovement on F[var](box), x coordinates at xoff, U0 = val
+    OP_LID = 13,       // lidDrivenMovement on F[var](box), x coordinates at xoff, U0 = val
+    OP_SINE = 14,      // periodicSine: F[var](box) += xs[xoff + i - i1] * sin(val * t)
+    OP_HOLD = 15       // holdInlet: aux fields (U, V, W, E, then R) of the box <-> hold + xoff
 };
 
 struct BcOp {
@@ -45,7 +48,8 @@ struct BcOp {
     int len;        // extrapolation length
     int coef;       // 0 = neumannCoeffs, 1 = neumann2Coeffs
     int aux;        // divisor for corner averages
-    int xoff;       // offset of the box's x coordinates (OP_LID)
+    int xoff;       // offset of the box's x coordinates (OP_LID), of its x factors (OP_SINE), of
+                    // its values in the member's hold buffer (OP_HOLD)
     int sync;       // barrier after this op (the next op depends on this op's phase)
     double val;
     long long tape; // adjoint tape: offset of this op's recorded base values (-1: none)
@@ -58,10 +62,32 @@ struct BcProgram {
     int nops;
     const double *coef1;  // neumannCoeffs
     const double *coef2;  // neumann2Coeffs
-    const double *xs;     // disturbance coordinates
+    const double *xs;     // disturbance coordinates (OP_LID) and x factors (OP_SINE)
     double gamma;
     int nx, ny, nz;
+    // the time of the call: sp->t + tfac * sp->dt (the step's parameters on the device, so that
+    // one captured program serves every step), or tfix when sp is null
+    const StepParams *sp;
+    double tfac, tfix;
+    double *hold;         // holdInlet values, hstride per member
+    long long hstride;
+    int hold_save;        // 1: OP_HOLD keeps the fields (first call), 0: puts them back
 };
+
+__device__ __forceinline__ double bc_time(const BcProgram &pg)
+{
+    return pg.sp ? pg.sp->t + pg.tfac * pg.sp->dt : pg.tfix;
+}
+
+// periodicSine.F90:17-19: u + (amplitude sin(alpha (x_i - x_1))) sin(omega t), the x factor
+// precomputed per point; the product and the sum rounded separately as the reference does
+__device__ __forceinline__ double bc_sine(double u, double fx, double omega, double t)
+{
+    return __dadd_rn(u, __dmul_rn(fx, sin(omega * t)));
+}
+
+// holdInlet.F90 keeps u, v, w, e (and r with holdDensity): field of the v-th held value
+__device__ __forceinline__ int bc_hold_field(int v) { return v < 3 ? v : (v == 3 ? 4 : 3); }
 
 __device__ __forceinline__ long long bidx(const BcProgram &pg, int i, int j, int k)
 {
@@ -103,11 +129,12 @@ constexpr int kBcStagedOps = 48 * 1024 / (int)sizeof(BcOp);
 // tid of nthr; sync() is a barrier over all nthr threads that orders their memory accesses.
 // sops: the ops copied to this CTA's shared memory (nullptr: read them from pg.ops).
 template <typename Sync>
-__device__ __forceinline__ void bc_run(const BcProgram &pg, const BcOp *sops, double *const *F, double *P, int tid,
-                                       int nthr, Sync sync)
+__device__ __forceinline__ void bc_run(const BcProgram &pg, const BcOp *sops, double *const *F, double *P, double *H,
+                                       int tid, int nthr, Sync sync)
 {
     double *Rr = F[3], *Ee = F[4];
     const BcOp *ops = sops ? sops : pg.ops;
+    const double tnow = bc_time(pg);
     for (int o = 0; o < pg.nops; o++) {
         const BcOp op = ops[o];
         if (op.code == OP_NEU || op.code == OP_P_NEU) {
@@ -146,6 +173,14 @@ __device__ __forceinline__ void bc_run(const BcProgram &pg, const BcOp *sops, do
                 F[op.var][p] = op.val * (pp * pp);
                 break;
             }
+            case OP_SINE: F[op.var][p] = bc_sine(F[op.var][p], pg.xs[op.xoff + i - op.box[0]], op.val, tnow); break;
+            case OP_HOLD:
+                for (int v = 0; v < op.aux; v++) {
+                    double *h = H + op.xoff + (long long)v * total + q2;
+                    if (pg.hold_save) *h = F[bc_hold_field(v)][p];
+                    else F[bc_hold_field(v)][p] = *h;
+                }
+                break;
             default: break;
             }
         }
@@ -175,7 +210,8 @@ __global__ void k_bc(BcProgram pg, StateSet q, double *Pbase, long long pstride)
 #pragma unroll
     for (int f = 0; f < 5; f++) F[f] = q.v[f] + b * q.bstride;
     const BcOp *sops = bc_stage_ops(pg, bc_sops);
-    bc_run(pg, sops, F, Pbase + b * pstride, threadIdx.x, blockDim.x, [] { __syncthreads(); });
+    double *H = pg.hold ? pg.hold + b * pg.hstride : nullptr;
+    bc_run(pg, sops, F, Pbase + b * pstride, H, threadIdx.x, blockDim.x, [] { __syncthreads(); });
 }
 
 // One cluster of CTAs per batch member (cluster barriers); launched with a cluster dimension.
@@ -191,7 +227,8 @@ __global__ void k_bc_cluster(BcProgram pg, StateSet q, double *Pbase, long long 
     const int nthr = (int)cl.num_threads();
     const int tid = (int)cl.block_rank() * blockDim.x + threadIdx.x;
     const BcOp *sops = bc_stage_ops(pg, bc_sops);
-    bc_run(pg, sops, F, Pbase + b * pstride, tid, nthr, [&] { cl.sync(); });
+    double *H = pg.hold ? pg.hold + b * pg.hstride : nullptr;
+    bc_run(pg, sops, F, Pbase + b * pstride, H, tid, nthr, [&] { cl.sync(); });
 }
 
 // ---- tangent-linear and adjoint of the program (no counterpart in the reference) -------
@@ -244,6 +281,8 @@ __device__ __forceinline__ void k_bc_rec_run(int b, int tid, int nthr, Sync sync
     double *P = Pbase + b * pstride;
     double *Rr = F[3], *Ee = F[4];
     double *tp = tape + b * tstride;
+    double *H = pg.hold ? pg.hold + b * pg.hstride : nullptr;
+    const double tnow = bc_time(pg);
     for (int o = 0; o < pg.nops; o++) {
         const BcOp op = pg.ops[o];
         if (op.code == OP_NEU || op.code == OP_P_NEU) {
@@ -281,6 +320,10 @@ __device__ __forceinline__ void k_bc_rec_run(int b, int tid, int nthr, Sync sync
                 F[op.var][p] = op.val * (pp * pp);
                 break;
             }
+            case OP_SINE: F[op.var][p] = bc_sine(F[op.var][p], pg.xs[op.xoff + i - op.box[0]], op.val, tnow); break;
+            case OP_HOLD:  // the fields put back (the tangent and adjoint never run a first call)
+                for (int v = 0; v < op.aux; v++) F[bc_hold_field(v)][p] = H[op.xoff + (long long)v * total + q2];
+                break;
             default: break;
             }
         }
@@ -314,6 +357,8 @@ __device__ __forceinline__ void k_bc_tl_run(int b, int tid, int nthr, Sync sync,
     for (int f = 0; f < 5; f++) { F[f] = q.v[f] + b * q.bstride; dF[f] = dq.v[f] + b * dq.bstride; }
     double *P = Pbase + b * pstride, *dP = dPbase + b * pstride;
     double *Rr = F[3], *Ee = F[4], *dR = dF[3], *dE = dF[4];
+    double *H = pg.hold ? pg.hold + b * pg.hstride : nullptr;
+    const double tnow = bc_time(pg);
     for (int o = 0; o < pg.nops; o++) {
         const BcOp op = pg.ops[o];
         if (op.code == OP_NEU || op.code == OP_P_NEU) {
@@ -366,6 +411,14 @@ __device__ __forceinline__ void k_bc_tl_run(int b, int tid, int nthr, Sync sync,
                 dF[op.var][p] = 0.0;
                 break;
             }
+            // an additive forcing in time: the tangent passes through
+            case OP_SINE: F[op.var][p] = bc_sine(F[op.var][p], pg.xs[op.xoff + i - op.box[0]], op.val, tnow); break;
+            case OP_HOLD:  // held fields are constants
+                for (int v = 0; v < op.aux; v++) {
+                    F[bc_hold_field(v)][p] = H[op.xoff + (long long)v * total + q2];
+                    dF[bc_hold_field(v)][p] = 0.0;
+                }
+                break;
             default: break;
             }
         }
@@ -463,6 +516,10 @@ __device__ __forceinline__ void k_bc_adj_run(int b, int tid, int nthr, Sync sync
                 break;
             }
             case OP_LID: L[op.var][p] = 0.0; break;
+            case OP_SINE: break;
+            case OP_HOLD:
+                for (int v = 0; v < op.aux; v++) L[bc_hold_field(v)][p] = 0.0;
+                break;
             default: break;
             }
         }

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -85,7 +86,7 @@ struct HostBC {
 };
 
 struct Dist {
-    int type, var, ind[6], xoff;
+    int type, var, ind[6], xoff;  // xoff: x coordinates (lid) or x factors (periodic sine) in distx
     double par;
 };
 
@@ -125,6 +126,12 @@ struct gatt_ctx {
     BcOp *d_ops = nullptr;
     int nops = 0;
     double *d_coef1 = nullptr, *d_coef2 = nullptr, *d_xs = nullptr;
+    // holdInlet: the values the first gatt_apply_bc kept, hold_len per member, laid out as the
+    // program's OP_HOLD ops say (hold_sig: their boxes and field counts)
+    double *d_hold = nullptr;
+    long long hold_len = 0;
+    std::vector<int> hold_sig;
+    bool hold_saved = false;
     bool bc_dirty = true;
     // SFD
     int sfd_type = 0;
@@ -1139,9 +1146,24 @@ int build_bc_program(gatt_ctx *c)
     }
     TRY(neumann_lists(GATT_BC_SECOND, N2, 1));
     // disturbances (runDisturbances.F90)
+    long long hold_len = 0;
+    std::vector<int> hold_sig;
     for (const Dist &d : c->dists) {
         TRY(check_box(c, d.ind));
-        BcOp o = mk(OP_LID, d.var, d.ind); o.xoff = d.xoff; o.val = d.par; ops.push_back(o);
+        if (d.type == GATT_DIST_HOLD_INLET) {
+            BcOp o = mk(OP_HOLD, 0, d.ind);
+            o.aux = d.par > 0.5 ? 5 : 4;
+            const long long n = (long long)(d.ind[1] - d.ind[0] + 1) * (d.ind[3] - d.ind[2] + 1) * (d.ind[5] - d.ind[4] + 1);
+            if (hold_len + o.aux * n > INT_MAX) return fail(GATT_ERR_BADARG, "holdInlet boxes too large");
+            o.xoff = (int)hold_len;
+            hold_len += o.aux * n;
+            hold_sig.insert(hold_sig.end(), d.ind, d.ind + 6);
+            hold_sig.push_back(o.aux);
+            ops.push_back(o);
+        } else {
+            BcOp o = mk(d.type == GATT_DIST_PERIODIC_SINE ? OP_SINE : OP_LID, d.var, d.ind);
+            o.xoff = d.xoff; o.val = d.par; ops.push_back(o);
+        }
     }
     // phases: an op joins the running phase unless it reads or writes a field point that an op
     // of the phase writes, or writes one that it reads (fields U, V, W, R, E and the P scratch;
@@ -1152,6 +1174,8 @@ int build_bc_program(gatt_ctx *c)
             rd = wr = 0;
             switch (o.code) {
             case OP_SET: case OP_LID: wr = U; break;
+            case OP_SINE: rd = wr = U; break;
+            case OP_HOLD: rd = wr = 0x17u | (o.aux == 5 ? R : 0u); break;  // U V W E (R)
             case OP_DIR_P: rd = E; wr = R; break;
             case OP_NEU: rd = wr = U; break;
             case OP_P_LOAD: rd = R | E; wr = P; break;
@@ -1225,7 +1249,35 @@ int build_bc_program(gatt_ctx *c)
         CU(cudaMalloc(&c->d_xs, c->distx.size() * sizeof(double)));
         CU(cudaMemcpy(c->d_xs, c->distx.data(), c->distx.size() * sizeof(double), cudaMemcpyHostToDevice));
     }
+    if (hold_sig != c->hold_sig || (hold_len > 0 && !c->d_hold)) {  // a new hold layout: saved afresh
+        cudaFree(c->d_hold); c->d_hold = nullptr;
+        if (hold_len > 0) CU(cudaMalloc(&c->d_hold, sizeof(double) * (size_t)hold_len * c->nb));
+        c->hold_len = hold_len;
+        c->hold_sig = hold_sig;
+        c->hold_saved = false;
+    }
     c->bc_dirty = false;
+    return GATT_OK;
+}
+
+// The program as the kernels take it, at time t + tfac dt of the step parameters on the device
+BcProgram bc_program(const gatt_ctx *c, double tfac)
+{
+    BcProgram pg;
+    pg.ops = c->d_ops; pg.nops = c->nops; pg.coef1 = c->d_coef1; pg.coef2 = c->d_coef2; pg.xs = c->d_xs;
+    pg.gamma = c->ph.gamma; pg.nx = c->nx; pg.ny = c->ny; pg.nz = c->nz;
+    pg.sp = c->d_params; pg.tfac = tfac; pg.tfix = 0.0;
+    pg.hold = c->d_hold; pg.hstride = c->hold_len; pg.hold_save = 0;
+    return pg;
+}
+
+// holdInlet puts back what the first boundary-condition call kept (main.F90:112 makes that
+// call on the initial state): steps need it made
+int check_hold(gatt_ctx *c)
+{
+    if (c->bc_dirty) TRY(build_bc_program(c));
+    if (c->hold_len > 0 && !c->hold_saved)
+        return fail(GATT_ERR_STATE, "holdInlet: call gatt_apply_bc on the initial state before stepping");
     return GATT_OK;
 }
 
@@ -1309,13 +1361,19 @@ int launch_bc(gatt_ctx *c, void (*kblock)(KArgs...), void (*kcluster)(KArgs...),
     return GATT_OK;
 }
 
-int apply_bc(gatt_ctx *c, const StateSet &q, int nmem)
+// applyBoundCond at time t + tfac dt of the step (timeIntegration.F90 passes t + dt/2 or
+// t + dt by stage); fixed: at time tfix, keeping the holdInlet values on a first call
+int apply_bc(gatt_ctx *c, const StateSet &q, int nmem, double tfac, bool fixed = false, double tfix = 0.0)
 {
     if (c->bc_dirty) TRY(build_bc_program(c));
     if (c->nops == 0) return GATT_OK;
-    BcProgram pg;
-    pg.ops = c->d_ops; pg.nops = c->nops; pg.coef1 = c->d_coef1; pg.coef2 = c->d_coef2; pg.xs = c->d_xs;
-    pg.gamma = c->ph.gamma; pg.nx = c->nx; pg.ny = c->ny; pg.nz = c->nz;
+    BcProgram pg = bc_program(c, tfac);
+    if (fixed) {
+        pg.sp = nullptr; pg.tfix = tfix;
+        pg.hold_save = c->hold_saved ? 0 : 1;
+    } else if (c->hold_len > 0 && !c->hold_saved) {
+        return fail(GATT_ERR_STATE, "holdInlet: call gatt_apply_bc on the initial state before stepping");
+    }
     const size_t smem = c->nops <= kBcStagedOps ? (size_t)c->nops * sizeof(BcOp) : 0;  // staged ops
     TRY(before_launch(c, PC_BC));
     TRY(launch_bc(c, k_bc, k_bc_cluster, c->bc_cluster, nmem, smem, pg, q, c->P, (long long)c->npts));
@@ -1396,16 +1454,16 @@ int step_body(gatt_ctx *c)
     // input, updates the stage state and applies the boundary conditions
     if (c->time_stepping == 2) {  // EULER_2D/3D (timeIntegration.F90:158-223, 500-567)
         TRY(rhs_stage(c, q0, q0, qs, RK_EULER, nm, c->d1, c->tq, c->d2, c->delta));
-        TRY(apply_bc(c, qst, nm));
+        TRY(apply_bc(c, qst, nm, c->is3d ? 0.0 : 1.0));  // EULER_3D passes t, EULER_2D t + dt
     } else if (c->time_stepping == 3) {  // SSPRK3_2D/3D (timeIntegration.F90:225-336, 569-680)
         for (int s = 0; s < 3; s++) {
             TRY(rhs_stage(c, s == 0 ? q0 : qs, q0, qs, SSP_STAGE1 + s, nm, c->d1, c->tq, c->d2, c->delta));
-            TRY(apply_bc(c, qst, nm));
+            TRY(apply_bc(c, qst, nm, s == 1 ? 0.5 : 1.0));
         }
     } else {  // RK4_2D/3D (timeIntegration.F90:8-156, 338-498)
         for (int s = 1; s <= 4; s++) {
             TRY(rhs_stage(c, s == 1 ? q0 : qs, q0, qs, s, nm, c->d1, c->tq, c->d2, c->delta));
-            TRY(apply_bc(c, qst, nm));
+            TRY(apply_bc(c, qst, nm, s <= 2 ? 0.5 : 1.0));
         }
     }
     // nothing after the filter (no SFD, no boundary program): its last sweep can take the
@@ -1421,7 +1479,7 @@ int step_body(gatt_ctx *c)
                                                                           c->is3d ? 5 : 4, c->npts, c->d_params);
         TRY(after_launch(c));
     }
-    TRY(apply_bc(c, qs, nm));
+    TRY(apply_bc(c, qs, nm, 1.0));  // main.F90:405, at t + dt
     if (!mc_done) {
         TRY(before_launch(c, PC_MAXCHANGE));
         k_maxchange<<<dim3(grid_for(c, c->npts), nm), kBlock, 0, c->stream>>>(qs, q0, c->acc, c->npts);
@@ -1475,6 +1533,7 @@ int run_steps(gatt_ctx *c, int nsteps, double t0, double dt, double *maxChange, 
     if (nsteps < 1) return fail(GATT_ERR_BADARG, "nsteps < 1");
     if (!(dt > 0) || !std::isfinite(dt)) return fail(GATT_ERR_BADARG, "dt must be positive and finite");
     if (c->sfd_type > 0 && !c->chi) return fail(GATT_ERR_STATE, "SFD field not set");
+    TRY(check_hold(c));
     TRY(ensure_hist(c, nsteps));
     if (c->sfd_type > 0 && !c->mean_init) {
         // Umean = U when no mean flow was given (main.F90:158-163)
@@ -1766,7 +1825,7 @@ int check_diff(gatt_ctx *c, bool adjoint, bool step = false)
     if (step && c->time_stepping != 1)
         return fail(GATT_ERR_STATE, "the tangent-linear and adjoint steps are those of RK4 (timeStepping 1)");
     if (c->fc.n > 0) return fail(GATT_ERR_STATE, "the tangent-linear and adjoint do not cover forcings");
-    if (c->bc_dirty) TRY(build_bc_program(c));
+    TRY(check_hold(c));
     if (step && diff_sfd(c) && (!c->mean || !c->mean_init))
         return fail(GATT_ERR_STATE, "SFD: upload the mean (gatt_upload_mean) or run a step before the tangent/adjoint");
     const int ndir = c->is3d ? 3 : 2;
@@ -1833,31 +1892,23 @@ int diff_alloc(gatt_ctx *c, bool adjoint)
     return GATT_OK;
 }
 
-BcProgram bc_program(const gatt_ctx *c)
-{
-    BcProgram pg;
-    pg.ops = c->d_ops; pg.nops = c->nops; pg.coef1 = c->d_coef1; pg.coef2 = c->d_coef2; pg.xs = c->d_xs;
-    pg.gamma = c->ph.gamma; pg.nx = c->nx; pg.ny = c->ny; pg.nz = c->nz;
-    return pg;
-}
-
-// boundary program on base x and tangent y together
-int bc_tl(gatt_ctx *c, const StateSet &x, const StateSet &y)
+// boundary program on base x and tangent y together, at time t + tfac dt
+int bc_tl(gatt_ctx *c, const StateSet &x, const StateSet &y, double tfac)
 {
     if (c->nops == 0) return GATT_OK;
     TRY(before_launch(c, PC_BC));
-    TRY(launch_bc(c, k_bc_tl, k_bc_tl_cluster, c->bc_cluster_tl, c->nb, 0, bc_program(c), x, c->P, y, c->t_P,
+    TRY(launch_bc(c, k_bc_tl, k_bc_tl_cluster, c->bc_cluster_tl, c->nb, 0, bc_program(c, tfac), x, c->P, y, c->t_P,
                   (long long)c->npts));
     return after_launch(c);
 }
 
-// boundary program on base x, recording tape number `which` (0..4)
-int bc_rec(gatt_ctx *c, const StateSet &x, int which)
+// boundary program on base x at time t + tfac dt, recording tape number `which` (0..4)
+int bc_rec(gatt_ctx *c, const StateSet &x, int which, double tfac)
 {
     if (c->nops == 0) return GATT_OK;
     const long long ts = std::max(1LL, c->tape_len);
     TRY(before_launch(c, PC_BC));
-    TRY(launch_bc(c, k_bc_rec, k_bc_rec_cluster, c->bc_cluster_rec, c->nb, 0, bc_program(c), x, c->P,
+    TRY(launch_bc(c, k_bc_rec, k_bc_rec_cluster, c->bc_cluster_rec, c->nb, 0, bc_program(c, tfac), x, c->P,
                   (long long)c->npts, c->a_tape + which * ts * c->nb, ts));
     return after_launch(c);
 }
@@ -1869,7 +1920,7 @@ int bc_adj(gatt_ctx *c, const StateSet &lam, int which)
     const long long ts = std::max(1LL, c->tape_len);
     CU(cudaMemsetAsync(c->a_lP, 0, sizeof(double) * (size_t)c->npts * c->nb, c->stream));
     TRY(before_launch(c, PC_BC));
-    TRY(launch_bc(c, k_bc_adj, k_bc_adj_cluster, c->bc_cluster_adj, c->nb, 0, bc_program(c), lam, c->a_lP,
+    TRY(launch_bc(c, k_bc_adj, k_bc_adj_cluster, c->bc_cluster_adj, c->nb, 0, bc_program(c, 1.0), lam, c->a_lP,
                   (long long)c->npts, (const double *)(c->a_tape + which * ts * c->nb), ts));
     return after_launch(c);
 }
@@ -1965,13 +2016,13 @@ int tl_step(gatt_ctx *c)
     const StateSet Y0 = set5(c, c->dy[0]), YA = set5(c, c->dy[1]), YB = set5(c, c->dy[2]);
     // boundary conditions after every stage (timeIntegration.F90:406-491) and after the filter
     TRY(tl_stage(c, X0, X0, XA, Y0, Y0, YA, RK_STAGE1));
-    TRY(bc_tl(c, XA, YA));
+    TRY(bc_tl(c, XA, YA, 0.5));
     TRY(tl_stage(c, XA, X0, XB, YA, Y0, YB, RK_STAGE2));
-    TRY(bc_tl(c, XB, YB));
+    TRY(bc_tl(c, XB, YB, 0.5));
     TRY(tl_stage(c, XB, X0, XA, YB, Y0, YA, RK_STAGE3));
-    TRY(bc_tl(c, XA, YA));
+    TRY(bc_tl(c, XA, YA, 1.0));
     TRY(tl_stage(c, XA, X0, XB, YA, Y0, YB, RK_STAGE4));
-    TRY(bc_tl(c, XB, YB));
+    TRY(bc_tl(c, XB, YB, 1.0));
     // the filter is linear: the same sweeps act on the tangent (main.F90:357-378)
     const double *bdt = c->fct > 0 ? &c->d_params->dt : nullptr;
     TRY(filter_set(c, XB, c->nb, 0.0, bdt));
@@ -1981,7 +2032,7 @@ int tl_step(gatt_ctx *c)
         TRY(sfd_set(c, XB, c->dxm));
         TRY(sfd_set(c, YB, c->dym));
     }
-    TRY(bc_tl(c, XB, YB));
+    TRY(bc_tl(c, XB, YB, 1.0));
     TRY(copy_set5(c, c->dx[0], c->dx[2]));
     return copy_set5(c, c->dy[0], c->dy[2]);
 }
@@ -2052,7 +2103,7 @@ int adj_step(gatt_ctx *c, double dt)
     // recording the boundary program's tapes: 0..3 after the stages, 4 after filter and SFD
     for (int s = 1; s <= 4; s++) {
         TRY(rhs_stage_d(c, X[s - 1], X[0], X[s], s));
-        TRY(bc_rec(c, X[s], s - 1));
+        TRY(bc_rec(c, X[s], s - 1, s <= 2 ? 0.5 : 1.0));
     }
     if (c->nops > 0) {
         TRY(copy_set5(c, c->a_tmp, c->dx[4]));
@@ -2061,7 +2112,7 @@ int adj_step(gatt_ctx *c, double dt)
             TRY(copy_set5(c, c->a_mscr, c->dxm));
             TRY(sfd_set(c, set5(c, c->a_tmp), c->a_mscr));
         }
-        TRY(bc_rec(c, set5(c, c->a_tmp), 4));
+        TRY(bc_rec(c, set5(c, c->a_tmp), 4, 1.0));
     }
     TRY(bc_adj(c, set5(c, c->a_lam), 4));
     if (diff_sfd(c)) {
@@ -2446,7 +2497,7 @@ void gatt_destroy(gatt_ctx *c)
         cudaFree(c->ltype[d]);
     }
     double *bufs[] = {c->qA, c->qB, c->delta, c->mean, c->d1, c->tq, c->d2, c->P, c->tmp, c->tmp_side, c->tin, c->tout, c->chi, c->hist,
-                      c->d_coef1, c->d_coef2, c->d_xs, c->arn_zeta, c->arn_B, c->arn_base, c->arn_um,
+                      c->d_coef1, c->d_coef2, c->d_xs, c->d_hold, c->arn_zeta, c->arn_B, c->arn_base, c->arn_um,
                       c->arn_part, c->arn_h};
     cudaFree(c->arn_region);
     for (double *p : c->dx) cudaFree(p);
@@ -2655,17 +2706,31 @@ int gatt_set_corners(gatt_ctx *c, int cN, const int *cL, const int *cD, const in
 int gatt_add_disturbance(gatt_ctx *c, int type, int var, const int *ind, const double *x, int npar, const double *par)
 {
     if (!c) return fail(GATT_ERR_BADARG, "null context");
-    if (type != GATT_DIST_LID_DRIVEN) return fail(GATT_ERR_BADARG, "unsupported disturbance type");
-    if (var < 0 || var > 4 || !ind || !x || npar < 1 || !par) return fail(GATT_ERR_BADARG, "bad disturbance arguments");
+    if (type != GATT_DIST_LID_DRIVEN && type != GATT_DIST_PERIODIC_SINE && type != GATT_DIST_HOLD_INLET)
+        return fail(GATT_ERR_BADARG, "unsupported disturbance type");
+    const bool hold = type == GATT_DIST_HOLD_INLET;
+    const int need = type == GATT_DIST_PERIODIC_SINE ? 2 : 1;
+    if ((!hold && (var < 0 || var > 4 || !x)) || !ind || npar < need || !par)
+        return fail(GATT_ERR_BADARG, "bad disturbance arguments");
     Dist d;
-    d.type = type; d.var = var;
+    d.type = type; d.var = hold ? 0 : var;
     for (int q = 0; q < 6; q++) d.ind[q] = ind[q];
-    if (d.ind[1] < d.ind[0]) return fail(GATT_ERR_BADARG, "empty disturbance box");
+    for (int q = 0; q < 3; q++)
+        if (d.ind[2 * q + 1] < d.ind[2 * q]) return fail(GATT_ERR_BADARG, "empty disturbance box");
     const int nxb = d.ind[1] - d.ind[0] + 1;
-    if (nxb > 1 && x[nxb - 1] == x[0]) return fail(GATT_ERR_BADARG, "degenerate disturbance coordinates");
     d.xoff = (int)c->distx.size();
-    c->distx.insert(c->distx.end(), x, x + nxb);
     d.par = par[0];
+    if (type == GATT_DIST_LID_DRIVEN) {
+        if (nxb > 1 && x[nxb - 1] == x[0]) return fail(GATT_ERR_BADARG, "degenerate disturbance coordinates");
+        c->distx.insert(c->distx.end(), x, x + nxb);
+    } else if (type == GATT_DIST_PERIODIC_SINE) {
+        // periodicSine.F90:14-19: pi and alpha are default (single precision) reals there; the
+        // factor amplitude*sin(alpha*(x_i - x_1)) of each x is formed here once
+        if (nxb < 2 || x[nxb - 1] == x[0]) return fail(GATT_ERR_BADARG, "degenerate disturbance coordinates");
+        const float pi = (float)(4.0 * atan(1.0));
+        const float alpha = (float)(2.0 * (double)pi / (x[nxb - 1] - x[0]));
+        for (int i = 0; i < nxb; i++) c->distx.push_back(par[1] * sin((double)alpha * (x[i] - x[0])));
+    }
     c->dists.push_back(d);
     c->bc_dirty = true;
     invalidate_graphs(c);
@@ -2819,11 +2884,12 @@ int gatt_state_device_ptr(gatt_ctx *c, int b, int var, double **dptr)
 
 int gatt_apply_bc(gatt_ctx *c, double t)
 {
-    (void)t;
     if (!c) return fail(GATT_ERR_BADARG, "null context");
     if (!c->phys_set) return fail(GATT_ERR_STATE, "gatt_set_physics not called");
-    TRY(apply_bc(c, state_set(c, 0), c->nb));
+    if (!std::isfinite(t)) return fail(GATT_ERR_BADARG, "t must be finite");
+    TRY(apply_bc(c, state_set(c, 0), c->nb, 0.0, true, t));
     TRY(sync_stream(c));
+    if (c->hold_len > 0) c->hold_saved = true;
     return GATT_OK;
 }
 
@@ -3035,6 +3101,7 @@ int gatt_profile_kernels(gatt_ctx *c, double t0, double dt, int nsteps, double *
     TRY(check_ready(c, true));
     TRY(ensure_hist(c, 1));
     if (c->sfd_type > 0 && !c->mean_init) return fail(GATT_ERR_STATE, "run a step before profiling with SFD");
+    TRY(check_hold(c));
     for (int i = 0; i < PC_N; i++) { ms[i] = 0; launches[i] = 0; }
     double t = t0;
     int rc = GATT_OK;

@@ -259,7 +259,7 @@ def write_run_disturbances_f90(case: Case, path):
             args = "%d,%d,%d,(/%s/),(/%s/),(/%s/),t" % (
                 i[1] - i[0] + 1, i[3] - i[2] + 1, i[5] - i[4] + 1, ",".join(_fmt(v) for v in X),
                 ",".join(_fmt(v) for v in Y), ",".join(_fmt(v) for v in Z))
-            args += ",%s(%d:%d,%d:%d,%d:%d)" % (d["var"], i[0], i[1], i[2], i[3], i[4], i[5])
+            args += "".join(",%s(%d:%d,%d:%d,%d:%d)" % (v, i[0], i[1], i[2], i[3], i[4], i[5]) for v in d["var"])
             args += "".join("," + _fmt(p) for p in d["par"])
             f.write("            call %s(%s)\n" % (d["type"], args))
         f.write("    end select\n")
@@ -307,7 +307,7 @@ def read_run_forcings_f90(path):
 
 
 def read_run_disturbances_f90(path):
-    """Disturbance calls of rank 0 (only lidDrivenMovement is supported by the GPU path)."""
+    """Disturbance calls of rank 0 (lidDrivenMovement, periodicSine, holdInlet)."""
     text = open(path).read()
     r0, _ = _rank0(text)
     out = []
@@ -315,10 +315,10 @@ def read_run_disturbances_f90(path):
         name, args = m.group(1), m.group(2)
         arrays = re.findall(r"\(/(.*?)/\)", args)
         X = np.array([_to_float(t) for t in arrays[0].split(",")])
-        box = re.search(r",([UVWRE])\((\d+):(\d+),(\d+):(\d+),(\d+):(\d+)\)", args)
-        var = box.group(1)
-        ind = np.array([int(box.group(k)) for k in range(2, 8)], dtype=np.int32)
-        tail = args[box.end():]
+        boxes = list(re.finditer(r",([UVWRE])\((\d+):(\d+),(\d+):(\d+),(\d+):(\d+)\)", args))
+        var = "".join(b.group(1) for b in boxes)
+        ind = np.array([int(boxes[0].group(k)) for k in range(2, 8)], dtype=np.int32)
+        tail = args[boxes[-1].end():]
         par = [_to_float(t) for t in tail.split(",") if t.strip()]
         out.append(dict(type=name, var=var, ind=ind, X=X, par=par))
     return out
@@ -339,7 +339,8 @@ def case_from_fortran_dir(bin_dir, name="reference_case", sfd_chi=None):
     bc.neumannCoeffs, bc.neumann2Coeffs = n1, n2
     rd = os.path.join(bin_dir, "runDisturbances.F90")
     if os.path.exists(rd):
-        bc.disturbances = [d for d in read_run_disturbances_f90(rd) if d["type"] == "lidDrivenMovement"]
+        bc.disturbances = [d for d in read_run_disturbances_f90(rd)
+                           if d["type"] in ("lidDrivenMovement", "periodicSine", "holdInlet")]
     forcings = []
     for nm in ("runForcings3D.F90", "runForcings2D.F90"):
         rf = os.path.join(bin_dir, nm)

@@ -19,7 +19,7 @@ _pd = ctypes.POINTER(ctypes.c_double)
 _pi = ctypes.POINTER(ctypes.c_int)
 
 KIND = {"d": 0, "n": 1, "s": 2}
-DIST_TYPE = {"lidDrivenMovement": 1}
+DIST_TYPE = {"lidDrivenMovement": 1, "periodicSine": 2, "holdInlet": 3}
 FORCE_TYPE = {"pressureGradient": 1, "turbulenceGenerator": 2}  # GATT_FORCE_*
 
 
@@ -109,7 +109,9 @@ class GattDNS:
             ind = _i32(d["ind"])
             x = _f64(d["X"])
             par = _f64(d["par"])
-            _lib.check(L.gatt_add_disturbance(self.h, DIST_TYPE[d["type"]], VAR_INDEX[d["var"]], _ip(ind), _dp(x),
+            # holdInlet acts on all of U, V, R, W, E (its var is "UVRWE"); the others on one variable
+            var = 0 if d["type"] == "holdInlet" else VAR_INDEX[d["var"]]
+            _lib.check(L.gatt_add_disturbance(self.h, DIST_TYPE[d["type"]], var, _ip(ind), _dp(x),
                                               par.size, _dp(par)), "gatt_add_disturbance")
         for f in getattr(c, "forcings", None) or []:
             ind = np.ascontiguousarray(np.asarray(f["ind"], dtype=np.int32))

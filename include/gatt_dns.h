@@ -45,7 +45,7 @@ enum {
 
 enum { GATT_VAR_U = 0, GATT_VAR_V = 1, GATT_VAR_W = 2, GATT_VAR_R = 3, GATT_VAR_E = 4 };
 enum { GATT_BC_DIRICHLET = 0, GATT_BC_NEUMANN = 1, GATT_BC_SECOND = 2 };
-enum { GATT_DIST_LID_DRIVEN = 1 };
+enum { GATT_DIST_LID_DRIVEN = 1, GATT_DIST_PERIODIC_SINE = 2, GATT_DIST_HOLD_INLET = 3 };
 
 const char *gatt_strerror(int code);
 /* Text of the last error raised on this host thread (CUDA message, argument name). */
@@ -104,10 +104,21 @@ int gatt_set_bc(gatt_ctx *ctx, int var, int kind, int n, const int *ind, const d
 /* Corners: cN, cL(cN,6), cD(cN,3), cAdiabatic(cN) of boundaryInfo.F90 (nseq.F90:402-488). */
 int gatt_set_corners(gatt_ctx *ctx, int cN, const int *cL, const int *cD, const int *cAdiabatic);
 
-/* One generated disturbance call of runDisturbances.F90 (writeFortranDisturbances.m:35-90):
- * type GATT_DIST_LID_DRIVEN = lidDrivenMovement(nx,ny,nz,x,y,z,t,u,U0)
- * (source/disturbances/lidDrivenMovement.F90), applied to variable `var` on the 1-based
- * box ind[6] with the box's x coordinates x[ind[1]-ind[0]+1] and parameters par[npar]. */
+/* One generated disturbance call of runDisturbances.F90 (writeFortranDisturbances.m:35-90)
+ * on the 1-based box ind[6], applied in the order added, with the box's x coordinates
+ * x[ind[1]-ind[0]+1] and parameters par[npar]:
+ * GATT_DIST_LID_DRIVEN = lidDrivenMovement(nx,ny,nz,x,y,z,t,u,U0)
+ *   (source/disturbances/lidDrivenMovement.F90) on variable `var`, par = {U0};
+ * GATT_DIST_PERIODIC_SINE = periodicSine(nx,ny,nz,x,y,z,t,u,omega,amplitude)
+ *   (source/disturbances/periodicSine.F90) on variable `var`, par = {omega, amplitude}, at the
+ *   time of each boundary-condition call (t + dt/2 or t + dt by stage, as timeIntegration.F90
+ *   passes it; gatt_apply_bc's t);
+ * GATT_DIST_HOLD_INLET = holdInlet(nx,ny,nz,x,y,z,t,u,v,r,w,e,holdDensity)
+ *   (source/Fortran/holdInlet.F90) on U, V, W, E and, with par[0] > 0.5, R (var and x
+ *   unused): the first gatt_apply_bc keeps their values on the box (main.F90:112 makes that
+ *   call on the initial state), every later call puts them back.  Steps, the tangent-linear
+ *   and the adjoint return GATT_ERR_STATE until that first call was made; adding or
+ *   clearing disturbances that changes the held boxes drops the kept values. */
 int gatt_add_disturbance(gatt_ctx *ctx, int type, int var, const int *ind, const double *x,
                          int npar, const double *par);
 int gatt_clear_disturbances(gatt_ctx *ctx);
@@ -148,7 +159,8 @@ int gatt_download_wnew(gatt_ctx *ctx, int b, double *Wnew);
  * on the GPU between calls.  Valid until gatt_destroy. */
 int gatt_state_device_ptr(gatt_ctx *ctx, int b, int var, double **dptr);
 
-/* applyBoundCond on the device state at time t (nseq.F90:327-518), all members. */
+/* applyBoundCond on the device state at time t (nseq.F90:327-518), all members; the first
+ * call keeps the holdInlet values (GATT_DIST_HOLD_INLET). */
 int gatt_apply_bc(gatt_ctx *ctx, double t);
 
 /* One compact line solve -- solveSystem{X,Y,Z}[per] (derivs.F90:556-948) -- of the host

@@ -15,6 +15,8 @@ module gatt_dns
         GATT_VAR_E = 4
     integer(c_int), parameter :: GATT_BC_DIRICHLET = 0, GATT_BC_NEUMANN = 1, GATT_BC_SECOND = 2
     integer(c_int), parameter :: GATT_DIST_LID_DRIVEN = 1
+    integer(c_int), parameter :: GATT_DIST_PERIODIC_SINE = 2
+    integer(c_int), parameter :: GATT_DIST_HOLD_INLET = 3
 
     interface
         function gatt_strerror(code) bind(C, name='gatt_strerror')

@@ -46,7 +46,9 @@ class _Case(ctypes.Structure):
                 ("distX", _pd), ("distXoff", _pi), ("distPar", _pd),
                 ("sfdType", ctypes.c_int), ("sfdDelta", ctypes.c_double), ("sfdChi", _pd),
                 ("timeStepping", ctypes.c_int),
-                ("nForce", ctypes.c_int), ("forceType", _pi), ("forceInd", _pi), ("forcePar", _pd)]
+                ("nForce", ctypes.c_int), ("forceType", _pi), ("forceInd", _pi), ("forcePar", _pd),
+                ("distPar2", _pd), ("holdSave", _pd), ("holdOff", ctypes.POINTER(ctypes.c_long)),
+                ("holdSaved", _pi)]
 
 
 def build():
@@ -136,8 +138,9 @@ class Oracle:
         nd = len(bc.disturbances)
         c.nDist = nd
         if nd:
-            typ = self._hold(np.array([1 for _ in bc.disturbances], dtype=np.int32))
-            var = self._hold(np.array([vmap["P" if d["var"] == "R" else d["var"]] for d in bc.disturbances],
+            dcode = {"lidDrivenMovement": 1, "periodicSine": 2, "holdInlet": 3}
+            typ = self._hold(np.array([dcode[d["type"]] for d in bc.disturbances], dtype=np.int32))
+            var = self._hold(np.array([vmap["P" if d["var"][0] == "R" else d["var"][0]] for d in bc.disturbances],
                                       dtype=np.int32))
             ind = self._hold(np.asfortranarray(np.array([d["ind"] for d in bc.disturbances], dtype=np.int32)))
             xs, offs = [], []
@@ -147,6 +150,17 @@ class Oracle:
             X = self._hold(np.concatenate(xs))
             off = self._hold(np.array(offs, dtype=np.int32))
             par = self._hold(np.array([d["par"][0] for d in bc.disturbances], dtype=np.float64))
+            par2 = self._hold(np.array([d["par"][1] if len(d["par"]) > 1 else 0.0 for d in bc.disturbances],
+                                       dtype=np.float64))
+            c.distPar2 = par2.ctypes.data_as(_pd)
+            # holdInlet: the first call's values, U V W E R per box (holdInlet.F90)
+            sizes = [5 * int(np.prod([d["ind"][2 * a + 1] - d["ind"][2 * a] + 1 for a in range(3)]))
+                     if d["type"] == "holdInlet" else 0 for d in bc.disturbances]
+            hoff = self._hold(np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64))
+            hsave = self._hold(np.zeros(max(1, int(np.sum(sizes)))))
+            self.hold_saved = self._hold(np.zeros(nd, dtype=np.int32))
+            c.holdSave, c.holdSaved = hsave.ctypes.data_as(_pd), self.hold_saved.ctypes.data_as(_pi)
+            c.holdOff = hoff.ctypes.data_as(ctypes.POINTER(ctypes.c_long))
             c.distType, c.distVar, c.distInd = (a.ctypes.data_as(_pi) for a in (typ, var, ind))
             c.distX, c.distXoff, c.distPar = X.ctypes.data_as(_pd), off.ctypes.data_as(_pi), par.ctypes.data_as(_pd)
         c.timeStepping = int(getattr(case, "time_stepping", 1))

@@ -393,6 +393,39 @@ static void apply_neumann(const orc_case *c, double *u, box_t b, int dir, int le
         for (int j_ = (b).j1; j_ <= (b).j2; j_++) \
             for (int i_ = (b).i1; i_ <= (b).i2; i_++)
 
+/* periodicSine (source/disturbances/periodicSine.F90): pi and alpha are default reals
+ * (single precision) there, so they are rounded to float here too. */
+static void periodic_sine(const orc_case *c, double *u, box_t b, const double *x, double omega, double amp,
+                          double t)
+{
+    const int n = b.i2 - b.i1 + 1;
+    const float pi = (float)(4.0 * atan(1.0));
+    const float alpha = (float)(2.0 * (double)pi / (x[n - 1] - x[0]));
+    for (int k = b.k1; k <= b.k2; k++)
+        for (int j = b.j1; j <= b.j2; j++)
+            for (int i = 0; i < n; i++) {
+                const long p = IDX(c, b.i1 + i, j, k);
+                u[p] = u[p] + amp * sin((double)alpha * (x[i] - x[0])) * sin(omega * t);
+            }
+}
+
+/* holdInlet (source/Fortran/holdInlet.F90): the first call keeps U, V, W, E (and R when the
+ * density is held) on the box, every later call puts them back. */
+static void hold_inlet(const orc_case *c, double *const *F, box_t b, double *save, int *saved, int holdR)
+{
+    const int order[5] = {0, 1, 2, 4, 3};  /* u, v, w, e, then r */
+    const int nv = (*saved ? *saved - 1 : holdR) ? 5 : 4;
+    long q = 0;
+    for (int v = 0; v < nv; v++)
+        FOR_BOX(b) {
+            const long p = IDX(c, i_, j_, k_);
+            if (*saved) F[order[v]][p] = save[q];
+            else save[q] = F[order[v]][p];
+            q++;
+        }
+    if (!*saved) *saved = 1 + holdR;  /* 1: U, V, W, E held; 2: R too */
+}
+
 /* lidDrivenMovement (source/disturbances/lidDrivenMovement.F90:1-19). */
 static void lid_driven(const orc_case *c, double *u, box_t b, const double *x, double U0)
 {
@@ -409,7 +442,6 @@ static void lid_driven(const orc_case *c, double *u, box_t b, const double *x, d
 
 void orc_apply_bc(const orc_case *c, double *U, double *V, double *W, double *R, double *E, double t)
 {
-    (void)t;
     const long n = (long)c->nx * c->ny * c->nz;
     double *F[5] = {U, V, W, NULL, E};
     const double g = c->gamma;
@@ -496,6 +528,10 @@ void orc_apply_bc(const orc_case *c, double *U, double *V, double *W, double *R,
         box_t b = box_of(c->distInd, c->nDist, d);
         if (c->distType[d] == 1)
             lid_driven(c, vars[c->distVar[d]], b, c->distX + c->distXoff[d], c->distPar[d]);
+        else if (c->distType[d] == 2)
+            periodic_sine(c, vars[c->distVar[d]], b, c->distX + c->distXoff[d], c->distPar[d], c->distPar2[d], t);
+        else if (c->distType[d] == 3)
+            hold_inlet(c, vars, b, c->holdSave + c->holdOff[d], c->holdSaved + d, c->distPar[d] > 0.5);
     }
 }
 

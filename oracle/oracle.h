@@ -72,6 +72,14 @@ typedef struct {
     int nForce;
     const int *forceType, *forceInd;
     const double *forcePar;          /* two per forcing */
+    /* disturbances of types 2 = periodicSine (distPar = omega, distPar2 = amplitude; uses the
+     * boundary-condition time) and 3 = holdInlet (distPar > 0.5: hold the density too; the
+     * first call saves U, V, W, E (and R) on the box into holdSave + holdOff[d] and sets
+     * holdSaved[d], later calls restore them) */
+    const double *distPar2;
+    double *holdSave;
+    const long *holdOff;
+    int *holdSaved;
 } orc_case;
 
 int orc_num_threads(void);

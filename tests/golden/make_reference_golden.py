@@ -2,10 +2,11 @@
 small cases, through the Fortran-subset translator beside this script.
 
 Run it where the reference tree is present (it reads ``source/Fortran/derivs.F90``,
-``nseq.F90``, ``timeIntegration.F90`` and ``source/disturbances/lidDrivenMovement.F90``
-there, unmodified):
+``nseq.F90``, ``timeIntegration.F90``, ``holdInlet.F90`` and the disturbances
+``source/disturbances/lidDrivenMovement.F90``, ``periodicSine.F90``, ``pressureGradient.F90``
+and ``turbulenceGenerator.F90`` there, unmodified):
 
-    python tests/golden/make_reference_golden.py [reference root]
+    python tests/golden/make_reference_golden.py [reference root [case names...]]
 
 Each fixture holds, for one case built by ``gatt_dns_b200.case`` (the same builders the
 tests use; a checksum of the coefficient arrays is stored so that a changed builder is
@@ -60,7 +61,24 @@ def golden_cases():
         "turb_box": cs.turbulence_box(nxyz=(16, 12, 8)),
         "cavity2d_dpdx": _with_forcing(cs.cavity_channel(nx=24, ny=24, nz=1, sfd={"X": 0.05, "Delta": 10.0, "buffer": 6}),
                                        {"type": "pressureGradient", "ind": [3, 20, 2, 23, 1, 1], "par": [0.008]}),
+        # a boundary layer whose mesh starts downstream of the leading edge: holdInlet keeps the
+        # inflow plane (boundaryLayerIsothermal.m:53-66), and a periodicSine strip of V on the
+        # plate (the blowing and suction of source/disturbances/periodicSine.F90)
+        "bl_hold": _with_sine(cs.boundary_layer_isothermal(40, 28, 1, x_range=(0.5, 4.0))),
+        # the same in 3-D with the density held too (holdInlet's holdDensity > 0.5)
+        "bl_hold3d": _with_sine(_hold_density(cs.boundary_layer_isothermal(24, 24, 8, x_range=(0.5, 3.0))), i1=6, i2=14),
     }
+
+
+def _with_sine(case, i1=10, i2=20):
+    return cs.periodic_sine_strip(case, i1, i2, omega=7.0, amp=0.02)
+
+
+def _hold_density(case):
+    for d in case.bc.disturbances:
+        if d["type"] == "holdInlet":
+            d["par"] = [1.0]
+    return case
 
 
 def _with_forcing(case, f):
@@ -69,7 +87,7 @@ def _with_forcing(case, f):
 
 
 # cases that also hold one Euler and one SSPRK3 step (timeIntegration.F90:158-336, 500-680)
-SCHEME_CASES = ("box", "cavity2d", "lid", "bl_cavity", "turb_box")
+SCHEME_CASES = ("box", "cavity2d", "lid", "bl_cavity", "turb_box", "bl_hold", "bl_hold3d")
 
 
 def matrices_checksum(case):
@@ -106,8 +124,10 @@ def reference(case, root):
     nx, ny, nz = case.nx, case.ny, case.nz
     src = os.path.join(root, "source")
     texts = [open(os.path.join(src, "Fortran", f)).read() for f in ("derivs.F90", "nseq.F90", "timeIntegration.F90")]
-    for f in ("lidDrivenMovement", "pressureGradient", "turbulenceGenerator"):
+    for f in ("lidDrivenMovement", "periodicSine", "pressureGradient", "turbulenceGenerator"):
         texts.append(open(os.path.join(src, "disturbances", f + ".F90")).read())
+    # holdInlet lives beside the solver (writeFortranDisturbances.m:108-113)
+    texts.append(open(os.path.join(src, "Fortran", "holdInlet.F90")).read())
     one = np.array([1, 1, 1])
     size = np.array([nx, ny, nz])
     g = {"xstart": one, "ystart": one, "zstart": one, "xend": size, "yend": size, "zend": size,
@@ -291,6 +311,9 @@ def make(name, case, root):
 
 
 if __name__ == "__main__":
+    # make_reference_golden.py [reference root [case names...]]
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    only = set(sys.argv[2:])
     for name, case in golden_cases().items():
-        print(make(name, case, root))
+        if not only or name in only:
+            print(make(name, case, root))

@@ -5,7 +5,8 @@ with SFD the step maps the state and the mean, and the step vectors carry both (
 mE).  Cases: the 2-D lid-driven cavity (wall lists, corners, the moving-lid disturbance),
 a 2-D and a 3-D cavity channel with SFD on a buffer ramp, and the 2-D boundary layer over a
 cavity (free-slip upstream wall, break point, SFD in the buffer zones: the config-3 base-flow
-problem).  Checks as in test_gpu_tangent.py: RHS and step tangents against central finite
+problem), and 2-D and 3-D boundary layers that start downstream of the leading edge (holdInlet
+on the inflow plane, with the density held in 3-D; a periodicSine strip on the plate).  Checks as in test_gpu_tangent.py: RHS and step tangents against central finite
 differences of the nonlinear path (state and mean perturbed together), dot-product tests of
 the checkpointed adjoint, and the gradient of J = 1/2 sum(u^2 + v^2 + w^2).
 Tolerances: dot-product tests 1e-10 relative; central differences with h = 1e-4: 1e-6 (the
@@ -38,6 +39,17 @@ def _case(name):
             c = cs.cavity_channel(nx=24, ny=20, nz=8, adiabatic_corners=True,
                                   sfd={"X": 0.05, "Delta": 10.0, "buffer": 6})
             q = cs.random_flow(c, seed=5, amp=0.05)
+        elif name in ("bl_hold", "bl_hold3d"):
+            if name == "bl_hold":
+                c = cs.boundary_layer_isothermal(40, 28, 1, x_range=(0.5, 4.0))
+            else:
+                c = cs.boundary_layer_isothermal(24, 24, 8, x_range=(0.5, 3.0))
+                c.bc.disturbances[0]["par"] = [1.0]  # hold the density too
+            c = cs.periodic_sine_strip(c, 6, 14)
+            q = cs.blasius_flow(c)
+            r = cs.random_flow(c, seed=5, amp=0.01)
+            for k in ("U", "V", "W"):
+                q[k] = q[k] + r[k]
         else:
             c = cs.boundary_layer_cavity(nx=64, ny=40, buffers=((6, 5), (0, 6)))
             q = cs.blasius_flow(c)
@@ -60,7 +72,7 @@ def _case(name):
     return _CASES[name]
 
 
-@pytest.fixture(scope="module", params=["lid", "cavity2d_sfd", "cavity3d_sfd", "bl_cavity"])
+@pytest.fixture(scope="module", params=["lid", "cavity2d_sfd", "cavity3d_sfd", "bl_cavity", "bl_hold", "bl_hold3d"])
 def case(request):
     return _case(request.param)
 
@@ -90,6 +102,13 @@ def rel_err(a, b, keys):
 
 def _dt(c, q):
     return c.cfl_dt(q["U"], q["V"], q["W"], 0.5)
+
+
+def _prime(g, c, q, m):
+    """holdInlet: the first boundary-condition call keeps the unperturbed inflow plane."""
+    if any(d["type"] == "holdInlet" for d in c.bc.disturbances):
+        _start(g, q, m)
+        g.apply_bound_cond(0.0)
 
 
 def _start(g, q, m, v=None, h=0.0):
@@ -126,6 +145,7 @@ def test_step_tangent_against_differences(cuda_lib, case):
     v = rand_vec(c, 8, sfd)
     keys = (KEYS if c.is3d else ("U", "V", "R", "E"))
     with GattDNS(c) as g:
+        _prime(g, c, q, m)
         _start(g, q, m)
         jv = g.jvp(v, nsteps, 0.0, dt)
         out = {}
@@ -148,6 +168,7 @@ def test_step_dot_product_checkpointed(cuda_lib, case, nsteps, every):
     dt = _dt(c, q)
     v, w = rand_vec(c, 9, sfd), rand_vec(c, 10, sfd)
     with GattDNS(c) as g:
+        _prime(g, c, q, m)
         _start(g, q, m)
         jv = g.jvp(v, nsteps, 0.0, dt)
         _start(g, q, m)
@@ -184,6 +205,7 @@ def test_energy_gradient(cuda_lib, case):
         return float(sum(np.sum((up[k] - um[k]) * (up[k] + um[k])) for k in vel)) / (4 * h)
 
     with GattDNS(c) as g:
+        _prime(g, c, q, m)
         fN = final(g)
         z = np.zeros_like(fN["R"])
         lamN = {"U": fN["U"], "V": fN["V"], "W": fN["W"] if c.is3d else z, "R": z, "E": z}

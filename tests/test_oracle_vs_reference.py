@@ -3,7 +3,8 @@
 tests/golden/reference_<case>.npz were made by tests/golden/make_reference_golden.py, which
 runs the reference's unmodified derivs.F90, nseq.F90 and timeIntegration.F90 (and the
 lid-driven disturbance) through a Fortran-subset translator on small cases (periodic box,
-3-D and 2-D cavity channels with SFD, lid-driven cavity, boundary layer over a cavity): the
+3-D and 2-D cavity channels with SFD, lid-driven cavity, boundary layer over a cavity, 2-D
+and 3-D boundary layers with holdInlet and a periodicSine strip): the
 line solves of every direction and kind, the right-hand side, the boundary conditions, the
 filters with and without the blend, and one time step as main.F90 sequences it, with each
 of its three integrators and with the reference's forcings.  Here the oracle runs the same
@@ -35,7 +36,14 @@ def rel(a, b):
     return float(np.max(np.abs(np.asarray(a) - b)) / (s if s > 0 else 1.0))
 
 
-NAMES = ["box", "cavity3d", "cavity2d", "lid", "bl_cavity", "turb_box", "cavity2d_dpdx"]
+NAMES = ["box", "cavity3d", "cavity2d", "lid", "bl_cavity", "turb_box", "cavity2d_dpdx", "bl_hold", "bl_hold3d"]
+
+
+def prime_hold(o, case, z, flow):
+    """holdInlet keeps what the first applyBoundCond saw: the generator's first call was on
+    the seeded flow at t (main.F90:112 makes it on the initial state), so make it here too."""
+    if any(d["type"] == "holdInlet" for d in case.bc.disturbances):
+        o.apply_bound_cond(flow, float(z["t"]))
 
 
 @pytest.mark.parametrize("name", NAMES)
@@ -89,6 +97,7 @@ def test_time_step_matches_reference(oracle_lib, name):
     mk, case, z = _load(name)
     o = oracle.Oracle(case)
     flow = {k: z["flow_" + k] for k in ("U", "V", "W", "R", "E")}
+    prime_hold(o, case, z, flow)
     st = o.new_state(flow)
     mc = o.step(st, float(z["t"]), float(z["dt"]))
     for k in ("U", "V", "W", "R", "E"):
@@ -103,7 +112,7 @@ def test_time_step_matches_reference(oracle_lib, name):
 
 
 @pytest.mark.parametrize("scheme", [2, 3])
-@pytest.mark.parametrize("name", ["box", "cavity2d", "lid", "bl_cavity", "turb_box"])
+@pytest.mark.parametrize("name", ["box", "cavity2d", "lid", "bl_cavity", "turb_box", "bl_hold", "bl_hold3d"])
 def test_euler_and_ssprk3_steps_match_reference(oracle_lib, name, scheme):
     """timeStepping 2 (EULER_2D/3D) and 3 (SSPRK3_2D/3D) in the same main-loop step."""
     import dataclasses
@@ -113,6 +122,7 @@ def test_euler_and_ssprk3_steps_match_reference(oracle_lib, name, scheme):
     key = {2: "euler_", 3: "ssprk3_"}[scheme]
     o = oracle.Oracle(case)
     flow = {k: z["flow_" + k] for k in ("U", "V", "W", "R", "E")}
+    prime_hold(o, case, z, flow)
     st = o.new_state(flow)
     mc = o.step(st, float(z["t"]), float(z["dt"]))
     for k in ("U", "V", "W", "R", "E"):
