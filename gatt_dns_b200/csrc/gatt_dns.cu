@@ -1825,7 +1825,8 @@ int check_diff(gatt_ctx *c, bool adjoint, bool step = false)
     if (step && c->time_stepping != 1)
         return fail(GATT_ERR_STATE, "the tangent-linear and adjoint steps are those of RK4 (timeStepping 1)");
     if (c->fc.n > 0) return fail(GATT_ERR_STATE, "the tangent-linear and adjoint do not cover forcings");
-    TRY(check_hold(c));
+    if (step) TRY(check_hold(c));  // the right-hand side alone applies no boundary conditions
+    else if (c->bc_dirty) TRY(build_bc_program(c));
     if (step && diff_sfd(c) && (!c->mean || !c->mean_init))
         return fail(GATT_ERR_STATE, "SFD: upload the mean (gatt_upload_mean) or run a step before the tangent/adjoint");
     const int ndir = c->is3d ? 3 : 2;
