@@ -1009,15 +1009,17 @@ int rhs_stage(gatt_ctx *c, const StateSet &q, const StateSet &q0, const StateSet
     const int fin[4] = {0, 1, 3, 4};
     const int ox[4] = {D2_UX, D2_VX, D2_RX, D2_EX};
     const int oy[4] = {D2_UY, D2_VY, D2_RY, D2_EY};
-    TRY(sweep(c, 0, 0, qin, qbs, fin, d1, bd1, ox, 4, nmem, 0, nullptr, PC_D1X));
+    TRY(beside(c, [&] { return sweep(c, 0, 0, qin, qbs, fin, d1, bd1, ox, 4, nmem, 0, nullptr, PC_D1X); }));
     TRY(sweep(c, 1, 0, qin, qbs, fin, d1, bd1, oy, 4, nmem, 0, nullptr, PC_D1Y));
+    TRY(join_side(c));
     TRY(before_launch(c, PC_VISC));
     k_visc2d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(c->ph, q, fset(c, d1, D2_N), fset(c, tq, T2_N), n);
     TRY(after_launch(c));
     const int ix[3] = {T2_XY, T2_XX, T2_QX}, sx[3] = {S2_TXYX, S2_TXXX, S2_HTX};
     const int iy[3] = {T2_XY, T2_YY, T2_QY}, sy[3] = {S2_TXYY, S2_TYYY, S2_HTY};
-    TRY(sweep(c, 0, 0, tq, btq, ix, d2, bd2, sx, 3, nmem, 0, nullptr, PC_D2X));
+    TRY(beside(c, [&] { return sweep(c, 0, 0, tq, btq, ix, d2, bd2, sx, 3, nmem, 0, nullptr, PC_D2X); }));
     TRY(sweep(c, 1, 0, tq, btq, iy, d2, bd2, sy, 3, nmem, 0, nullptr, PC_D2Y));
+    TRY(join_side(c));
     TRY(before_launch(c, PC_ASSEMBLE));
     k_assemble2d<<<dim3(grid_for(c, n), nmem), kBlock, 0, c->stream>>>(
         c->ph, q, q0, out, fset(c, delta, 5), fset(c, d1, D2_N), fset(c, tq, T2_N), fset(c, d2, S2_N), n, mode, sp,
@@ -1408,11 +1410,13 @@ int filter_set(gatt_ctx *c, const StateSet &q, int nmem, double blend, const dou
         }
         return GATT_OK;
     };
-    if (!c->fork_x || c->profiling || !c->side || !c->is3d) return chain(fl, rl, nf);
-    // 3-D: the fields' filters are independent -- U, V, W on the context's stream, R, E beside
+    if (!c->fork_x || c->profiling || !c->side) return chain(fl, rl, nf);
+    // the fields' filters are independent -- U, V (and W) on the context's stream, R, E beside
     // them on the side stream, so that each direction's last partial wave overlaps the other
     // chain's launches
-    const int fa[3] = {0, 1, 2}, ra[3] = {2, 1, 0}, fb[2] = {3, 4}, rb[2] = {4, 3};
+    const int fa3[3] = {0, 1, 2}, ra3[3] = {2, 1, 0}, fa2[2] = {0, 1}, ra2[2] = {1, 0}, fb[2] = {3, 4}, rb[2] = {4, 3};
+    const int *fa = c->is3d ? fa3 : fa2, *ra = c->is3d ? ra3 : ra2;
+    const int na = c->is3d ? 3 : 2;
     CU(cudaEventRecord(c->ev_fork, c->stream));
     CU(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
     int r;
@@ -1422,7 +1426,7 @@ int filter_set(gatt_ctx *c, const StateSet &q, int nmem, double blend, const dou
     }
     TRY(r);
     CU(cudaEventRecord(c->ev_join, c->side));
-    TRY(chain(fa, ra, 3));
+    TRY(chain(fa, ra, na));
     CU(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
     return GATT_OK;
 }

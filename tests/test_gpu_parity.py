@@ -501,13 +501,15 @@ def test_x_tile_order_matches_tile_inner(libs, monkeypatch, name):
 
 
 @pytest.mark.parametrize("env", ["GATT_VISC_V2", "GATT_FZ_REV", "GATT_X_COMPACT", "GATT_X_WSTORE", "GATT_FORK_X"])
-@pytest.mark.parametrize("name", ["box", "box_ragged", "box_odd", "box_x400", "cavity3d"])
+@pytest.mark.parametrize("name", ["box", "box_ragged", "box_odd", "box_x400", "cavity3d", "lid", "cavity2d",
+                                  "lid_x400", "bl_cavity"])
 def test_stress_and_filter_order_variants_match(libs, monkeypatch, env, name):
     """The two-points-per-thread stress kernel, the reversed field order of every second
     filter direction, the compact shared-memory layout of the uniform-band x solver, the x
-    tiles stored chunk by chunk by their warps, and the x sweeps beside the y/z sweeps and two
-    filter field chains side by side on a second stream (the defaults; box_x400 takes the
-    global-memory line solver, whose scratch field each stream has its own of) against their
+    tiles stored chunk by chunk by their warps, and the x sweeps beside the y (and z) sweeps
+    and two filter field chains side by side on a second stream, in 3-D and 2-D (the defaults;
+    box_x400 and lid_x400 take the global-memory line solver, whose scratch field each stream
+    has its own of) against their
     plain forms (env var = 0): same arithmetic on every point and line, so states after three
     steps are equal bit for bit."""
     from gatt_dns_b200.solver import GattDNS
